@@ -1,0 +1,227 @@
+/*
+ * slg.h -- C ABI of the B200 (sm_100a) implementation of SuperLite's
+ * per-timestep hot path: physical LTE opacity + Planck/Rosseland means, DDMC
+ * leakage opacities and emission probabilities, the 1-D spherical IMC/DDMC
+ * particle loop, and the flux and source tallies.
+ *
+ * Each entry point replaces one argument-less Fortran subroutine of the
+ * reference (gururajw/superlite) that works on module arrays; the arrays it
+ * reads and writes become explicit arguments, with the reference's
+ * column-major layouts:  "(ng, ncell)" means group index fastest.
+ *
+ * Conventions
+ *  - The caller owns every host array.  The library copies inputs to the GPU,
+ *    runs, copies outputs back and keeps no host pointer after returning.
+ *  - Return value 0 = success.  Transport errors reuse the reference's ierr
+ *    codes (transport11: 1, 3, 4, 17; diffusion11: 100, 102) plus 1001 (the
+ *    per-particle step guard); library errors are negative (SLG_ERR_*).
+ *    slg_last_error() gives a message.  The library never exits the process.
+ *  - Fortran logicals are passed as int32 0/1.
+ *  - A context is bound to one device and one stream and is not re-entrant;
+ *    calls on one context must come from one host thread at a time.
+ *  - The grid is 1-D spherical without void cells: grd_icell(ix,1,1) = ix and
+ *    ncell = nx.
+ *  - Entry points named slg_dev_* take device pointers (and run on the
+ *    context's stream without host synchronisation); the others take host
+ *    pointers.
+ */
+#ifndef SLG_H
+#define SLG_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SLG_OK 0
+#define SLG_ERR_CUDA (-1)      /* a CUDA call failed (message in slg_last_error) */
+#define SLG_ERR_ARG (-2)       /* invalid argument or shape */
+#define SLG_ERR_STATE (-3)     /* required set-up call missing */
+#define SLG_ERR_UNSORTED (-4)  /* bb line list not sorted by wl0 */
+#define SLG_ERR_OOM (-5)       /* device allocation failed */
+#define SLG_ERR_NOT_BUILT (-6) /* kernel variant not compiled in */
+
+typedef struct slg_ctx slg_ctx;
+
+/* Line record, bbxsmod.f:27-34 (type bb_xs_data, 16 bytes). */
+typedef struct slg_bbxs {
+  float wl0;   /* line centre [Angstrom] */
+  float gxs;   /* g * f * pi e^2 / (m_e c) */
+  float chilw; /* lower level energy [cm^-1] */
+  int16_t iz;  /* element */
+  int16_t ii;  /* ion stage, 1 = neutral */
+} slg_bbxs;
+
+/* Particle record, particlemod.f90:7-11 (type packet, 64 bytes). */
+typedef struct slg_packet {
+  double x, y, z, mu, om, e, e0, wl;
+} slg_packet;
+
+/* ------------------------------------------------------------------ set-up */
+
+/* Create a context on CUDA device `device` (its own stream).  NULL on failure. */
+slg_ctx* slg_create(int device);
+void slg_destroy(slg_ctx* ctx);
+const char* slg_last_error(const slg_ctx* ctx);
+/* Library version string (build date + compiled arch). */
+const char* slg_version(void);
+
+/* groupmod_init (groupmod.f:29-96): grp_wl(ng+1) in cm, increasing.  Also sets
+ * grd_nep = nint(sqrt(ng)), grd_nepg = ceiling(ng/(nep+1)) (gridmod.f:121-122). */
+int slg_set_groups(slg_ctx* ctx, int32_t ng, const double* grp_wl);
+
+/* grid_setup + grid_volume (GRID/grid_setup.f:3-62, GRID/grid_volume.f:66-105):
+ * grd_xarr(nx+1), grd_vxarr(nx+1), grd_vol(nx), grd_divv(nx). */
+int slg_set_grid(slg_ctx* ctx, int32_t nx, const double* xarr, const double* vxarr,
+                 const double* vol, const double* divv);
+
+/* Permanent atomic data after bcast_permanent (mpimod_mpi.f:23-501):
+ * ion_el(iz)%ni (nelem), the bb line list sorted by wl0 (read_bbxs_data.f:84),
+ * bf_ph1(6,7,30,30), bf_ph2(7,30,30) (bfxsmod.f:14) and ff_gff(81,41)
+ * (ffxsmod.f:18-20).  nstage = slots per element in the oc/ginv arrays. */
+int slg_set_atomic_data(slg_ctx* ctx, int32_t nelem, int32_t nstage, const int32_t* ion_ni,
+                        int64_t nline, const slg_bbxs* bb_xs, const float* bf_ph1,
+                        const float* bf_ph2, const double* ff_gff);
+
+/* ------------------------------------------------------------------ opacity */
+
+/* Gas state read by physical_opacity (gasmod.f), all per shell (ncell = nx). */
+typedef struct slg_gas {
+  const double* temp;    /* gas_temp (ncell) */
+  const double* natom;   /* gas_natom (ncell) */
+  const double* nelec;   /* gas_nelec (ncell), electrons per atom */
+  const double* vol;     /* gas_vol (ncell) */
+  const double* mass;    /* gas_mass (ncell) */
+  const double* natomfr; /* gas_natomfr (0:nelem, ncell) */
+  const double* oc;      /* ion_grndlev(iz,i)%oc(ii) as (ncell, nstage, nelem) */
+  const double* ginv;    /* ion_grndlev(iz,i)%ginv(ii) as (ncell, nstage, nelem) */
+} slg_gas;
+
+typedef struct slg_opacity_flags {
+  int32_t nobb, nobf, noff, nothmson; /* in_nobbopac, in_nobfopac, in_noffopac, in_nothmson */
+  int32_t ngs;                        /* in_grp_ngs sub-groups per group (>= 1) */
+  double opacmixrossel;               /* in_opacmixrossel */
+} slg_opacity_flags;
+
+/* physical_opacity (GAS/physical_opacity.f:3-357).  Outputs gas_sig (ncell),
+ * gas_cap (ng, ncell) real*4, gas_emiss (ng, ncell) real*4 and optionally
+ * cap64 (ncell, ng), the double opacity before sngl() (:267).  *sanity
+ * (optional) receives the bitmask of the checks at :282-291. */
+int slg_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_flags* flags,
+                         double* gas_sig, float* gas_cap, float* gas_emiss, double* cap64,
+                         int32_t* sanity);
+
+/* analytic_opacity (GAS/analytic_opacity.f90:3-77).  kind: 1 grey, 2 mono, 3 line. */
+int slg_analytic_opacity(slg_ctx* ctx, const double* temp, const double* rho, int32_t kind,
+                         double capcoef, double captpwr, double caprpwr, double sigcoef,
+                         double sigtpwr, double sigrpwr, double ldisp1, double ldisp2,
+                         double* gas_sig, float* gas_cap);
+
+/* opacity_planckmean + opacity_rossmean (GAS/opacity_planckmean.f:17-24,
+ * GAS/opacity_rossmean.f:17-21): gas_capgrey, gas_capross (ncell). */
+int slg_opacity_means(slg_ctx* ctx, const double* temp, const double* sig, const float* gas_cap,
+                      double* capgrey, double* capross);
+
+/* ------------------------------------------------------------------ grid coefficients */
+
+/* leakage_opacity11 (GRID/leakage_opacity11.f90:3-174): grd_opaclump (11, ncell).
+ * capemit (ng, ncell) may be NULL (LTE: treated as zero). */
+int slg_leakage_opacity11(slg_ctx* ctx, const double* tempinv, const double* sig,
+                          const float* cap, const float* capemit, double tauddmc,
+                          double taulump, double* opaclump);
+
+/* emission_probability (GRID/emission_probability.f90:3-67, LTE): grd_emitprob (nep, ncell). */
+int slg_emission_probability(slg_ctx* ctx, const double* tempinv, const float* cap,
+                             const double* capgrey, double* emitprob);
+
+/* ------------------------------------------------------------------ transport */
+
+/* Grid/opacity state read by particle_advance (gridmod.f, transportmod.f). */
+typedef struct slg_transport_in {
+  const double* tempinv;   /* grd_tempinv (ncell) */
+  const double* sig;       /* grd_sig (ncell) */
+  const double* capgrey;   /* grd_capgrey (ncell) */
+  const double* emitprob;  /* grd_emitprob (nep, ncell) */
+  const double* opaclump;  /* grd_opaclump (11, ncell) */
+  const float* cap;        /* grd_cap (ng, ncell) */
+  double tauddmc;          /* trn_tauddmc */
+  double taulump;          /* trn_taulump */
+  int32_t puretran, noampfact, errorfatal, thm_aniso, dogrdtally;
+  int32_t precision;       /* 0: FP64 (reference arithmetic); 1: mixed FP32/FP64 */
+  int64_t max_steps;       /* per-particle step guard; 0 = none */
+} slg_transport_in;
+
+/* Tallies written by particle_advance.  tally/eamp/methodswap (ncell),
+ * jrad (ng, ncell) are overwritten (particle_advance.f90:65-72); the tot_*
+ * fields accumulate into the caller's values (totalsmod.f). */
+typedef struct slg_transport_out {
+  double* tally;
+  double* jrad;
+  double* eamp;
+  int32_t* methodswap;
+  double tot_evelo, tot_eout, tot_sflux;
+  int64_t npckt, nflux, nstepimc, nstepddmc, nmethodswap, nstepmax;
+  int64_t ndist[11];       /* ndist(-3:7) */
+  int64_t nposwarn;        /* ierr = -99 position warnings */
+  int32_t ierr;            /* first fatal transport error (lowest particle index) */
+  int32_t ierr_part;       /* its 1-based particle index */
+} slg_transport_out;
+
+/* particle_advance (particle_advance.f90:4-327) with transport11 / diffusion11
+ * (TRANSPORT1/transport11.f90, TRANSPORT1/diffusion11.f90).  Random numbers:
+ * one Philox4x32-10 stream per particle keyed by `seed` (replaces the
+ * per-thread mzran streams of randommod.f).  prt (npart) and isvacant (npart,
+ * logical as int32) are updated in place: dead particles become vacant,
+ * escaped ones keep x = huge (:283-288). */
+int slg_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packet* prt,
+                         int32_t* isvacant, int64_t npart, uint64_t seed,
+                         slg_transport_out* out);
+
+/* Optional per-particle event trace of the next particle_advance call on this
+ * context: an FNV-1a hash of (idist, itype, ic, ig, stat) after every event and
+ * the step count, for parity tests.  Host arrays of npart entries; pass NULLs
+ * to disable. */
+int slg_set_trace(slg_ctx* ctx, uint64_t* trace_hash, int32_t* trace_nstep);
+
+/* fluxtally (fluxtally.f:3-61) on flux grid flx_wl (flx_ng+1) with one polar
+ * and one azimuthal bin (in_flx_ndim = ng,1,1): luminos, lumdev (flx_ng) and
+ * lumnum (flx_ng); tallied slots become vacant. */
+int slg_fluxtally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, int32_t* isvacant,
+                  int32_t flx_ng, const double* flx_wl, double* luminos, double* lumdev,
+                  int32_t* lumnum);
+
+/* sourcetally (sourcetally.f:3-48): src_energy, src_number (ncell, ng). */
+int slg_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, const int32_t* isvacant,
+                    double* src_energy, int32_t* src_number);
+
+/* ------------------------------------------------------------------ device-pointer forms */
+/* Same semantics as above; every array argument is a device pointer, work is
+ * queued on the context's stream, and the call returns after queueing (the
+ * transport counters in *out are only valid after slg_sync()). */
+int slg_dev_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_flags* flags,
+                             double* gas_sig, float* gas_cap, float* gas_emiss, double* cap64);
+int slg_dev_opacity_means(slg_ctx* ctx, const double* temp, const double* sig,
+                          const float* gas_cap, double* capgrey, double* capross);
+int slg_dev_leakage_opacity11(slg_ctx* ctx, const double* tempinv, const double* sig,
+                              const float* cap, const float* capemit, double tauddmc,
+                              double taulump, double* opaclump);
+int slg_dev_emission_probability(slg_ctx* ctx, const double* tempinv, const float* cap,
+                                 const double* capgrey, double* emitprob);
+int slg_dev_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packet* prt,
+                             int32_t* isvacant, int64_t npart, uint64_t seed,
+                             slg_transport_out* out);
+int slg_dev_fluxtally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, int32_t* isvacant,
+                      int32_t flx_ng, const double* flx_wl, double* luminos, double* lumdev,
+                      int32_t* lumnum);
+int slg_dev_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt,
+                        const int32_t* isvacant, double* src_energy, int32_t* src_number);
+/* Wait for the context's stream; returns a pending error if any. */
+int slg_sync(slg_ctx* ctx);
+/* The context's cudaStream_t, as an opaque handle. */
+void* slg_stream(slg_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

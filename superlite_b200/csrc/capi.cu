@@ -1,0 +1,518 @@
+// capi.cu -- extern "C" entry points of libslg (declared in include/slg.h).
+//
+// Host-pointer entry points stage their arrays in context-owned device
+// buffers, call the device-pointer form on the context's stream, copy the
+// outputs back and synchronise.  Device-pointer entry points only queue work.
+#include <cuda_runtime.h>
+#include <cstdarg>
+#include <cstring>
+#include <algorithm>
+#include "slg.h"
+#include "slg_internal.h"
+
+namespace slg {
+
+int set_error(slg_ctx* ctx, int code, const char* fmt, ...) {
+  if (!ctx) return code;
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  ctx->err = buf;
+  return code;
+}
+
+int cuda_check(slg_ctx* ctx, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return SLG_OK;
+  return set_error(ctx, SLG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+void* scratch(slg_ctx* ctx, int slot, size_t bytes) {
+  DevBuf& b = ctx->scratch[slot];
+  if (bytes == 0) bytes = 16;
+  if (b.bytes >= bytes) return b.p;
+  if (b.p) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    if (slot >= 12 && slot <= 20) ctx->tables.nx = ctx->tables.ng = 0;
+  }
+  const size_t alloc = bytes + bytes / 8;  // headroom for small growth
+  if (cudaMalloc(&b.p, alloc) != cudaSuccess) {
+    cudaGetLastError();
+    set_error(ctx, SLG_ERR_OOM, "cudaMalloc of %zu bytes failed", alloc);
+    return nullptr;
+  }
+  b.bytes = alloc;
+  return b.p;
+}
+
+int opacity_flags(slg_ctx* ctx, int32_t* sanity, int32_t* binning);
+int sourcetally_error(slg_ctx* ctx, int* err);
+
+}  // namespace slg
+
+using namespace slg;
+
+namespace {
+
+// Staging slots used by the host-pointer entry points.
+enum {
+  H_A = 32, H_B, H_C, H_D, H_E, H_F, H_G, H_H, H_I, H_J, H_K, H_L, H_M, H_N, H_O, H_P
+};
+
+template <class T>
+T* up(slg_ctx* ctx, int slot, const T* h, size_t n, int* rc) {
+  if (*rc) return nullptr;
+  if (!h) return nullptr;
+  T* d = (T*)scratch(ctx, slot, sizeof(T) * n);
+  if (!d) { *rc = SLG_ERR_OOM; return nullptr; }
+  *rc = cuda_check(ctx, cudaMemcpyAsync(d, h, sizeof(T) * n, cudaMemcpyHostToDevice, ctx->stream), "upload");
+  return d;
+}
+template <class T>
+T* out_buf(slg_ctx* ctx, int slot, size_t n, int* rc) {
+  if (*rc) return nullptr;
+  T* d = (T*)scratch(ctx, slot, sizeof(T) * n);
+  if (!d) *rc = SLG_ERR_OOM;
+  return d;
+}
+template <class T>
+void down(slg_ctx* ctx, T* h, const T* d, size_t n, int* rc) {
+  if (*rc || !h || !d) return;
+  *rc = cuda_check(ctx, cudaMemcpyAsync(h, d, sizeof(T) * n, cudaMemcpyDeviceToHost, ctx->stream), "download");
+}
+int finish(slg_ctx* ctx, int rc) {
+  const int rs = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "stream sync");
+  return rc ? rc : rs;
+}
+bool need_grid(slg_ctx* ctx) { return ctx->nx > 0 && ctx->ng > 0; }
+
+void free_dev(void* p) {
+  if (p) cudaFree(p);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* slg_version(void) { return "superlite_b200 libslg sm_100a " __DATE__; }
+
+slg_ctx* slg_create(int device) {
+  if (cudaSetDevice(device) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+  slg_ctx* ctx = new slg_ctx();
+  ctx->device = device;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete ctx;
+    return nullptr;
+  }
+  cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaMalloc(&ctx->d_acc, sizeof(TransportAcc)) != cudaSuccess ||
+      cudaMallocHost(&ctx->h_acc, sizeof(TransportAcc)) != cudaSuccess) {
+    cudaGetLastError();
+    slg_destroy(ctx);
+    return nullptr;
+  }
+  std::memset(ctx->h_acc, 0, sizeof(TransportAcc));
+  return ctx;
+}
+
+void slg_destroy(slg_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& b : ctx->scratch) free_dev(b.p);
+  free_dev(ctx->d_wl); free_dev(ctx->d_wlinv);
+  free_dev(ctx->d_xarr); free_dev(ctx->d_vxarr); free_dev(ctx->d_vol); free_dev(ctx->d_divv);
+  free_dev(ctx->d_ion_ni); free_dev(ctx->d_bb); free_dev(ctx->d_ph1); free_dev(ctx->d_ph2);
+  free_dev(ctx->d_gff); free_dev(ctx->d_acc);
+  if (ctx->h_acc) cudaFreeHost(ctx->h_acc);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* slg_last_error(const slg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void* slg_stream(slg_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int slg_sync(slg_ctx* ctx) {
+  if (!ctx) return SLG_ERR_ARG;
+  int rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "stream sync");
+  if (!rc && ctx->pending_out) {
+    slg_transport_out* o = ctx->pending_out;
+    ctx->pending_out = nullptr;
+    rc = finish_particle_advance(ctx, nullptr, o);
+  }
+  return rc;
+}
+
+int slg_set_groups(slg_ctx* ctx, int32_t ng, const double* grp_wl) {
+  if (!ctx || ng < 1 || !grp_wl) return set_error(ctx, SLG_ERR_ARG, "slg_set_groups: bad arguments");
+  for (int k = 0; k < ng; ++k)
+    if (!(grp_wl[k + 1] > grp_wl[k]) || !(grp_wl[k] > 0.0))
+      return set_error(ctx, SLG_ERR_ARG, "slg_set_groups: wavelength grid not increasing at %d", k);
+  cudaSetDevice(ctx->device);
+  free_dev(ctx->d_wl);
+  free_dev(ctx->d_wlinv);
+  ctx->d_wl = ctx->d_wlinv = nullptr;
+  std::vector<double> inv(ng + 1);
+  for (int k = 0; k <= ng; ++k) inv[k] = 1.0 / grp_wl[k];  // groupmod.f:51
+  int rc = cuda_check(ctx, cudaMalloc(&ctx->d_wl, sizeof(double) * (ng + 1)), "alloc wl");
+  if (!rc) rc = cuda_check(ctx, cudaMalloc(&ctx->d_wlinv, sizeof(double) * (ng + 1)), "alloc wlinv");
+  if (!rc) rc = cuda_check(ctx, cudaMemcpy(ctx->d_wl, grp_wl, sizeof(double) * (ng + 1), cudaMemcpyHostToDevice), "wl");
+  if (!rc) rc = cuda_check(ctx, cudaMemcpy(ctx->d_wlinv, inv.data(), sizeof(double) * (ng + 1), cudaMemcpyHostToDevice), "wlinv");
+  if (rc) return rc;
+  ctx->ng = ng;
+  ctx->h_wl.assign(grp_wl, grp_wl + ng + 1);
+  ctx->nep = (int)lround(std::sqrt((double)ng));                 // gridmod.f:121
+  ctx->nepg = (int)std::ceil(ng / (ctx->nep + 1.0));              // gridmod.f:122
+  ctx->tables.nx = ctx->tables.ng = 0;
+  return SLG_OK;
+}
+
+int slg_set_grid(slg_ctx* ctx, int32_t nx, const double* xarr, const double* vxarr, const double* vol,
+                 const double* divv) {
+  if (!ctx || nx < 1 || !xarr || !vxarr || !vol || !divv)
+    return set_error(ctx, SLG_ERR_ARG, "slg_set_grid: bad arguments");
+  for (int k = 0; k < nx; ++k)
+    if (!(xarr[k + 1] > xarr[k])) return set_error(ctx, SLG_ERR_ARG, "slg_set_grid: xarr not increasing at %d", k);
+  cudaSetDevice(ctx->device);
+  if (nx != ctx->nx) {
+    free_dev(ctx->d_xarr); free_dev(ctx->d_vxarr); free_dev(ctx->d_vol); free_dev(ctx->d_divv);
+    ctx->d_xarr = ctx->d_vxarr = ctx->d_vol = ctx->d_divv = nullptr;
+    int rc = cuda_check(ctx, cudaMalloc(&ctx->d_xarr, sizeof(double) * (nx + 1)), "alloc xarr");
+    if (!rc) rc = cuda_check(ctx, cudaMalloc(&ctx->d_vxarr, sizeof(double) * (nx + 1)), "alloc vxarr");
+    if (!rc) rc = cuda_check(ctx, cudaMalloc(&ctx->d_vol, sizeof(double) * nx), "alloc vol");
+    if (!rc) rc = cuda_check(ctx, cudaMalloc(&ctx->d_divv, sizeof(double) * nx), "alloc divv");
+    if (rc) return rc;
+  }
+  int rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_xarr, xarr, sizeof(double) * (nx + 1), cudaMemcpyHostToDevice, ctx->stream), "xarr");
+  if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_vxarr, vxarr, sizeof(double) * (nx + 1), cudaMemcpyHostToDevice, ctx->stream), "vxarr");
+  if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_vol, vol, sizeof(double) * nx, cudaMemcpyHostToDevice, ctx->stream), "vol");
+  if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_divv, divv, sizeof(double) * nx, cudaMemcpyHostToDevice, ctx->stream), "divv");
+  if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "grid sync");
+  if (rc) return rc;
+  ctx->nx = nx;
+  ctx->h_xarr.assign(xarr, xarr + nx + 1);
+  ctx->tables.nx = ctx->tables.ng = 0;
+  return SLG_OK;
+}
+
+int slg_set_atomic_data(slg_ctx* ctx, int32_t nelem, int32_t nstage, const int32_t* ion_ni, int64_t nline,
+                        const slg_bbxs* bb_xs, const float* bf_ph1, const float* bf_ph2, const double* ff_gff) {
+  if (!ctx || nelem < 1 || nelem > 30 || nstage < 1 || !ion_ni || nline < 0 || (nline > 0 && !bb_xs))
+    return set_error(ctx, SLG_ERR_ARG, "slg_set_atomic_data: bad arguments");
+  if (nline > 0x7fffffffLL) return set_error(ctx, SLG_ERR_ARG, "slg_set_atomic_data: too many lines");
+  for (int64_t l = 0; l + 1 < nline; ++l)
+    if (!(bb_xs[l].wl0 <= bb_xs[l + 1].wl0))
+      return set_error(ctx, SLG_ERR_UNSORTED, "slg_set_atomic_data: lines not sorted by wl0 at %lld", (long long)l);
+  for (int64_t l = 0; l < nline; ++l)
+    if (bb_xs[l].iz < 1 || bb_xs[l].iz > nelem || bb_xs[l].ii < 1 || bb_xs[l].ii > nstage)
+      return set_error(ctx, SLG_ERR_ARG, "slg_set_atomic_data: line %lld has ion (%d,%d) outside the tables",
+                       (long long)l, bb_xs[l].iz, bb_xs[l].ii);
+  cudaSetDevice(ctx->device);
+  free_dev(ctx->d_ion_ni); free_dev(ctx->d_bb); free_dev(ctx->d_ph1); free_dev(ctx->d_ph2); free_dev(ctx->d_gff);
+  ctx->d_ion_ni = nullptr; ctx->d_bb = nullptr; ctx->d_ph1 = ctx->d_ph2 = nullptr; ctx->d_gff = nullptr;
+  int rc = cuda_check(ctx, cudaMalloc(&ctx->d_ion_ni, sizeof(int32_t) * nelem), "alloc ion_ni");
+  if (!rc) rc = cuda_check(ctx, cudaMemcpy(ctx->d_ion_ni, ion_ni, sizeof(int32_t) * nelem, cudaMemcpyHostToDevice), "ion_ni");
+  if (!rc && nline > 0) {
+    rc = cuda_check(ctx, cudaMalloc(&ctx->d_bb, sizeof(slg_bbxs) * nline), "alloc bb");
+    if (!rc) rc = cuda_check(ctx, cudaMemcpy(ctx->d_bb, bb_xs, sizeof(slg_bbxs) * nline, cudaMemcpyHostToDevice), "bb");
+  }
+  if (!rc && bf_ph1 && bf_ph2) {
+    rc = cuda_check(ctx, cudaMalloc(&ctx->d_ph1, sizeof(float) * 6 * 7 * 30 * 30), "alloc ph1");
+    if (!rc) rc = cuda_check(ctx, cudaMalloc(&ctx->d_ph2, sizeof(float) * 7 * 30 * 30), "alloc ph2");
+    if (!rc) rc = cuda_check(ctx, cudaMemcpy(ctx->d_ph1, bf_ph1, sizeof(float) * 6 * 7 * 30 * 30, cudaMemcpyHostToDevice), "ph1");
+    if (!rc) rc = cuda_check(ctx, cudaMemcpy(ctx->d_ph2, bf_ph2, sizeof(float) * 7 * 30 * 30, cudaMemcpyHostToDevice), "ph2");
+  }
+  if (!rc && ff_gff) {
+    rc = cuda_check(ctx, cudaMalloc(&ctx->d_gff, sizeof(double) * 81 * 41), "alloc gff");
+    if (!rc) rc = cuda_check(ctx, cudaMemcpy(ctx->d_gff, ff_gff, sizeof(double) * 81 * 41, cudaMemcpyHostToDevice), "gff");
+  }
+  if (rc) return rc;
+  ctx->nelem = nelem;
+  ctx->nstage = nstage;
+  ctx->nline = nline;
+  ctx->h_ion_ni.assign(ion_ni, ion_ni + nelem);
+  return SLG_OK;
+}
+
+int slg_set_trace(slg_ctx* ctx, uint64_t* trace_hash, int32_t* trace_nstep) {
+  if (!ctx) return SLG_ERR_ARG;
+  ctx->trace_hash = trace_hash;
+  ctx->trace_nstep = trace_nstep;
+  return SLG_OK;
+}
+
+// ------------------------------------------------------------------ device forms
+int slg_dev_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_flags* flags, double* gas_sig,
+                             float* gas_cap, float* gas_emiss, double* cap64) {
+  if (!ctx || !gas || !flags || !gas_sig || !gas_cap || !gas_emiss) return set_error(ctx, SLG_ERR_ARG, "null argument");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  cudaSetDevice(ctx->device);
+  return launch_physical_opacity(ctx, gas, flags, gas_sig, gas_cap, gas_emiss, cap64);
+}
+
+int slg_dev_opacity_means(slg_ctx* ctx, const double* temp, const double* sig, const float* gas_cap, double* capgrey,
+                          double* capross) {
+  if (!ctx || !temp || !gas_cap || !capgrey) return set_error(ctx, SLG_ERR_ARG, "null argument");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  cudaSetDevice(ctx->device);
+  return launch_opacity_means(ctx, temp, sig, gas_cap, capgrey, capross);
+}
+
+int slg_dev_leakage_opacity11(slg_ctx* ctx, const double* tempinv, const double* sig, const float* cap,
+                              const float* capemit, double tauddmc, double taulump, double* opaclump) {
+  if (!ctx || !tempinv || !sig || !cap || !opaclump) return set_error(ctx, SLG_ERR_ARG, "null argument");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  cudaSetDevice(ctx->device);
+  return launch_leakage(ctx, tempinv, sig, cap, capemit, tauddmc, taulump, opaclump);
+}
+
+int slg_dev_emission_probability(slg_ctx* ctx, const double* tempinv, const float* cap, const double* capgrey,
+                                 double* emitprob) {
+  if (!ctx || !tempinv || !cap || !capgrey || !emitprob) return set_error(ctx, SLG_ERR_ARG, "null argument");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  cudaSetDevice(ctx->device);
+  return launch_emitprob(ctx, tempinv, cap, capgrey, emitprob);
+}
+
+int slg_dev_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packet* prt, int32_t* isvacant,
+                             int64_t npart, uint64_t seed, slg_transport_out* out) {
+  if (!ctx || !in || !out || (npart > 0 && (!prt || !isvacant)) || npart < 0)
+    return set_error(ctx, SLG_ERR_ARG, "null argument");
+  if (!in->tempinv || !in->sig || !in->capgrey || !in->emitprob || !in->opaclump || !in->cap)
+    return set_error(ctx, SLG_ERR_ARG, "slg_transport_in has a null array");
+  if (!out->tally || !out->jrad || !out->eamp || (in->dogrdtally && !out->methodswap))
+    return set_error(ctx, SLG_ERR_ARG, "slg_transport_out has a null array");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  if (ctx->nx < 2) return set_error(ctx, SLG_ERR_ARG, "transport needs at least 2 shells");
+  if (in->precision != 0) return set_error(ctx, SLG_ERR_NOT_BUILT, "precision %d not available", in->precision);
+  cudaSetDevice(ctx->device);
+  const int rc = launch_particle_advance(ctx, in, prt, isvacant, npart, seed, out, nullptr, nullptr);
+  ctx->pending_out = rc ? nullptr : out;
+  return rc;
+}
+
+int slg_dev_fluxtally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, int32_t* isvacant, int32_t flx_ng,
+                      const double* flx_wl, double* luminos, double* lumdev, int32_t* lumnum) {
+  if (!ctx || flx_ng < 1 || !flx_wl || !luminos || !lumdev || !lumnum || npart < 0)
+    return set_error(ctx, SLG_ERR_ARG, "bad argument");
+  cudaSetDevice(ctx->device);
+  return launch_fluxtally(ctx, npart, prt, isvacant, flx_ng, flx_wl, luminos, lumdev, lumnum);
+}
+
+int slg_dev_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, const int32_t* isvacant,
+                        double* src_energy, int32_t* src_number) {
+  if (!ctx || !src_energy || !src_number || npart < 0) return set_error(ctx, SLG_ERR_ARG, "bad argument");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  cudaSetDevice(ctx->device);
+  return launch_sourcetally(ctx, npart, prt, isvacant, src_energy, src_number);
+}
+
+// ------------------------------------------------------------------ host forms
+int slg_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_flags* flags, double* gas_sig,
+                         float* gas_cap, float* gas_emiss, double* cap64, int32_t* sanity) {
+  if (!ctx || !gas || !flags || !gas_sig || !gas_cap || !gas_emiss) return set_error(ctx, SLG_ERR_ARG, "null argument");
+  if (!need_grid(ctx) || ctx->nelem < 1) return set_error(ctx, SLG_ERR_STATE, "groups/grid/atomic data not set");
+  cudaSetDevice(ctx->device);
+  const size_t nc = ctx->nx, ng = ctx->ng, ns = (size_t)ctx->nstage * ctx->nelem;
+  int rc = 0;
+  slg_gas d;
+  d.temp = up(ctx, H_A, gas->temp, nc, &rc);
+  d.natom = up(ctx, H_B, gas->natom, nc, &rc);
+  d.nelec = up(ctx, H_C, gas->nelec, nc, &rc);
+  d.vol = up(ctx, H_D, gas->vol, nc, &rc);
+  d.mass = up(ctx, H_E, gas->mass, nc, &rc);
+  d.natomfr = up(ctx, H_F, gas->natomfr, nc * (ctx->nelem + 1), &rc);
+  d.oc = up(ctx, H_G, gas->oc, nc * ns, &rc);
+  d.ginv = up(ctx, H_H, gas->ginv, nc * ns, &rc);
+  double* dsig = out_buf<double>(ctx, H_I, nc, &rc);
+  float* dcap = out_buf<float>(ctx, H_J, nc * ng, &rc);
+  float* dem = out_buf<float>(ctx, H_K, nc * ng, &rc);
+  double* dc64 = cap64 ? out_buf<double>(ctx, H_L, nc * ng, &rc) : nullptr;
+  if (!rc && (!d.temp || !d.natom || !d.nelec || !d.vol || !d.mass || !d.natomfr || !d.oc || !d.ginv))
+    rc = set_error(ctx, SLG_ERR_ARG, "slg_gas has a null array");
+  if (!rc) rc = launch_physical_opacity(ctx, &d, flags, dsig, dcap, dem, dc64);
+  down(ctx, gas_sig, dsig, nc, &rc);
+  down(ctx, gas_cap, dcap, nc * ng, &rc);
+  down(ctx, gas_emiss, dem, nc * ng, &rc);
+  if (cap64) down(ctx, cap64, dc64, nc * ng, &rc);
+  rc = finish(ctx, rc);
+  if (!rc) {
+    int32_t s = 0, b = 0;
+    rc = opacity_flags(ctx, &s, &b);
+    if (!rc && (b & 1)) rc = set_error(ctx, SLG_ERR_UNSORTED, "bb line list not sorted by wl0");
+    if (!rc && (b & 2)) rc = set_error(ctx, SLG_ERR_CUDA, "line binning: shared-memory staging timed out");
+    if (sanity) *sanity = s;
+  }
+  return rc;
+}
+
+int slg_analytic_opacity(slg_ctx* ctx, const double* temp, const double* rho, int32_t kind, double capcoef,
+                         double captpwr, double caprpwr, double sigcoef, double sigtpwr, double sigrpwr,
+                         double ldisp1, double ldisp2, double* gas_sig, float* gas_cap) {
+  if (!ctx || !temp || !rho || !gas_sig || !gas_cap || kind < 1 || kind > 3)
+    return set_error(ctx, SLG_ERR_ARG, "bad argument");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  cudaSetDevice(ctx->device);
+  const size_t nc = ctx->nx, ng = ctx->ng;
+  int rc = 0;
+  const double* dt = up(ctx, H_A, temp, nc, &rc);
+  const double* dr = up(ctx, H_B, rho, nc, &rc);
+  double* ds = out_buf<double>(ctx, H_I, nc, &rc);
+  float* dc = out_buf<float>(ctx, H_J, nc * ng, &rc);
+  const double c[8] = {capcoef, captpwr, caprpwr, sigcoef, sigtpwr, sigrpwr, ldisp1, ldisp2};
+  if (!rc) rc = launch_analytic_opacity(ctx, dt, dr, kind, c, ds, dc);
+  down(ctx, gas_sig, ds, nc, &rc);
+  down(ctx, gas_cap, dc, nc * ng, &rc);
+  return finish(ctx, rc);
+}
+
+int slg_opacity_means(slg_ctx* ctx, const double* temp, const double* sig, const float* gas_cap, double* capgrey,
+                      double* capross) {
+  if (!ctx || !temp || !gas_cap || !capgrey) return set_error(ctx, SLG_ERR_ARG, "null argument");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  cudaSetDevice(ctx->device);
+  const size_t nc = ctx->nx, ng = ctx->ng;
+  int rc = 0;
+  const double* dt = up(ctx, H_A, temp, nc, &rc);
+  const double* ds = up(ctx, H_B, sig, nc, &rc);
+  const float* dc = up(ctx, H_C, gas_cap, nc * ng, &rc);
+  double* dg = out_buf<double>(ctx, H_I, nc, &rc);
+  double* dr = capross ? out_buf<double>(ctx, H_K, nc, &rc) : nullptr;
+  if (!rc) rc = launch_opacity_means(ctx, dt, ds, dc, dg, dr);
+  down(ctx, capgrey, dg, nc, &rc);
+  if (capross) down(ctx, capross, dr, nc, &rc);
+  return finish(ctx, rc);
+}
+
+int slg_leakage_opacity11(slg_ctx* ctx, const double* tempinv, const double* sig, const float* cap,
+                          const float* capemit, double tauddmc, double taulump, double* opaclump) {
+  if (!ctx || !tempinv || !sig || !cap || !opaclump) return set_error(ctx, SLG_ERR_ARG, "null argument");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  cudaSetDevice(ctx->device);
+  const size_t nc = ctx->nx, ng = ctx->ng;
+  int rc = 0;
+  const double* dt = up(ctx, H_A, tempinv, nc, &rc);
+  const double* ds = up(ctx, H_B, sig, nc, &rc);
+  const float* dc = up(ctx, H_C, cap, nc * ng, &rc);
+  const float* de = capemit ? up(ctx, H_D, capemit, nc * ng, &rc) : nullptr;
+  double* dol = out_buf<double>(ctx, H_I, nc * 11, &rc);
+  if (!rc) rc = launch_leakage(ctx, dt, ds, dc, de, tauddmc, taulump, dol);
+  down(ctx, opaclump, dol, nc * 11, &rc);
+  return finish(ctx, rc);
+}
+
+int slg_emission_probability(slg_ctx* ctx, const double* tempinv, const float* cap, const double* capgrey,
+                             double* emitprob) {
+  if (!ctx || !tempinv || !cap || !capgrey || !emitprob) return set_error(ctx, SLG_ERR_ARG, "null argument");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  cudaSetDevice(ctx->device);
+  const size_t nc = ctx->nx, ng = ctx->ng;
+  int rc = 0;
+  const double* dt = up(ctx, H_A, tempinv, nc, &rc);
+  const float* dc = up(ctx, H_C, cap, nc * ng, &rc);
+  const double* dg = up(ctx, H_B, capgrey, nc, &rc);
+  double* dep = out_buf<double>(ctx, H_I, nc * ctx->nep, &rc);
+  if (!rc) rc = launch_emitprob(ctx, dt, dc, dg, dep);
+  down(ctx, emitprob, dep, nc * ctx->nep, &rc);
+  return finish(ctx, rc);
+}
+
+int slg_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packet* prt, int32_t* isvacant, int64_t npart,
+                         uint64_t seed, slg_transport_out* out) {
+  if (!ctx || !in || !out || (npart > 0 && (!prt || !isvacant)) || npart < 0)
+    return set_error(ctx, SLG_ERR_ARG, "null argument");
+  if (!in->tempinv || !in->sig || !in->capgrey || !in->emitprob || !in->opaclump || !in->cap)
+    return set_error(ctx, SLG_ERR_ARG, "slg_transport_in has a null array");
+  if (!out->tally || !out->jrad || !out->eamp || (in->dogrdtally && !out->methodswap))
+    return set_error(ctx, SLG_ERR_ARG, "slg_transport_out has a null array");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  if (ctx->nx < 2) return set_error(ctx, SLG_ERR_ARG, "transport needs at least 2 shells");
+  if (in->precision != 0) return set_error(ctx, SLG_ERR_NOT_BUILT, "precision %d not available", in->precision);
+  cudaSetDevice(ctx->device);
+  const size_t nc = ctx->nx, ng = ctx->ng, np = (size_t)npart;
+  int rc = 0;
+  slg_transport_in d = *in;
+  d.tempinv = up(ctx, H_A, in->tempinv, nc, &rc);
+  d.sig = up(ctx, H_B, in->sig, nc, &rc);
+  d.capgrey = up(ctx, H_C, in->capgrey, nc, &rc);
+  d.emitprob = up(ctx, H_D, in->emitprob, nc * ctx->nep, &rc);
+  d.opaclump = up(ctx, H_E, in->opaclump, nc * 11, &rc);
+  d.cap = up(ctx, H_F, in->cap, nc * ng, &rc);
+  slg_packet* dp = up(ctx, H_G, prt, np, &rc);
+  int32_t* dv = up(ctx, H_H, isvacant, np, &rc);
+  slg_transport_out o = *out;
+  o.tally = out_buf<double>(ctx, H_I, nc, &rc);
+  o.jrad = out_buf<double>(ctx, H_J, nc * ng, &rc);
+  o.eamp = out_buf<double>(ctx, H_K, nc, &rc);
+  o.methodswap = out_buf<int32_t>(ctx, H_L, nc, &rc);
+  uint64_t* dth = ctx->trace_hash ? out_buf<uint64_t>(ctx, H_M, np, &rc) : nullptr;
+  int32_t* dtn = ctx->trace_nstep ? out_buf<int32_t>(ctx, H_N, np, &rc) : nullptr;
+  if (!rc && dth) cudaMemsetAsync(dth, 0, sizeof(uint64_t) * np, ctx->stream);
+  if (!rc && dtn) cudaMemsetAsync(dtn, 0, sizeof(int32_t) * np, ctx->stream);
+  if (!rc) rc = launch_particle_advance(ctx, &d, dp, dv, npart, seed, &o, dth, dtn);
+  down(ctx, prt, dp, np, &rc);
+  down(ctx, isvacant, dv, np, &rc);
+  down(ctx, out->tally, o.tally, nc, &rc);
+  down(ctx, out->jrad, o.jrad, nc * ng, &rc);
+  down(ctx, out->eamp, o.eamp, nc, &rc);
+  if (in->dogrdtally && out->methodswap) down(ctx, out->methodswap, o.methodswap, nc, &rc);
+  if (dth) down(ctx, ctx->trace_hash, dth, np, &rc);
+  if (dtn) down(ctx, ctx->trace_nstep, dtn, np, &rc);
+  rc = finish(ctx, rc);
+  if (rc) return rc;
+  return finish_particle_advance(ctx, in, out);
+}
+
+int slg_fluxtally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, int32_t* isvacant, int32_t flx_ng,
+                  const double* flx_wl, double* luminos, double* lumdev, int32_t* lumnum) {
+  if (!ctx || flx_ng < 1 || !flx_wl || !luminos || !lumdev || !lumnum || npart < 0 || (npart > 0 && (!prt || !isvacant)))
+    return set_error(ctx, SLG_ERR_ARG, "bad argument");
+  cudaSetDevice(ctx->device);
+  const size_t np = (size_t)npart;
+  int rc = 0;
+  const slg_packet* dp = up(ctx, H_G, prt, np, &rc);
+  int32_t* dv = up(ctx, H_H, isvacant, np, &rc);
+  const double* dw = up(ctx, H_A, flx_wl, (size_t)flx_ng + 1, &rc);
+  double* dl = out_buf<double>(ctx, H_I, flx_ng, &rc);
+  double* dd = out_buf<double>(ctx, H_J, flx_ng, &rc);
+  int32_t* dn = out_buf<int32_t>(ctx, H_K, flx_ng, &rc);
+  if (!rc) rc = launch_fluxtally(ctx, npart, dp, dv, flx_ng, dw, dl, dd, dn);
+  down(ctx, isvacant, dv, np, &rc);
+  down(ctx, luminos, dl, flx_ng, &rc);
+  down(ctx, lumdev, dd, flx_ng, &rc);
+  down(ctx, lumnum, dn, flx_ng, &rc);
+  return finish(ctx, rc);
+}
+
+int slg_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, const int32_t* isvacant, double* src_energy,
+                    int32_t* src_number) {
+  if (!ctx || !src_energy || !src_number || npart < 0 || (npart > 0 && (!prt || !isvacant)))
+    return set_error(ctx, SLG_ERR_ARG, "bad argument");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  cudaSetDevice(ctx->device);
+  const size_t np = (size_t)npart, n = (size_t)ctx->nx * ctx->ng;
+  int rc = 0;
+  const slg_packet* dp = up(ctx, H_G, prt, np, &rc);
+  const int32_t* dv = up(ctx, H_H, isvacant, np, &rc);
+  double* de = out_buf<double>(ctx, H_I, n, &rc);
+  int32_t* dn = out_buf<int32_t>(ctx, H_J, n, &rc);
+  if (!rc) rc = launch_sourcetally(ctx, npart, dp, dv, de, dn);
+  down(ctx, src_energy, de, n, &rc);
+  down(ctx, src_number, dn, n, &rc);
+  rc = finish(ctx, rc);
+  if (!rc) {
+    int e = 0;
+    rc = sourcetally_error(ctx, &e);
+    if (!rc && (e & 1)) rc = set_error(ctx, SLG_ERR_ARG, "sourcetally: ic outside range");
+    if (!rc && (e & 2)) rc = set_error(ctx, SLG_ERR_ARG, "sourcetally: ig outside range");
+  }
+  return rc;
+}
+
+}  // extern "C"

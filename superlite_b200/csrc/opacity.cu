@@ -1,0 +1,603 @@
+// opacity.cu -- physical LTE opacity (bound-bound expansion opacity binned into
+// groups, Verner bound-free, Sutherland free-free), analytic opacity and the
+// Planck / Rosseland means, for sm_100a.
+//
+// Reference: GAS/physical_opacity.f:3-357, bfxsmod.f:184-272,
+// GAS/analytic_opacity.f90:3-77, GAS/opacity_planckmean.f:17-24,
+// GAS/opacity_rossmean.f:17-21.
+//
+// Design (one B200):
+//  * bin_lines: lines (sorted by wl0) are binned to sub-groups by a
+//    warp-cooperative kernel: the sub-group edges are staged into shared memory
+//    with one TMA bulk copy (cp.async.bulk + mbarrier), each thread binary-
+//    searches its lines there, and a shared-memory histogram of lines per
+//    sub-group is flushed to global counts; a scan turns counts into ranges.
+//  * opacity_fwd: one warp per (group, 32 shells).  Every lane walks the
+//    lines of its group in file order (warp-uniform broadcast reads) and
+//    accumulates bb, then bf (ions in the reference's iz,ii order), then ff
+//    (elements in order) into one register, i.e. exactly the reference's
+//    per-(cell,sub-group) summation order.  Sub-groups are collapsed in
+//    registers, then cap and emissivity are written through a shared-memory
+//    tile so each shell's 8 groups leave as one 32-byte sector.
+//  * FP64 throughout, no FMA contraction (-fmad=false), so sums round like the
+//    single-threaded Fortran; only exp/log10/pow may differ in the last ulp.
+#include <cuda_runtime.h>
+#include <cfloat>
+#include "slg_device.cuh"
+#include "slg_internal.h"
+
+namespace slg {
+
+namespace {
+
+constexpr int OPAC_GT = 8;   // groups per block (one warp each)
+constexpr int OPAC_CT = 32;  // shells per block (one per lane)
+
+// ------------------------------------------------------------ TMA bulk helpers
+__device__ inline uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ inline void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ inline void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ inline void tma_bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// Bounded wait on phase 0 of the barrier.  Returns false on time-out.
+__device__ inline bool mbar_wait(uint64_t* bar, uint32_t parity, long max_polls) {
+  for (long it = 0; it < max_polls; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (it > 64) __nanosleep(64);
+  }
+  return false;
+}
+
+// ------------------------------------------------------------ line binning
+// counts[igs] (igs = 0..ngsub+1) = number of lines whose sub-group pointer is
+// igs (physical_opacity.f:117-125): igs = #{k : wlsub(k) <= wl0}.
+__global__ void __launch_bounds__(256) bin_lines_kernel(const slg_bbxs* __restrict__ bb, int64_t nline,
+                                                        const double* __restrict__ wlsub_pad,
+                                                        int nedge, int nedge_pad,
+                                                        unsigned int* __restrict__ counts,
+                                                        int* __restrict__ flags) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+  double* edges = reinterpret_cast<double*>(smem + 16);
+  unsigned int* hist = reinterpret_cast<unsigned int*>(smem + 16 + sizeof(double) * nedge_pad);
+  const int nbins = nedge + 1;  // 0..ngsub+1
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_expect_tx(bar, (uint32_t)(sizeof(double) * nedge_pad));
+    tma_bulk_g2s(edges, wlsub_pad, (uint32_t)(sizeof(double) * nedge_pad), bar);
+  }
+  for (int k = threadIdx.x; k < nbins; k += blockDim.x) hist[k] = 0u;
+  __syncthreads();
+  if (!mbar_wait(bar, 0, 1L << 24)) {
+    if (threadIdx.x == 0) atomicOr(flags + 1, 2);
+    // keep waiting (bounded) for the copy in flight before leaving
+    mbar_wait(bar, 0, 1L << 24);
+    return;
+  }
+  const int64_t per_block = (int64_t)blockDim.x * 8;
+  const int64_t l0 = (int64_t)blockIdx.x * per_block;
+  for (int it = 0; it < 8; ++it) {
+    const int64_t l = l0 + (int64_t)it * blockDim.x + threadIdx.x;
+    if (l >= nline) break;
+    const float w = bb[l].wl0;
+    if (l + 1 < nline && !(w <= bb[l + 1].wl0)) atomicOr(flags + 1, 1);
+    const double wl0 = (double)w * pc_ang;
+    // upper bound: number of edges <= wl0
+    int lo = 0, hi = nedge;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (edges[mid] <= wl0) lo = mid + 1;
+      else hi = mid;
+    }
+    atomicAdd(&hist[lo], 1u);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nbins; k += blockDim.x)
+    if (hist[k]) atomicAdd(&counts[k], hist[k]);
+}
+
+// exclusive scan of counts (n <= a few 1e4) in one block
+__global__ void __launch_bounds__(1024) scan_counts_kernel(const unsigned int* __restrict__ counts, int n,
+                                                           int* __restrict__ start) {
+  __shared__ int part[1024];
+  const int per = (n + blockDim.x - 1) / blockDim.x;
+  const int b = threadIdx.x * per;
+  int s = 0;
+  for (int k = b; k < b + per && k < n; ++k) s += (int)counts[k];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int t = 0; t < (int)blockDim.x; ++t) {
+      const int v = part[t];
+      part[t] = acc;
+      acc += v;
+    }
+  }
+  __syncthreads();
+  int acc = part[threadIdx.x];
+  for (int k = b; k < b + per && k < n; ++k) {
+    start[k] = acc;
+    acc += (int)counts[k];
+  }
+  if (threadIdx.x == blockDim.x - 1) start[n] = acc;
+}
+
+// ------------------------------------------------------------ per-cell preparation
+// hckt (physical_opacity.f:81), gas_sig (:84-89), hlparr (:203), grndlev (:95-101,
+// :165-171) and the per-(cell,element) free-free Gaunt row indices (:226-231).
+__global__ void opac_cell_prep_kernel(int nc, int nelem, int nst, const int32_t* __restrict__ ion_ni,
+                                      const double* __restrict__ temp, const double* __restrict__ natom,
+                                      const double* __restrict__ nelec, const double* __restrict__ vol,
+                                      const double* __restrict__ mass, const double* __restrict__ oc,
+                                      const double* __restrict__ ginv, int nothmson,
+                                      double* __restrict__ hckt, double* __restrict__ gas_sig,
+                                      double* __restrict__ hlparr, double* __restrict__ grndlev,
+                                      int* __restrict__ ffigg, double* __restrict__ ffdgg) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nc) return;
+  const double h = pc_hc / (pc_kb * temp[i]);
+  hckt[i] = h;
+  double s = 0.0;
+  if (!nothmson) {
+    s = cthomson * nelec[i] * natom[i] / vol[i];
+    if (mass[i] <= 0.0) s = 0.0;
+  }
+  gas_sig[i] = s;
+  hlparr[i] = sq(natom[i] / vol[i]) * nelec[i];
+  for (int iz = 1; iz <= nelem; ++iz) {
+    const int lim = min(iz, ion_ni[iz - 1] - 1);
+    for (int ii = 1; ii <= nst; ++ii) {
+      const size_t k = (size_t)(iz - 1) * nst + (ii - 1);
+      double v = 0.0;
+      if (ii <= lim && mass[i] > 0.0) v = oc[k * nc + i] * ginv[k * nc + i];
+      grndlev[k * nc + i] = v;
+    }
+    const double gg = (double)(iz * iz) * pc_rydberg * h;
+    const double rgg = 5.0 * (log10(gg) + 4.0) + 1.0;
+    int igg = rgg < 1.0 ? 1 : (rgg >= (double)(FF_NGG - 1) ? FF_NGG - 1 : (int)floor(rgg));
+    ffigg[(size_t)(iz - 1) * nc + i] = rgg > (double)FF_NGG ? -igg : igg;  // sign: gff >= 1 clamp (:238)
+    ffdgg[(size_t)(iz - 1) * nc + i] = rgg - igg;
+  }
+}
+
+// Which ion slots (iz,ii) carry any population: 1 if any cell has oc != 0.
+__global__ void ion_active_kernel(int nc, const double* __restrict__ oc, int* __restrict__ active) {
+  const int k = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += gridDim.x * blockDim.x)
+    if (oc[(size_t)k * nc + i] != 0.0) { active[k] = 1; return; }
+}
+
+// Active slots in the reference's loop order (iz ascending, ii = 1..min(iz,ni-1)),
+// physical_opacity.f:180-181.  Single thread; nelem*nst is at most a few hundred.
+__global__ void ion_compact_kernel(int nelem, int nst, const int32_t* __restrict__ ion_ni,
+                                   const int* __restrict__ active, int16_t* __restrict__ act_slot,
+                                   int* __restrict__ nact) {
+  int n = 0;
+  for (int iz = 1; iz <= nelem; ++iz) {
+    const int lim = min(iz, ion_ni[iz - 1] - 1);
+    for (int ii = 1; ii <= lim && ii <= nst; ++ii) {
+      const int s = (iz - 1) * nst + (ii - 1);
+      if (active[s]) act_slot[n++] = (int16_t)s;
+    }
+  }
+  *nact = n;
+}
+
+// Sub-group edges wlsub (physical_opacity.f:65-78), padded with DBL_MAX.
+__global__ void wlsub_kernel(int ng, int ngs, int nedge_pad, const double* __restrict__ wl,
+                             double* __restrict__ wlsub) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;  // 0-based edge
+  if (k >= nedge_pad) return;
+  const int nedge = ng * ngs + 1;
+  double v = DBL_MAX;
+  if (k < nedge) {
+    if (ngs == 1 || k == 0) {
+      v = wl[ngs == 1 ? k : 0];
+    } else {
+      const int ig = (k - 1) / ngs + 1, i = (k - 1) % ngs + 1;
+      const double help = 1.0 / ngs;
+      v = (1.0 - i * help) * wl[ig - 1] + i * help * wl[ig];
+    }
+  }
+  wlsub[k] = v;
+}
+
+// ------------------------------------------------------------ bound-free cross sections
+__device__ inline float PH1(const float* t, int k, int is, int nz, int ne) {
+  return t[(k - 1) + 6 * ((is - 1) + 7 * ((nz - 1) + 30 * (ne - 1)))];
+}
+__device__ inline float PH2(const float* t, int k, int nz, int ne) {
+  return t[(k - 1) + 7 * ((nz - 1) + 30 * (ne - 1))];
+}
+__device__ inline float sqf(float x) { return __fmul_rn(x, x); }  // real*4 ** 2
+
+// bfxsmod.f:184-272
+__device__ double bfxs(const float* __restrict__ ph1, const float* __restrict__ ph2, int nz, int ne,
+                       double e) {
+  const int ll[7] = {0, 0, 1, 0, 1, 2, 0};
+  const int ninn[30] = {0, 0, 1, 1, 1, 1, 1, 1, 1, 1, 3, 3, 3, 3, 3,
+                        3, 3, 3, 5, 5, 5, 5, 5, 5, 5, 5, 5, 5, 5, 5};
+  const int ntot[30] = {1, 1, 2, 2, 3, 3, 3, 3, 3, 3, 4, 4, 5, 5, 5,
+                        5, 5, 5, 6, 6, 6, 6, 6, 6, 6, 6, 6, 6, 7, 7};
+  double xs = 0.0;
+  if (nz < 1 || nz > 30) return xs;
+  if (ne < 1 || ne > nz) return xs;
+  int nout = ntot[ne - 1];
+  if (nz > 18) {
+    if (nz == ne) nout = 7;
+    if (nz == ne + 1 && (nz == 20 || nz == 21 || nz == 22 || nz == 25 || nz == 26)) nout = 7;
+  }
+  if (e < (double)PH1(ph1, 1, nout, nz, ne)) return xs;
+  const int nint_ = ninn[ne - 1];
+  double einn;
+  if (nz == 15 || nz == 17 || nz == 19 || (nz > 20 && nz != 26)) einn = 0.0;
+  else einn = ne < 3 ? (double)1.0e30f : (double)PH1(ph1, 1, nint_, nz, ne);
+  for (int is = 1; is <= nout; ++is) {
+    if (e < (double)PH1(ph1, 1, is, nz, ne)) continue;
+    if (is < nout && is > nint_ && e < einn) continue;
+    if (is <= nint_ || e >= einn) {
+      const double p1 = -(double)PH1(ph1, 5, is, nz, ne);
+      const double y = e / (double)PH1(ph1, 2, is, nz, ne);
+      const double q = -0.5 * p1 - (double)ll[is - 1] - 5.5;
+      const double a = (double)PH1(ph1, 3, is, nz, ne) * (sq(y - 1.0) + (double)sqf(PH1(ph1, 6, is, nz, ne)));
+      const double b = sqrt(y / (double)PH1(ph1, 4, is, nz, ne)) + 1.0;
+      xs = xs + a * pow(y, q) * pow(b, p1);
+    } else {
+      const double p1 = -(double)PH2(ph2, 4, nz, ne);
+      const double q = -0.5 * p1 - 5.5;
+      const double x = e / (double)PH2(ph2, 1, nz, ne) - (double)PH2(ph2, 6, nz, ne);
+      const double z = sqrt(x * x + (double)sqf(PH2(ph2, 7, nz, ne)));
+      const double a = (double)PH2(ph2, 2, nz, ne) * (sq(x - 1.0) + (double)sqf(PH2(ph2, 5, nz, ne)));
+      const double b = 1.0 + sqrt(z / (double)PH2(ph2, 3, nz, ne));
+      xs = xs + a * pow(z, q) * pow(b, p1);
+    }
+  }
+  return xs;
+}
+
+// xstab[(igs-1)*nact + a] = bfxs(iz, iz-ii+1, hc/(ev*wlsub(igs))), :177-183
+__global__ void bf_table_kernel(int ngsub, int maxact, const int* __restrict__ pnact,
+                                const int16_t* __restrict__ act_slot, int nst,
+                                const double* __restrict__ wlsub, const float* __restrict__ ph1,
+                                const float* __restrict__ ph2, double* __restrict__ xstab) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)ngsub * maxact) return;
+  const int igs = (int)(t / maxact) + 1;
+  const int a = (int)(t % maxact);
+  if (a >= *pnact) return;
+  const int slot = act_slot[a];
+  const int iz = slot / nst + 1, ii = slot % nst + 1;
+  const double wl = wlsub[igs - 1];
+  const double en = pc_hc / (pc_ev * wl);
+  xstab[t] = bfxs(ph1, ph2, iz, iz - ii + 1, en);
+}
+
+struct OpacArgs {
+  int nc, ng, ngs, ngsub, nelem, nst, maxact;
+  int nobb, nobf, noff;
+  const int* pnact;         // number of active bound-free ion slots (device)
+  double mix;
+  const double* wlsub;
+  const double* grp_wl;
+  const int* lstart;        // (ngsub+2)+1 offsets by igs
+  const slg_bbxs* bb;
+  const double* grndlev;    // [slot][cell]
+  const double* oc;         // [slot][cell]
+  const int16_t* act_slot;  // active slots, reference order
+  const double* xstab;      // [(igs-1)*maxact + a]
+  const double* hckt;
+  const double* hlparr;
+  const double* mass;
+  const double* natomfr;    // (0:nelem, ncell)
+  const double* temp;
+  const int* ffigg;         // [iz-1][cell], negative: apply gff >= 1
+  const double* ffdgg;
+  const double* gff;        // (81,41)
+  double ffc1;
+  float* cap32;             // (ng, ncell)
+  float* emiss32;
+  double* cap64;            // (ncell, ng) optional
+  int* flags;
+};
+
+// One sub-group igs for shell i: bb, bf and ff in the reference's order.
+__device__ inline double subgroup_opacity(const OpacArgs& A, int i, int igs, bool live) {
+  double cap = 0.0;
+  if (!live) return cap;
+  const double h = A.hckt[i];
+  if (!A.nobb) {
+    const int l0 = A.lstart[igs], l1 = A.lstart[igs + 1];
+    if (l1 > l0) {
+      const double wa = A.wlsub[igs - 1], wb = A.wlsub[igs];
+      const double wl = 0.5 * (wa + wb);
+      const double wlinv = 1.0 / wl;
+      const double dwl = wb - wa;
+      const double expfac = 1.0 - exp(-(h * wlinv));
+      const double phi = wl * wl / (dwl * pc_c);
+      for (int l = l0; l < l1; ++l) {
+        const float4 rec = __ldg(reinterpret_cast<const float4*>(A.bb) + l);
+        const float gxs = rec.y, chilw = rec.z;
+        const uint32_t izii = __float_as_uint(rec.w);
+        const int iz = (int)(int16_t)(izii & 0xffffu), ii = (int)(int16_t)(izii >> 16);
+        const double ocg = A.grndlev[((size_t)(iz - 1) * A.nst + (ii - 1)) * A.nc + i];
+        if (ocg <= 0.0) continue;
+        const double caphelp = phi * (double)gxs * ocg * exp(-((double)chilw * h)) * expfac;
+        cap = cap + caphelp;
+      }
+    }
+  }
+  if (!A.nobf) {
+    const double* xs = A.xstab + (size_t)(igs - 1) * A.maxact;
+    const int nact = *A.pnact;
+    for (int a = 0; a < nact; ++a) {
+      const double x = xs[a];
+      if (x == 0.0) continue;
+      const double o = A.oc[(size_t)A.act_slot[a] * A.nc + i];
+      if (o == 0.0) continue;  // adds +0 in the reference
+      cap = cap + x * pc_mbarn * o;
+    }
+  }
+  if (!A.noff) {
+    const double wl = A.wlsub[igs - 1];
+    const double wlinv = 1.0 / wl;
+    const double u = h * wlinv;
+    const double ru = 10.0 * (log10(u) + 4.0) + 1.0;
+    const int iu = ru < 1.0 ? 1 : (ru >= (double)(FF_NU - 1) ? FF_NU - 1 : (int)floor(ru));
+    const double du = ru - iu;
+    const double help = A.ffc1 * sqrt(h) * (1.0 - exp(-u)) * cube(wl) * A.hlparr[i];
+    const double* nfr = A.natomfr + (size_t)(A.nelem + 1) * i;
+    for (int iz = 1; iz <= A.nelem; ++iz) {
+      const double fr = nfr[iz];
+      if (fr == 0.0) continue;  // adds +0 in the reference
+      int igg = A.ffigg[(size_t)(iz - 1) * A.nc + i];
+      const bool clamp1 = igg < 0;
+      igg = clamp1 ? -igg : igg;
+      const double dgg = A.ffdgg[(size_t)(iz - 1) * A.nc + i];
+      const double* G = A.gff;
+      double g = (1.0 - du) * (1.0 - dgg) * G[(iu - 1) + FF_NU * (igg - 1)] +
+                 du * (1.0 - dgg) * G[iu + FF_NU * (igg - 1)] +
+                 (1.0 - du) * dgg * G[(iu - 1) + FF_NU * igg] + du * dgg * G[iu + FF_NU * igg];
+      if (clamp1) g = g > 1.0 ? g : 1.0;
+      cap = cap + help * g * (double)(iz * iz) * fr;
+    }
+  }
+  return cap;
+}
+
+__global__ void __launch_bounds__(OPAC_GT * 32) opacity_fwd_kernel(const OpacArgs A) {
+  __shared__ float tcap[OPAC_CT][OPAC_GT + 1];
+  __shared__ float tem[OPAC_CT][OPAC_GT + 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ig = blockIdx.y * OPAC_GT + warp + 1;  // 1-based group
+  const int i = blockIdx.x * OPAC_CT + lane;       // 0-based shell
+  const bool valid = ig <= A.ng && i < A.nc;
+  const bool live = valid && A.mass[i] > 0.0;
+  double cap = 0.0;
+  if (valid) {
+    if (A.ngs == 1) {
+      cap = subgroup_opacity(A, i, ig, live);
+    } else {
+      // collapse subgridding, physical_opacity.f:252-264
+      double sp = 0.0, sr = 0.0;
+      for (int s = 1; s <= A.ngs; ++s) {
+        const double v = subgroup_opacity(A, i, (ig - 1) * A.ngs + s, live);
+        if (v > 0.0) { sp = sp + v; sr = sr + 1.0 / v; }
+      }
+      const double help = 1.0 / A.ngs;
+      const double capp = sp * help;
+      double capr = sr * help;
+      if (capr > 0.0) capr = 1.0 / capr;
+      cap = (1.0 - A.mix) * capp + A.mix * capr;
+    }
+  }
+  float c32 = (float)cap, e32 = 0.f;
+  if (live) {
+    const double wl = 0.5 * (A.grp_wl[ig] + A.grp_wl[ig - 1]);
+    const double B_nu = (wl * wl / pc_c) * planck(wl, A.temp[i]);
+    e32 = (float)(0.0 + cap * B_nu);
+    int f = 0;
+    if (c32 == 0.f) f |= 1;
+    if (c32 < 0.f) f |= 2;
+    if (c32 != c32) f |= 4;
+    if (c32 > FLT_MAX) f |= 8;
+    if (f) atomicOr(A.flags, f);
+  }
+  if (valid && A.cap64) A.cap64[(size_t)(ig - 1) * A.nc + i] = cap;
+  tcap[lane][warp] = c32;
+  tem[lane][warp] = e32;
+  __syncthreads();
+  // write (ng, ncell): each shell's OPAC_GT consecutive groups together
+  const int ci = threadIdx.x / OPAC_GT, gj = threadIdx.x % OPAC_GT;
+  const int i2 = blockIdx.x * OPAC_CT + ci, g2 = blockIdx.y * OPAC_GT + gj;
+  if (i2 < A.nc && g2 < A.ng) {
+    A.cap32[(size_t)i2 * A.ng + g2] = tcap[ci][gj];
+    A.emiss32[(size_t)i2 * A.ng + g2] = tem[ci][gj];
+  }
+}
+
+// ------------------------------------------------------------ analytic opacity
+__global__ void analytic_opacity_kernel(int nc, int ng, const double* __restrict__ wlinv,
+                                        const double* __restrict__ temp, const double* __restrict__ rho,
+                                        int kind, double capcoef, double captpwr, double caprpwr,
+                                        double sigcoef, double sigtpwr, double sigrpwr, double ldisp1,
+                                        double ldisp2, double* __restrict__ sig, float* __restrict__ cap) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nc * ng) return;
+  const int i = (int)(t / ng), ig = (int)(t % ng) + 1;
+  const double cc = capcoef * pow(temp[i], captpwr) * pow(rho[i], caprpwr);
+  double v;
+  if (kind == 1) v = cc;
+  else if (kind == 2) {
+    const double x1 = pc_hc * wlinv[ig] / pc_kb;
+    const double x2 = pc_hc * wlinv[ig - 1] / pc_kb;
+    v = 0.5 * cc * (x1 + x2) / sq(x1 * x2);
+  } else {
+    v = (ig % 2 == 1) ? cc * ldisp1 : cc * ldisp2;
+  }
+  cap[t] = (float)v;
+  if (ig == 1) sig[i] = sigcoef * pow(temp[i], sigtpwr) * pow(rho[i], sigrpwr);
+}
+
+// ------------------------------------------------------------ Planck / Rosseland means
+// One block per shell; a fixed-shape tree reduction over groups.
+__global__ void __launch_bounds__(256) opacity_means_kernel(int nc, int ng, const double* __restrict__ wlinv,
+                                                            const double* __restrict__ temp,
+                                                            const double* __restrict__ sig,
+                                                            const float* __restrict__ cap,
+                                                            double* __restrict__ capgrey,
+                                                            double* __restrict__ capross) {
+  __shared__ double sp[256], sr[256];
+  const int i = blockIdx.x;
+  const double tinv = 1.0 / temp[i];
+  const double hct = hck * tinv;
+  const double s = sig ? sig[i] : 0.0;
+  double ap = 0.0, ar = 0.0;
+  for (int g = threadIdx.x; g < ng; g += blockDim.x) {
+    const double c = (double)cap[(size_t)i * ng + g];
+    ap = ap + c * specintv_elem(hct, wlinv, g);
+    ar = ar + (1.0 / (s + c)) * spectintv_elem(hct, wlinv, g);
+  }
+  sp[threadIdx.x] = ap;
+  sr[threadIdx.x] = ar;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      sp[threadIdx.x] = sp[threadIdx.x] + sp[threadIdx.x + w];
+      sr[threadIdx.x] = sr[threadIdx.x] + sr[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    capgrey[i] = sp[0];
+    if (capross) capross[i] = 1.0 / sr[0];
+  }
+}
+
+}  // namespace
+
+// ============================================================ launchers
+int launch_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_flags* flags,
+                            double* gas_sig, float* gas_cap, float* gas_emiss, double* cap64) {
+  const int nc = ctx->nx, ng = ctx->ng;
+  const int ngs = flags->ngs < 1 ? 1 : flags->ngs;
+  const int ngsub = ng * ngs;
+  const int nelem = ctx->nelem, nst = ctx->nstage;
+  const int nslot = nelem * nst;
+  cudaStream_t st = ctx->stream;
+  if (nelem <= 0) return set_error(ctx, SLG_ERR_STATE, "atomic data not set");
+  const int nedge = ngsub + 1, nedge_pad = (nedge + 1) & ~1;
+  double* d_wlsub = (double*)scratch(ctx, 0, sizeof(double) * nedge_pad);
+  unsigned int* d_counts = (unsigned int*)scratch(ctx, 1, sizeof(unsigned int) * (nedge + 2));
+  int* d_lstart = (int*)scratch(ctx, 2, sizeof(int) * (nedge + 3));
+  int* d_flags = (int*)scratch(ctx, 3, sizeof(int) * 4);
+  double* d_hckt = (double*)scratch(ctx, 4, sizeof(double) * nc);
+  double* d_hlp = (double*)scratch(ctx, 5, sizeof(double) * nc);
+  double* d_grnd = (double*)scratch(ctx, 6, sizeof(double) * (size_t)nc * nslot);
+  int* d_ffigg = (int*)scratch(ctx, 7, sizeof(int) * (size_t)nc * nelem);
+  double* d_ffdgg = (double*)scratch(ctx, 8, sizeof(double) * (size_t)nc * nelem);
+  int* d_active = (int*)scratch(ctx, 9, sizeof(int) * (nslot + 1));
+  int16_t* d_act = (int16_t*)scratch(ctx, 10, sizeof(int16_t) * nslot);
+  double* d_xs = (double*)scratch(ctx, 11, sizeof(double) * (size_t)ngsub * nslot);
+  if (!d_wlsub || !d_counts || !d_lstart || !d_flags || !d_hckt || !d_hlp || !d_grnd || !d_ffigg ||
+      !d_ffdgg || !d_active || !d_act || !d_xs)
+    return SLG_ERR_OOM;
+  int* d_nact = d_active + nslot;
+  cudaMemsetAsync(d_counts, 0, sizeof(unsigned int) * (nedge + 2), st);
+  cudaMemsetAsync(d_flags, 0, sizeof(int) * 4, st);
+  cudaMemsetAsync(d_active, 0, sizeof(int) * (nslot + 1), st);
+  wlsub_kernel<<<(nedge_pad + 255) / 256, 256, 0, st>>>(ng, ngs, nedge_pad, ctx->d_wl, d_wlsub);
+  const bool do_bb = ctx->nline > 0 && !flags->nobb;
+  if (do_bb) {
+    const size_t shm = 16 + sizeof(double) * nedge_pad + sizeof(unsigned int) * (nedge + 1);
+    if (shm > 220 * 1024)
+      return set_error(ctx, SLG_ERR_ARG, "too many sub-groups for line binning (%d)", ngsub);
+    cudaFuncSetAttribute(bin_lines_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    const int64_t per_block = 256 * 8;
+    const int nb = (int)((ctx->nline + per_block - 1) / per_block);
+    bin_lines_kernel<<<nb, 256, shm, st>>>(ctx->d_bb, ctx->nline, d_wlsub, nedge, nedge_pad, d_counts,
+                                           d_flags);
+    scan_counts_kernel<<<1, 1024, 0, st>>>(d_counts, nedge + 1, d_lstart);
+  } else {
+    cudaMemsetAsync(d_lstart, 0, sizeof(int) * (nedge + 3), st);
+  }
+  opac_cell_prep_kernel<<<(nc + 127) / 128, 128, 0, st>>>(
+      nc, nelem, nst, ctx->d_ion_ni, gas->temp, gas->natom, gas->nelec, gas->vol, gas->mass, gas->oc,
+      gas->ginv, flags->nothmson, d_hckt, gas_sig, d_hlp, d_grnd, d_ffigg, d_ffdgg);
+  const bool do_bf = !flags->nobf;
+  if (do_bf) {
+    dim3 ga((nc + 255) / 256 < 8 ? (nc + 255) / 256 : 8, nslot);
+    ion_active_kernel<<<ga, 256, 0, st>>>(nc, gas->oc, d_active);
+    ion_compact_kernel<<<1, 1, 0, st>>>(nelem, nst, ctx->d_ion_ni, d_active, d_act, d_nact);
+    const int64_t nt = (int64_t)ngsub * nslot;
+    bf_table_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(ngsub, nslot, d_nact, d_act, nst, d_wlsub,
+                                                                  ctx->d_ph1, ctx->d_ph2, d_xs);
+  }
+  OpacArgs A;
+  A.nc = nc; A.ng = ng; A.ngs = ngs; A.ngsub = ngsub; A.nelem = nelem; A.nst = nst; A.maxact = nslot;
+  A.pnact = d_nact;
+  A.nobb = !do_bb; A.nobf = !do_bf; A.noff = flags->noff;
+  A.mix = flags->opacmixrossel;
+  A.wlsub = d_wlsub; A.grp_wl = ctx->d_wl; A.lstart = d_lstart; A.bb = ctx->d_bb;
+  A.grndlev = d_grnd; A.oc = gas->oc; A.act_slot = d_act; A.xstab = d_xs;
+  A.hckt = d_hckt; A.hlparr = d_hlp; A.mass = gas->mass; A.natomfr = gas->natomfr; A.temp = gas->temp;
+  A.ffigg = d_ffigg; A.ffdgg = d_ffdgg; A.gff = ctx->d_gff;
+  A.ffc1 = ff_c1a * sqrt(ff_c1b);
+  A.cap32 = gas_cap; A.emiss32 = gas_emiss; A.cap64 = cap64; A.flags = d_flags;
+  if (!ctx->d_gff && !A.noff) return set_error(ctx, SLG_ERR_STATE, "free-free table not set");
+  dim3 grid((nc + OPAC_CT - 1) / OPAC_CT, (ng + OPAC_GT - 1) / OPAC_GT);
+  opacity_fwd_kernel<<<grid, OPAC_GT * 32, 0, st>>>(A);
+  return cuda_check(ctx, cudaGetLastError(), "opacity_fwd launch");
+}
+
+// Sanity bitmask of physical_opacity.f:282-291 (word 0) and line-binning
+// errors (word 1: 1 unsorted lines, 2 shared-memory staging time-out).
+int opacity_flags(slg_ctx* ctx, int32_t* sanity, int32_t* binning) {
+  int* d_flags = (int*)scratch(ctx, 3, sizeof(int) * 4);
+  int h[2] = {0, 0};
+  int rc = cuda_check(ctx, cudaMemcpyAsync(h, d_flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream),
+                      "flags download");
+  if (rc) return rc;
+  if ((rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "flags sync"))) return rc;
+  if (sanity) *sanity = h[0];
+  if (binning) *binning = h[1];
+  return SLG_OK;
+}
+
+int launch_analytic_opacity(slg_ctx* ctx, const double* temp, const double* rho, int kind,
+                            const double* c, double* gas_sig, float* gas_cap) {
+  const int64_t nt = (int64_t)ctx->nx * ctx->ng;
+  analytic_opacity_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, ctx->stream>>>(
+      ctx->nx, ctx->ng, ctx->d_wlinv, temp, rho, kind, c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7],
+      gas_sig, gas_cap);
+  return cuda_check(ctx, cudaGetLastError(), "analytic_opacity launch");
+}
+
+int launch_opacity_means(slg_ctx* ctx, const double* temp, const double* sig, const float* cap,
+                         double* capgrey, double* capross) {
+  opacity_means_kernel<<<ctx->nx, 256, 0, ctx->stream>>>(ctx->nx, ctx->ng, ctx->d_wlinv, temp, sig, cap,
+                                                        capgrey, capross);
+  return cuda_check(ctx, cudaGetLastError(), "opacity_means launch");
+}
+
+}  // namespace slg

@@ -1,0 +1,192 @@
+// slg_device.cuh -- device-side constants and helpers shared by the kernels.
+//
+// Physical constants are those of physconstmod.f:11-51; derived constants are
+// written with the Fortran expression order so that the FP64 kernels round
+// like the reference (integer powers as explicit products, no FMA contraction:
+// the FP64 translation units are compiled with -fmad=false).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace slg {
+
+constexpr double pc_acoef = 7.5657e-15;
+constexpr double pc_pi = 3.1415926535897932385;
+constexpr double pc_pi2 = 2.0 * pc_pi;
+constexpr double pc_pi4 = 4.0 * pc_pi;
+constexpr double pc_c = 2.997924562e10;
+constexpr double pc_kb = 1.3806505e-16;
+constexpr double pc_me = 9.1093826e-28;
+constexpr double pc_h = 6.6260693e-27;
+constexpr double pc_e = 4.80325e-10;
+constexpr double pc_rydberg = 1.0973731534e5;
+constexpr double pc_dext = 0.7104;
+constexpr double pc_ev = 1.60217653e-12;
+constexpr double pc_ang = 1e-8;
+constexpr double pc_mbarn = 1e-18;
+
+constexpr double cinv = 1.0 / pc_c;
+constexpr double pi_4th = (pc_pi * pc_pi) * (pc_pi * pc_pi);
+constexpr double hck = pc_h * pc_c / pc_kb;              // groupmod.f:110
+constexpr double ftpi4 = 15.0 / pi_4th;                   // groupmod.f:109
+constexpr double ftpi4r = 15.0 / (4.0 * pi_4th);          // groupmod.f:290
+constexpr double planck_c1 = 2.0 * pc_h * (pc_c * pc_c);  // physconstmod.f:87
+constexpr double planck_c2 = pc_h * pc_c / pc_kb;         // physconstmod.f:88
+constexpr double pc_hc = pc_h * pc_c;
+constexpr double e2c = pc_e * pc_e;
+constexpr double e4c = e2c * e2c;
+constexpr double e6c = e4c * e2c;
+constexpr double c2c = pc_c * pc_c;
+constexpr double c4c = c2c * c2c;
+constexpr double cthomson = 8.0 * pc_pi * e4c / (3.0 * (pc_me * pc_me) * c4c);  // physical_opacity.f:51
+constexpr double ff_c1a = 4.0 * e6c / (3.0 * pc_h * pc_me * c4c);              // physical_opacity.f:32
+constexpr double ff_c1b = pc_pi2 / (3.0 * pc_me * pc_h * pc_c);                 // argument of its sqrt
+// Fortran `1.0/3.0` is a real*4 quotient promoted to real*8 as an exponent.
+constexpr double third_r4 = (double)(1.0f / 3.0f);
+
+constexpr int FF_NU = 81, FF_NGG = 41;
+
+__host__ __device__ inline double sq(double x) { return x * x; }
+__host__ __device__ inline double cube(double x) { return x * x * x; }
+__host__ __device__ inline double pow4(double x) { double t = x * x; return t * t; }
+__host__ __device__ inline double pow5(double x) { double t = x * x; return t * t * x; }
+
+// MISC/binsrch.f90:3-77.  arr holds n values; returns the 1-based interval
+// index (clamped to 1..n-1 unless widerange), -1 for invalid input.
+__device__ inline int binsrch(double x, const double* __restrict__ arr, int n, bool widerange) {
+  if (n == 2) {
+    int r;
+    if (x >= arr[0] && x <= arr[1]) r = 1;
+    else if (x < arr[0]) r = 0;
+    else if (x > arr[1]) r = n;
+    else return -1;
+    if (!widerange) r = 1;
+    return r;
+  }
+  int imin = 1, imax = n, imid = (n + 1) / 2;
+  while (imax - imin > 1) {
+    const double amin = arr[imin - 1], amid = arr[imid - 1], amax = arr[imax - 1];
+    if (x >= amin && x < amid) {
+      imax = imid;
+      imid = (imax + imin) / 2;
+    } else if (x >= amid && x <= amax) {
+      imin = imid;
+      imid = (imax + imin) / 2;
+    } else {
+      if (x < arr[0]) { imin = 0; imid = 0; break; }
+      else if (x > arr[n - 1]) { imin = n; imid = n; break; }
+      else return -1;
+    }
+  }
+  if (imid != imin) imid = -1;
+  if (!widerange) {
+    imid = imid > n - 1 ? n - 1 : imid;
+    imid = imid < 1 ? 1 : imid;
+  }
+  return imid;
+}
+
+// groupmod.f:99-120 (specint0); ig is 1-based, wlinv holds grp_wlinv(1:ng+1)
+__device__ inline double specint0(double tempinv, const double* __restrict__ wlinv, int ig) {
+  double x = hck * tempinv;
+  const double dx = x * fabs(wlinv[ig] - wlinv[ig - 1]);
+  x = x * 0.5 * (wlinv[ig] + wlinv[ig - 1]);
+  if (x >= 300.0) x = 300.0;
+  return ftpi4 * dx * cube(x) / (exp(x) - 1.0);
+}
+
+// groupmod.f:123-143
+__device__ inline double dopspeccalc(double tempinv, const double* __restrict__ wlinv, int ig) {
+  double x = hck * tempinv;
+  x = x * wlinv[ig];
+  if (x >= 300.0) x = 300.0;
+  return ftpi4 * pow4(x) / (exp(x) - 1.0);
+}
+
+// Integrand of specintv, groupmod.f:263-270
+__device__ inline double fplanck(double x) {
+  if (x >= 300.0) return 27000000.0 / (exp(300.0) - 1.0);
+  return cube(x) / (exp(x) - 1.0);
+}
+// Integrand of spectintv, groupmod.f:395-402
+__device__ inline double fross(double x) {
+  if (x >= 300.0) {
+    const double e3 = exp(300.0);
+    return (8100000000.0 * e3) / sq(e3 - 1.0);
+  }
+  const double ex = exp(x);
+  return (pow4(x) * ex) / sq(ex - 1.0);
+}
+// One element k (0-based, group offset+k) of specintv mode 0 (groupmod.f:189-198):
+// x = hck*tempinv*wlinv, ss = ftpi4*|x2-x1|*f((x1+x2)/2).
+__device__ inline double specintv_elem(double hct, const double* __restrict__ wlinv, int g0) {
+  const double x1 = hct * wlinv[g0], x2 = hct * wlinv[g0 + 1];
+  return ftpi4 * fabs(x2 - x1) * fplanck(0.5 * (x2 + x1));
+}
+__device__ inline double spectintv_elem(double hct, const double* __restrict__ wlinv, int g0) {
+  const double x1 = hct * wlinv[g0], x2 = hct * wlinv[g0 + 1];
+  double s = ftpi4r * fabs(x2 - x1) * fross(0.5 * (x2 + x1));
+  return s != s ? 0.0 : s;  // groupmod.f:390-392
+}
+
+// physconstmod.f:79-93
+__device__ inline double planck(double wl, double temp) {
+  double b = 1.0 / (wl * temp);
+  if (planck_c2 * b >= 300.0) b = 300.0 / planck_c2;
+  return planck_c1 * pow5(temp * b) / (exp(planck_c2 * b) - 1.0);
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11).
+struct u32x4 { uint32_t a, b, c, d; };
+__device__ inline u32x4 philox4x32_10(u32x4 ctr, uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi0 = __umulhi(0xD2511F53u, ctr.a), lo0 = 0xD2511F53u * ctr.a;
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, ctr.c), lo1 = 0xCD9E8D57u * ctr.c;
+    ctr = u32x4{hi1 ^ ctr.b ^ k0, lo1, hi0 ^ ctr.d ^ k1, lo0};
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return ctr;
+}
+__device__ inline double u52_to_unit(uint32_t w0, uint32_t w1) {
+  const uint64_t m = ((uint64_t)w0 << 20) | (w1 >> 12);
+  return ((double)m + 0.5) * 0x1p-52;
+}
+
+// Per-particle stream: draw k uses counter (k/2, pid, stream), words (0,1) for
+// even k and (2,3) for odd k; the odd half is kept for the next draw.
+struct PhiloxStream {
+  uint32_t k0, k1, pid_lo, pid_hi, stream;
+  uint32_t k;
+  uint32_t w2, w3;
+  __device__ inline void init(uint64_t seed, uint64_t pid, uint32_t s) {
+    k0 = (uint32_t)seed; k1 = (uint32_t)(seed >> 32);
+    pid_lo = (uint32_t)pid; pid_hi = (uint32_t)(pid >> 32);
+    stream = s; k = 0;
+  }
+  __device__ inline double draw() {
+    double r;
+    if ((k & 1u) == 0u) {
+      const u32x4 o = philox4x32_10(u32x4{k >> 1, pid_lo, pid_hi, stream}, k0, k1);
+      w2 = o.c; w3 = o.d;
+      r = u52_to_unit(o.a, o.b);
+    } else {
+      r = u52_to_unit(w2, w3);
+    }
+    ++k;
+    return r;
+  }
+};
+
+__device__ inline uint64_t fnv_mix(uint64_t h, int32_t v) {
+  const uint32_t u = (uint32_t)v;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    h ^= (u >> (8 * b)) & 0xffu;
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+}  // namespace slg

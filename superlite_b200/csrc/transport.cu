@@ -1,0 +1,406 @@
+// transport.cu -- the 1-D spherical IMC/DDMC particle loop (FP64 form) and the
+// flux / source tallies, for sm_100a.
+//
+// Reference: particle_advance.f90:4-327, fluxtally.f:3-61, sourcetally.f:3-48.
+//
+// Layout and scheduling:
+//  * A persistent grid (a multiple of the SM count) processes particles one
+//    event per loop iteration.  A lane whose particle has finished takes the
+//    next slot from a global counter; the lanes of a warp that need work in
+//    the same iteration share one atomicAdd (warp-aggregated).  This keeps
+//    lanes busy while long DDMC random walks finish (lifetimes differ by
+//    orders of magnitude).
+//  * Particle state lives in registers for the whole flight; the 64-byte
+//    packet is read and written once with 16-byte vector accesses.
+//  * grd_tally / grd_jrad are accumulated in registers while the (cell,group)
+//    of consecutive events is unchanged and flushed with FP64 atomics;
+//    counters go through shared-memory atomics and one global atomic per block.
+//  * Random numbers: one Philox4x32-10 stream per particle (shared with the
+//    oracle), so event sequences can be compared particle by particle.
+#include <cuda_runtime.h>
+#include <cfloat>
+#include "slg_device.cuh"
+#include "slg_internal.h"
+#include "transport_impl.cuh"
+
+namespace slg {
+namespace {
+
+constexpr int TRN_BLOCK = 128;
+
+__device__ inline void load_packet(const slg_packet* p, double& x, double& y, double& z, double& mu,
+                                   double& om, double& e, double& e0, double& wl) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  const double2 a = q[0], b = q[1], c = q[2], d = q[3];
+  x = a.x; y = a.y; z = b.x; mu = b.y; om = c.x; e = c.y; e0 = d.x; wl = d.y;
+}
+__device__ inline void store_packet(slg_packet* p, double x, double y, double z, double mu, double om,
+                                    double e, double e0, double wl) {
+  double2* q = reinterpret_cast<double2*>(p);
+  q[0] = make_double2(x, y);
+  q[1] = make_double2(z, mu);
+  q[2] = make_double2(om, e);
+  q[3] = make_double2(e0, wl);
+}
+
+template <bool TRACE>
+__global__ void __launch_bounds__(TRN_BLOCK) particle_advance_kernel(const TrnArgs A) {
+  __shared__ unsigned long long s_cnt[20];
+  __shared__ double s_sum[3];
+  if (threadIdx.x < 20) s_cnt[threadIdx.x] = 0ull;
+  if (threadIdx.x < 3) s_sum[threadIdx.x] = 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  double evelo = 0.0, eout = 0.0, sflux = 0.0;
+  unsigned long long nimc = 0, nddmc = 0, nswap = 0, npckt = 0, nflux = 0, nwarn = 0, nmax = 0;
+  // current particle
+  long long ip = -1;
+  bool have = false;
+  Ptcl p;
+  double y = 0, z = 0, om = 0;
+  PhiloxStream rng;
+  int istep = 0;
+  uint64_t h = 0;
+  // register caches of the tallies
+  int t_ic = 0;
+  double t_acc = 0.0;
+  int j_ic = 0, j_ig = 0;
+  double j_acc = 0.0;
+  bool queue_done = false;
+  // Every lane stays in this loop until the whole warp is done, so the warp is
+  // converged at the top of each iteration (one event per iteration).
+  while (true) {
+    __syncwarp();
+    // ---- refill idle lanes (warp-aggregated)
+    const bool need = !have && !queue_done;
+    const unsigned needm = __ballot_sync(0xffffffffu, need);
+    if (needm) {
+      const int leader = __ffs(needm) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(&A.acc->next, (unsigned long long)__popc(needm));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        const long long cand = (long long)base + __popc(needm & ((1u << lane) - 1u));
+        if (cand >= A.npart) {
+          queue_done = true;
+        } else {
+          ip = cand;
+          if (A.isvacant[ip]) {
+            have = false;  // vacant slot: nothing to do, take another next iteration
+          } else {
+            // ---- particle set-up, particle_advance.f90:141-202
+            double x, mu, e, e0, wl;
+            load_packet(A.prt + ip, x, y, z, mu, om, e, e0, wl);
+            npckt++;
+            p.x = x; p.mu = mu; p.e = e; p.e0 = e0; p.wl = wl; p.dist = 0.0;
+            p.ix = binsrch(x, A.xarr, A.nx + 1, false);
+            p.ig = binsrch(wl, A.wl, A.ng + 1, false);
+            const double help = dxd(A, p.ix);
+            const double tau = (A.sig[p.ix - 1] + CAPd(A, p.ig, p.ix)) * help;
+            p.itype = (A.puretran || tau < A.tauddmc) ? 1 : 2;
+            p.vx = (A.vxarr[p.ix - 1] * (A.xarr[p.ix] - x) + A.vxarr[p.ix] * (x - A.xarr[p.ix - 1])) /
+                   (A.xarr[p.ix] - A.xarr[p.ix - 1]);
+            if (p.itype == 1) {
+              const double labfact = 1.0 - p.vx * p.mu / pc_c;
+              p.wl = p.wl * labfact;
+              p.e = p.e / labfact;
+              p.e0 = p.e0 / labfact;
+            }
+            p.stat = 0;
+            p.idist = 0;
+            istep = 0;
+            rng.init(A.seed, (uint64_t)ip, 0u);
+            if (TRACE) h = 1469598103934665603ull;
+            have = true;
+          }
+        }
+      }
+    }
+    if (__all_sync(0xffffffffu, !have && queue_done)) break;
+    if (!have) continue;
+    // ---- one event, particle_advance.f90:204-268
+    istep++;
+    const int icold = p.ix, igold = p.ig;
+    double eraddens, jrad, eamp = 0.0;
+    int ierr;
+    if (p.itype == 1 || A.puretran) {
+      nimc++;
+      transport11_dev(A, p, rng, eraddens, eamp, jrad, evelo, ierr);
+      if (p.itype != 1) {
+        nswap++;
+        if (A.dogrdtally) atomicAdd(&A.methodswap[icold - 1], 1);
+      }
+      if (!A.noampfact && eamp != 0.0) atomicAdd(&A.eamp[icold - 1], eamp);
+    } else {
+      nddmc++;
+      diffusion11_dev(A, p, rng, eraddens, jrad, evelo, ierr);
+      if (p.itype == 1) {
+        nswap++;
+        if (A.dogrdtally) atomicAdd(&A.methodswap[icold - 1], 1);
+      }
+    }
+    {
+      const int id = p.idist > -3 ? p.idist : -3;
+      atomicAdd(&s_cnt[9 + id + 3], 1ull);
+    }
+    if (icold != t_ic) {
+      if (t_ic > 0 && t_acc != 0.0) atomicAdd(&A.tally[t_ic - 1], t_acc);
+      t_ic = icold;
+      t_acc = 0.0;
+    }
+    t_acc = t_acc + eraddens;
+    if (icold != j_ic || igold != j_ig) {
+      if (j_ic > 0 && j_acc != 0.0) atomicAdd(&A.jrad[(size_t)(j_ic - 1) * A.ng + (j_ig - 1)], j_acc);
+      j_ic = icold;
+      j_ig = igold;
+      j_acc = 0.0;
+    }
+    j_acc = j_acc + jrad;
+    if (TRACE) {
+      h = fnv_mix(h, p.idist);
+      h = fnv_mix(h, p.itype);
+      h = fnv_mix(h, p.ix);
+      h = fnv_mix(h, p.ig);
+      h = fnv_mix(h, p.stat);
+    }
+    if (p.itype == 1 && p.stat == 0) {
+      if (p.x > A.xarr[p.ix] || p.x < A.xarr[p.ix - 1] || p.x != p.x) {
+        if (ierr == 0) ierr = -99;
+      }
+    }
+    if (ierr == -99) nwarn++;
+    if (ierr == 0 && A.max_steps > 0 && istep >= A.max_steps && p.stat == 0) ierr = 1001;
+    if (ierr > 0) {
+      if (A.errorfatal) {
+        const unsigned long long key = ((unsigned long long)(ip + 1) << 32) | (unsigned)ierr;
+        atomicMin(&A.acc->ierr_key, key);
+      }
+      p.stat = 2;
+    }
+    if (p.stat != 0) {
+      // ---- particle end, particle_advance.f90:271-292
+      if ((unsigned long long)istep > nmax) nmax = istep;
+      if (TRACE) {
+        A.trace_hash[ip] = h;
+        A.trace_nstep[ip] = istep;
+      }
+      if (p.stat == 2) {
+        A.isvacant[ip] = 1;
+      } else {
+        nflux++;
+        sflux = sflux - p.e;
+        eout = eout + p.e;
+        store_packet(A.prt + ip, DBL_MAX, y, z, p.mu, om, p.e, p.e0, p.wl);
+      }
+      have = false;
+    }
+  }
+  // ---- flush
+  if (t_ic > 0 && t_acc != 0.0) atomicAdd(&A.tally[t_ic - 1], t_acc);
+  if (j_ic > 0 && j_acc != 0.0) atomicAdd(&A.jrad[(size_t)(j_ic - 1) * A.ng + (j_ig - 1)], j_acc);
+  atomicAdd(&s_sum[0], evelo);
+  atomicAdd(&s_sum[1], eout);
+  atomicAdd(&s_sum[2], sflux);
+  atomicAdd(&s_cnt[0], npckt);
+  atomicAdd(&s_cnt[1], nflux);
+  atomicAdd(&s_cnt[2], nimc);
+  atomicAdd(&s_cnt[3], nddmc);
+  atomicAdd(&s_cnt[4], nswap);
+  atomicMax(&s_cnt[5], nmax);
+  atomicAdd(&s_cnt[6], nwarn);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    atomicAdd(&A.acc->evelo, s_sum[0]);
+    atomicAdd(&A.acc->eout, s_sum[1]);
+    atomicAdd(&A.acc->sflux, s_sum[2]);
+    atomicAdd(&A.acc->npckt, s_cnt[0]);
+    atomicAdd(&A.acc->nflux, s_cnt[1]);
+    atomicAdd(&A.acc->nimc, s_cnt[2]);
+    atomicAdd(&A.acc->nddmc, s_cnt[3]);
+    atomicAdd(&A.acc->nswap, s_cnt[4]);
+    atomicMax(&A.acc->nmax, s_cnt[5]);
+    atomicAdd(&A.acc->nwarn, s_cnt[6]);
+  }
+  if (threadIdx.x < 11 && s_cnt[9 + threadIdx.x]) atomicAdd(&A.acc->ndist[threadIdx.x], s_cnt[9 + threadIdx.x]);
+}
+
+// fluxtally.f:30-54; flux-grid histogram in shared memory, flushed once per block.
+__global__ void fluxtally_kernel(long long npart, const slg_packet* __restrict__ prt,
+                                 int32_t* __restrict__ isvacant, int flx_ng, const double* __restrict__ flx_wl,
+                                 double* __restrict__ luminos, double* __restrict__ lumdev,
+                                 int32_t* __restrict__ lumnum, int use_smem) {
+  extern __shared__ double sh[];
+  double* s_lum = sh;
+  double* s_dev = sh + flx_ng;
+  int* s_num = reinterpret_cast<int*>(sh + 2 * flx_ng);
+  if (use_smem) {
+    for (int k = threadIdx.x; k < flx_ng; k += blockDim.x) { s_lum[k] = 0.0; s_dev[k] = 0.0; s_num[k] = 0; }
+    __syncthreads();
+  }
+  for (long long ip = (long long)blockIdx.x * blockDim.x + threadIdx.x; ip < npart;
+       ip += (long long)gridDim.x * blockDim.x) {
+    if (isvacant[ip]) continue;
+    const slg_packet* q = prt + ip;
+    if (q->x != DBL_MAX) continue;
+    const double e = q->e;
+    const int ig = binsrch(q->wl, flx_wl, flx_ng + 1, false);
+    if (use_smem) {
+      atomicAdd(&s_lum[ig - 1], e);
+      atomicAdd(&s_dev[ig - 1], sq(e));
+      atomicAdd(&s_num[ig - 1], 1);
+    } else {
+      atomicAdd(&luminos[ig - 1], e);
+      atomicAdd(&lumdev[ig - 1], sq(e));
+      atomicAdd(&lumnum[ig - 1], 1);
+    }
+    isvacant[ip] = 1;
+  }
+  if (use_smem) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < flx_ng; k += blockDim.x) {
+      if (s_num[k]) {
+        atomicAdd(&luminos[k], s_lum[k]);
+        atomicAdd(&lumdev[k], s_dev[k]);
+        atomicAdd(&lumnum[k], s_num[k]);
+      }
+    }
+  }
+}
+
+// sourcetally.f:24-45: src_energy/src_number (ncell, ng), cell fastest.
+__global__ void sourcetally_kernel(long long npart, const slg_packet* __restrict__ prt,
+                                   const int32_t* __restrict__ isvacant, int nx, int ng,
+                                   const double* __restrict__ xarr, const double* __restrict__ wl,
+                                   double* __restrict__ src_energy, int32_t* __restrict__ src_number,
+                                   int* __restrict__ err) {
+  for (long long ip = (long long)blockIdx.x * blockDim.x + threadIdx.x; ip < npart;
+       ip += (long long)gridDim.x * blockDim.x) {
+    if (isvacant[ip]) continue;
+    const slg_packet* q = prt + ip;
+    const int ig = binsrch(q->wl, wl, ng + 1, false);
+    const int ic = binsrch(q->x, xarr, nx + 1, false);
+    if (ic < 1 || ic > nx) { atomicOr(err, 1); continue; }
+    if (ig < 1 || ig > ng) { atomicOr(err, 2); continue; }
+    atomicAdd(&src_energy[(size_t)(ig - 1) * nx + (ic - 1)], q->e);
+    atomicAdd(&src_number[(size_t)(ig - 1) * nx + (ic - 1)], 1);
+  }
+}
+
+}  // namespace
+
+int launch_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packet* prt, int32_t* isvacant,
+                            int64_t npart, uint64_t seed, slg_transport_out* out, uint64_t* d_trace_hash,
+                            int32_t* d_trace_nstep) {
+  const int nx = ctx->nx, ng = ctx->ng;
+  cudaStream_t st = ctx->stream;
+  int rc = build_cell_tables(ctx, in);
+  if (rc) return rc;
+  cudaMemsetAsync(out->tally, 0, sizeof(double) * nx, st);
+  cudaMemsetAsync(out->jrad, 0, sizeof(double) * (size_t)nx * ng, st);
+  cudaMemsetAsync(out->eamp, 0, sizeof(double) * nx, st);
+  if (in->dogrdtally && out->methodswap) cudaMemsetAsync(out->methodswap, 0, sizeof(int32_t) * nx, st);
+  cudaMemsetAsync(ctx->d_acc, 0, sizeof(TransportAcc), st);
+  cudaMemsetAsync(&ctx->d_acc->ierr_key, 0xff, sizeof(unsigned long long), st);
+  TrnArgs A;
+  A.nx = nx; A.ng = ng; A.nep = ctx->nep; A.nepg = ctx->nepg;
+  A.xarr = ctx->d_xarr; A.vxarr = ctx->d_vxarr; A.divv = ctx->d_divv; A.wl = ctx->d_wl; A.wlinv = ctx->d_wlinv;
+  A.tempinv = in->tempinv; A.sig = in->sig; A.capgrey = in->capgrey; A.emitprob = in->emitprob;
+  A.opaclump = in->opaclump; A.cap = in->cap; A.tauddmc = in->tauddmc; A.taulump = in->taulump;
+  A.puretran = in->puretran; A.noampfact = in->noampfact; A.errorfatal = in->errorfatal;
+  A.thm_aniso = in->thm_aniso; A.dogrdtally = in->dogrdtally; A.max_steps = in->max_steps;
+  A.T = ctx->tables; A.prt = prt; A.isvacant = isvacant; A.npart = npart; A.seed = seed;
+  A.tally = out->tally; A.jrad = out->jrad; A.eamp = out->eamp; A.methodswap = out->methodswap;
+  A.acc = ctx->d_acc; A.trace_hash = d_trace_hash; A.trace_nstep = d_trace_nstep;
+  const int block = TRN_BLOCK;
+  int per_sm = ctx->trn_grid_per_sm > 0 ? ctx->trn_grid_per_sm : 0;
+  if (per_sm == 0) {
+    int occ = 0;
+    if (d_trace_hash) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_kernel<true>, block, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_kernel<false>, block, 0);
+    per_sm = occ > 0 ? occ : 4;
+  }
+  long long nblk = (long long)ctx->num_sms * per_sm;
+  const long long need = (npart + block - 1) / block;
+  if (need < nblk) nblk = need > 0 ? need : 1;
+  if (d_trace_hash)
+    particle_advance_kernel<true><<<(unsigned)nblk, block, 0, st>>>(A);
+  else
+    particle_advance_kernel<false><<<(unsigned)nblk, block, 0, st>>>(A);
+  if ((rc = cuda_check(ctx, cudaGetLastError(), "particle_advance launch"))) return rc;
+  return cuda_check(ctx, cudaMemcpyAsync(ctx->h_acc, ctx->d_acc, sizeof(TransportAcc), cudaMemcpyDeviceToHost, st),
+                    "transport counters download");
+}
+
+// After the stream has reached the end of launch_particle_advance: fold the
+// device counters into *out (totals accumulate like totalsmod.f).
+int finish_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_transport_out* out) {
+  (void)in;
+  const TransportAcc& a = *ctx->h_acc;
+  out->tot_evelo += a.evelo;
+  out->tot_eout += a.eout;
+  out->tot_sflux += a.sflux;
+  out->npckt = (int64_t)a.npckt;
+  out->nflux = (int64_t)a.nflux;
+  out->nstepimc = (int64_t)a.nimc;
+  out->nstepddmc = (int64_t)a.nddmc;
+  out->nmethodswap = (int64_t)a.nswap;
+  out->nstepmax = (int64_t)a.nmax;
+  for (int k = 0; k < 11; ++k) out->ndist[k] = (int64_t)a.ndist[k];
+  out->nposwarn = (int64_t)a.nwarn;
+  if (a.ierr_key != ~0ull) {
+    out->ierr = (int32_t)(a.ierr_key & 0xffffffffu);
+    out->ierr_part = (int32_t)(a.ierr_key >> 32);
+  } else {
+    out->ierr = 0;
+    out->ierr_part = 0;
+  }
+  return out->ierr;
+}
+
+int launch_fluxtally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, int32_t* isvacant, int flx_ng,
+                     const double* flx_wl, double* luminos, double* lumdev, int32_t* lumnum) {
+  cudaStream_t st = ctx->stream;
+  cudaMemsetAsync(luminos, 0, sizeof(double) * flx_ng, st);
+  cudaMemsetAsync(lumdev, 0, sizeof(double) * flx_ng, st);
+  cudaMemsetAsync(lumnum, 0, sizeof(int32_t) * flx_ng, st);
+  const size_t shm = (size_t)flx_ng * (2 * sizeof(double) + sizeof(int));
+  const int use_smem = shm <= 96 * 1024;
+  if (use_smem) cudaFuncSetAttribute(fluxtally_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  long long nb = (npart + 255) / 256;
+  const long long cap = (long long)ctx->num_sms * 4;
+  if (nb > cap) nb = cap;
+  if (nb < 1) nb = 1;
+  fluxtally_kernel<<<(unsigned)nb, 256, use_smem ? shm : 0, st>>>(npart, prt, isvacant, flx_ng, flx_wl, luminos,
+                                                                  lumdev, lumnum, use_smem);
+  return cuda_check(ctx, cudaGetLastError(), "fluxtally launch");
+}
+
+int launch_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, const int32_t* isvacant,
+                       double* src_energy, int32_t* src_number) {
+  cudaStream_t st = ctx->stream;
+  const size_t n = (size_t)ctx->nx * ctx->ng;
+  int* d_err = (int*)scratch(ctx, 21, sizeof(int) * 2);
+  if (!d_err) return SLG_ERR_OOM;
+  cudaMemsetAsync(d_err, 0, sizeof(int) * 2, st);
+  cudaMemsetAsync(src_energy, 0, sizeof(double) * n, st);
+  cudaMemsetAsync(src_number, 0, sizeof(int32_t) * n, st);
+  long long nb = (npart + 255) / 256;
+  const long long cap = (long long)ctx->num_sms * 8;
+  if (nb > cap) nb = cap;
+  if (nb < 1) nb = 1;
+  sourcetally_kernel<<<(unsigned)nb, 256, 0, st>>>(npart, prt, isvacant, ctx->nx, ctx->ng, ctx->d_xarr, ctx->d_wl,
+                                                   src_energy, src_number, d_err);
+  return cuda_check(ctx, cudaGetLastError(), "sourcetally launch");
+}
+
+int sourcetally_error(slg_ctx* ctx, int* err) {
+  int* d_err = (int*)scratch(ctx, 21, sizeof(int) * 2);
+  int h = 0;
+  int rc = cuda_check(ctx, cudaMemcpyAsync(&h, d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "err");
+  if (rc) return rc;
+  rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+  *err = h;
+  return rc;
+}
+
+}  // namespace slg

@@ -1,0 +1,589 @@
+// transport_impl.cuh -- device bodies of one IMC event (transport11) and one
+// DDMC event (diffusion11) on a particle held in registers.
+//
+// Reference: TRANSPORT1/transport11.f90:3-515, TRANSPORT1/diffusion11.f90:3-633,
+// GRID/emitgroup.f:3-54.  Arithmetic follows the Fortran expression order;
+// the resolved-group scans of diffusion11 and the within-bin walk of
+// emitgroup are binary searches over the per-cell running sums built by
+// cell_tables_kernel (grid.cu), which hold the very partial sums the scans
+// would form.
+#pragma once
+#include "slg_device.cuh"
+#include "slg_internal.h"
+
+namespace slg {
+
+struct TrnArgs {
+  int nx, ng, nep, nepg;
+  const double *xarr, *vxarr, *divv, *wl, *wlinv, *tempinv, *sig, *capgrey, *emitprob, *opaclump;
+  const float* cap;
+  double tauddmc, taulump;
+  int puretran, noampfact, errorfatal, thm_aniso, dogrdtally;
+  long long max_steps;
+  CellTables T;
+  slg_packet* prt;
+  int32_t* isvacant;
+  long long npart;
+  uint64_t seed;
+  double *tally, *jrad, *eamp;
+  int32_t* methodswap;
+  TransportAcc* acc;
+  uint64_t* trace_hash;
+  int32_t* trace_nstep;
+};
+
+struct Ptcl {
+  double x, mu, e, e0, wl, vx, dist;
+  int ix, ig, itype, stat, idist;  // ic == ix (1-D, no void cells)
+};
+
+// first position q in [0,n) with a[q] > r, else n-1 (the last position a
+// linear scan visits)
+__device__ inline int first_gt(const double* __restrict__ a, int n, double r) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] > r) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo < n ? lo : n - 1;
+}
+
+__device__ inline double CAPd(const TrnArgs& A, int ig, int ic) {
+  return (double)__ldg(A.cap + (size_t)(ic - 1) * A.ng + (ig - 1));
+}
+__device__ inline double dxd(const TrnArgs& A, int i) { return A.xarr[i] - A.xarr[i - 1]; }
+
+// GRID/emitgroup.f:3-54 (LTE); ic 1-based.
+__device__ inline int emitgroup_dev(const TrnArgs& A, double r, int ic) {
+  const double* ep = A.emitprob + (size_t)A.nep * (ic - 1);
+  const double r1 = r * A.capgrey[ic - 1];
+  int iep = binsrch(r1, ep, A.nep, true);
+  if (iep < 0) iep = 0;
+  const int ig0 = iep * A.nepg + 1;
+  const int igp1 = min(ig0 + A.nepg - 1, A.ng);
+  if (ig0 > igp1 - 1) return min(ig0, A.ng);
+  const double* ec = A.T.emitcum + (size_t)(ic - 1) * A.ng + (ig0 - 1);
+  const int n = igp1 - ig0;  // candidates ig0 .. igp1-1
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (ec[mid] > r1) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo < n ? ig0 + lo : igp1;
+}
+
+// One IMC event, transport11.f90:3-515.
+template <class RNG>
+__device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, double& eraddens, double& eamp,
+                                       double& jrad, double& totevelo, int& ierr) {
+  int& ix = p.ix;
+  int& ig = p.ig;
+  double& x = p.x;
+  double& mu = p.mu;
+  double& e = p.e;
+  double& e0 = p.e0;
+  double& wl = p.wl;
+  double& vx = p.vx;
+  const int ic = ix;
+  ierr = 0;
+  eraddens = 0.0;
+  eamp = 0.0;
+  jrad = 0.0;
+  double elabfact = 1.0 - mu * vx * cinv;
+  const double elabfactold = elabfact;
+  const double* sc = A.T.scal + (size_t)SCAL_N * (ic - 1);
+  const double far = sc[SCAL_FAR];
+  const double Xa = A.xarr[ix - 1], Xb = A.xarr[ix];
+  double db;
+  int ixnext;
+  if (ix == 1 || mu >= -sqrt(1.0 - sq(Xa / x))) {
+    db = fabs(sqrt(sq(Xb) - (1.0 - sq(mu)) * sq(x)) - mu * x);
+    ixnext = ix + 1;
+  } else {
+    db = fabs(sqrt(sq(Xa) - (1.0 - sq(mu)) * sq(x)) + mu * x);
+    ixnext = ix - 1;
+  }
+  if (db != db) { ierr = 1; return; }
+  const double sigc = A.sig[ic - 1];
+  double dthm, dcol, ddop, r1, r2, help;
+  if (sigc > 0.0) {
+    r1 = rng.draw();
+    dthm = -log(r1) / (elabfact * sigc);
+  } else {
+    dthm = far;
+  }
+  const double capc = CAPd(A, ig, ic);
+  if (capc <= 0.0) {
+    dcol = far;
+  } else {
+    r1 = rng.draw();
+    dcol = -log(r1) / (elabfact * capc);
+  }
+  const double dvdr = sc[SCAL_DVDR];
+  const double vhelp = A.vxarr[ix - 1] - dvdr * Xa;
+  if (fabs(vx - vhelp) / pc_c >= 0.1) {
+    // Newton-Raphson Doppler distance (transport11.f90:159-199)
+    const double epstol = 1e-3;
+    int it = 0;
+    double shelp = db;
+    double xhelp = sqrt(sq(x) + sq(shelp) + 2.0 * shelp * x * mu);
+    double muhelp = (mu * x + shelp) / xhelp;
+    double phi = dvdr * mu * x - pc_c * (1.0 - wl * A.wlinv[ig]) + vhelp * muhelp + dvdr * shelp;
+    double dphi = dvdr + vhelp * (1.0 - sq(muhelp)) / xhelp;
+    ddop = shelp - phi / dphi;
+    while ((fabs(ddop - shelp) > ddop * epstol) && it < 100) {
+      it = it + 1;
+      shelp = ddop;
+      xhelp = sqrt(sq(x) + sq(shelp) + 2.0 * shelp * x * mu);
+      muhelp = (mu * x + shelp) / xhelp;
+      if (dvdr > 0.0 && ig < A.ng) {
+        phi = dvdr * mu * x - pc_c * (1.0 - wl * A.wlinv[ig]) + vhelp * muhelp + dvdr * shelp;
+      } else if (dvdr < 0.0 && ig > 1) {
+        phi = dvdr * mu * x - pc_c * (1.0 - wl * A.wlinv[ig - 1]) + vhelp * muhelp + dvdr * shelp;
+      } else {
+        ddop = far;
+        break;
+      }
+      dphi = dvdr + vhelp * (1.0 - sq(muhelp)) / xhelp;
+      ddop = shelp - phi / dphi;
+    }
+    if (ddop <= 0.0 || it == 100) ddop = far;
+  } else {
+    if (dvdr > 0.0 && ig < A.ng) {
+      ddop = 3.0 * pc_c / A.divv[ix - 1] * (elabfact - wl * A.wlinv[ig]);
+    } else if (dvdr < 0.0 && ig > 1) {
+      ddop = 3.0 * pc_c / A.divv[ix - 1] * (elabfact - wl * A.wlinv[ig - 1]);
+    } else {
+      ddop = far;
+    }
+    if (ddop < 0.0) ddop = far;
+  }
+  // minloc over [dcol,dthm,ddop,db]; ties resolve to the first
+  double d = dcol;
+  int im = 1;
+  if (dthm < d) { d = dthm; im = 2; }
+  if (ddop < d) { d = ddop; im = 3; }
+  if (db < d) { d = db; im = 4; }
+  p.idist = im;
+  p.dist = d;
+  if (dcol != dcol || dthm != dthm || ddop != ddop) { ierr = 3; return; }
+  if (d < 0.0) { ierr = 4; return; }
+  const double xold = x;
+  x = sqrt(sq(x) + sq(d) + 2.0 * d * x * mu);
+  vx = (A.vxarr[ix - 1] * (Xb - x) + A.vxarr[ix] * (x - Xa)) / dxd(A, ix);
+  if (x == 0.0) mu = 1.0;
+  else mu = (xold * mu + d) / x;
+  eraddens = e * sq(elabfact) * d * cinv;
+  jrad = pc_c * eraddens;
+  elabfact = 1.0 - mu * vx * cinv;
+  if (x < A.xarr[0]) {
+    x = A.xarr[0];
+    vx = A.vxarr[0];
+    ix = 1;
+    r1 = rng.draw();
+    mu = 1.0 - r1;
+    return;
+  }
+  if (d == dthm || d == dcol) {
+    r1 = rng.draw();
+    if (d == dthm && A.thm_aniso) {
+      // transport11.f90:259-281 (experimental)
+      const double s = sqrt(1.0 + 16.0 * pow(r1 - 0.5, 2.0));
+      const double mutemp = pow(4.0 * r1 - 2.0 + s, 1.0 / 3.0) - pow(s - (4.0 - 2.0 * r1), 1.0 / 3.0);
+      const double mh = mutemp;
+      const double B = 2.0 * mutemp * mh;
+      const double Cc = sq(mutemp) + sq(mh) - 1.0;
+      const double munew1 = (-B + sqrt(sq(B) - 4.0 * Cc)) / 2.0;
+      const double munew2 = (-B - sqrt(sq(B) - 4.0 * Cc)) / 2.0;
+      const bool ok1 = munew1 <= 1.0 && munew1 >= -1.0, ok2 = munew2 <= 1.0 && munew2 >= -1.0;
+      if (ok1 && ok2) mu = r1 < 0.5 ? munew1 : munew2;
+      else if (ok1) mu = munew1;
+      else if (ok2) mu = munew2;
+      else mu = 1.0 - 2.0 * r1;
+    } else {
+      mu = 1.0 - 2.0 * r1;
+    }
+    mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
+  } else if (d == db) {
+    if (mu >= 0.0 && ix == A.nx) { p.stat = 1; return; }
+  }
+  if (d == dthm) {
+    wl = wl * (1.0 - mu * vx * cinv) / elabfact;
+    help = elabfact / (1.0 - mu * vx * cinv);
+    totevelo = totevelo + e * (1.0 - help);
+    e = e * help;
+    e0 = e0 * help;
+  } else if (d == dcol) {
+    r1 = rng.draw();  // drawn and unused in the reference (transport11.f90:313)
+    help = elabfact / (1.0 - mu * vx * cinv);
+    totevelo = totevelo + e * (1.0 - help);
+    e = e * help;
+    e0 = e0 * help;
+    if (A.ng != 1) {
+      r1 = rng.draw();
+      ig = emitgroup_dev(A, r1, ic);
+      if (((sigc + CAPd(A, ig, ic)) * dxd(A, ix) >= A.tauddmc) && !A.puretran) p.itype = 2;
+    }
+    if (p.itype == 2) {
+      totevelo = totevelo + e * vx * mu * cinv;
+      e = e * (1.0 - vx * mu * cinv);
+      e0 = e0 * (1.0 - vx * mu * cinv);
+    } else {
+      r1 = rng.draw();
+      wl = 1.0 / ((1.0 - r1) * A.wlinv[ig - 1] + r1 * A.wlinv[ig]);
+      wl = wl * (1.0 - vx * mu * cinv);
+    }
+  } else if (d == db && ixnext > ix) {
+    const int l = ix + 1;
+    const double capl = CAPd(A, ig, l), sigl = A.sig[l - 1];
+    const double dxl = dxd(A, ix + 1);
+    if ((sigl + capl) * dxl < A.tauddmc || A.puretran) {
+      x = A.xarr[ix];
+      vx = A.vxarr[ix];
+      ix = ix + 1;
+    } else {
+      mu = (mu - vx * cinv) / (1.0 - vx * mu * cinv);
+      help = (capl + sigl) * dxl;
+      help = 4.0 / (3.0 * help + 6.0 * pc_dext);
+      r1 = rng.draw();
+      if (r1 < help * (1.0 + 1.5 * fabs(mu))) {
+        p.itype = 2;
+        totevelo = totevelo + e * (1.0 - elabfact);
+        e = e * elabfact;
+        e0 = e0 * elabfact;
+        wl = wl / elabfact;
+        ix = ix + 1;
+      } else {
+        r1 = rng.draw();
+        r2 = rng.draw();
+        mu = -(r1 > r2 ? r1 : r2);
+        mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
+        x = A.xarr[ix];
+        vx = A.vxarr[ix];
+      }
+    }
+  } else if (d == db) {
+    const int l = ix - 1;
+    const double capl = CAPd(A, ig, l), sigl = A.sig[l - 1];
+    const double dxl = dxd(A, ix - 1);
+    if ((sigl + capl) * dxl < A.tauddmc || A.puretran) {
+      x = A.xarr[ix - 1];
+      vx = A.vxarr[ix - 1];
+      ix = ix - 1;
+    } else {
+      mu = (mu - vx * cinv) / (1.0 - vx * mu * cinv);
+      if (!A.noampfact && mu < 0.0) {
+        help = 1.0 / fabs(mu);
+        help = help < 100.0 ? help : 100.0;
+        totevelo = totevelo - e * 2.0 * (0.55 * help - 1.25 * fabs(mu)) * vx * cinv;
+        const double hm2 = help - 2.0;
+        eamp = e * 2.0 * 0.55 * (hm2 > 0.0 ? hm2 : 0.0) * vx * cinv;
+        help = help < 2.0 ? help : 2.0;
+        e0 = e0 * (1.0 + 2.0 * (0.55 * help - 1.25 * fabs(mu)) * vx * cinv);
+        e = e * (1.0 + 2.0 * (0.55 * help - 1.25 * fabs(mu)) * vx * cinv);
+      }
+      help = (capl + sigl) * dxl;
+      help = 4.0 / (3.0 * help + 6.0 * pc_dext);
+      r1 = rng.draw();
+      if (r1 < help * (1.0 + 1.5 * fabs(mu))) {
+        p.itype = 2;
+        totevelo = totevelo + e * (1.0 - elabfact);
+        e = e * elabfact;
+        e0 = e0 * elabfact;
+        wl = wl / elabfact;
+        ix = ix - 1;
+      } else {
+        r1 = rng.draw();
+        r2 = rng.draw();
+        mu = r1 > r2 ? r1 : r2;
+        mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
+        x = A.xarr[ix - 1];
+        vx = A.vxarr[ix - 1];
+      }
+    }
+  } else if (d == ddop) {
+    if (dvdr > 0.0) {
+      if (ig < A.ng) {
+        ig = ig + 1;
+        wl = (A.wl[ig - 1] + 1e-6 * (A.wl[ig] - A.wl[ig - 1])) * elabfactold;
+      } else {
+        r1 = rng.draw();
+        wl = 1.0 / (r1 * A.wlinv[A.ng] + (1.0 - r1) * A.wlinv[A.ng - 1]);
+        wl = wl * elabfact;
+      }
+    } else if (dvdr < 0.0) {
+      if (ig > 1) {
+        wl = (A.wl[ig - 1] + 1e-6 * (A.wl[ig - 2] - A.wl[ig - 1])) * elabfactold;
+        ig = ig - 1;
+      } else {
+        r1 = rng.draw();
+        wl = 1.0 / (r1 * A.wlinv[0] + (1.0 - r1) * A.wlinv[1]);
+        wl = wl * elabfact;
+      }
+    }
+    if (((sigc + CAPd(A, ig, ic)) * dxd(A, ix) >= A.tauddmc) && !A.puretran) {
+      p.itype = 2;
+      totevelo = totevelo + e * vx * mu * cinv;
+      e = e * elabfact;
+      e0 = e0 * elabfact;
+      wl = wl / elabfact;
+    }
+  } else {
+    ierr = 17;
+  }
+}
+
+// One DDMC event, diffusion11.f90:3-633 (LTE).
+template <class RNG>
+__device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, double& eraddens, double& jrad,
+                                       double& totevelo, int& ierr) {
+  const int ng = A.ng;
+  int& ix = p.ix;
+  int& ig = p.ig;
+  double& x = p.x;
+  double& mu = p.mu;
+  double& e = p.e;
+  double& e0 = p.e0;
+  double& wl = p.wl;
+  double& vx = p.vx;
+  const int ic = ix;
+  ierr = 0;
+  eraddens = 0.0;
+  jrad = 0.0;
+  const double Xa = A.xarr[ix - 1], Xb = A.xarr[ix];
+  const double dist = Xb - Xa;
+  const size_t off = (size_t)(ic - 1) * ng;
+  const double* sc = A.T.scal + (size_t)SCAL_N * (ic - 1);
+  const double dx3 = sc[SCAL_DX3];
+  const double speclump = sc[SCAL_SPECLUMP];
+  const double capgreyinv = sc[SCAL_CAPGREYINV];
+  const double sigc = A.sig[ic - 1];
+  const double capc = CAPd(A, ig, ic);
+  const double tinv = A.tempinv[ic - 1];
+  const double divv = A.divv[ix - 1];
+  const int glump = (capc * dist >= A.taulump) ? A.T.nlump[ic - 1] : 0;
+  if ((sigc + capc) * dist < A.tauddmc) { ierr = 100; return; }
+  double emitlump, caplump, doplump, r1, r2, help;
+  double o1, o2;
+  if (glump > 0) {
+    emitlump = sc[SCAL_EMITLUMP];
+    caplump = sc[SCAL_CAPLUMP];
+    doplump = sc[SCAL_DOPLUMP];
+    const double* OL = A.opaclump + (size_t)11 * (ic - 1);
+    o1 = OL[0];
+    o2 = OL[1];
+  } else {
+    emitlump = specint0(tinv, A.wlinv, ig) * capgreyinv * capc;
+    caplump = capc;
+    const double spec_ig = A.T.specarr[off + ig - 1];
+    if (ig != ng && divv >= 0.0) {
+      doplump = dopspeccalc(tinv, A.wlinv, ig) * divv / (spec_ig * 3.0 * pc_c);
+    } else if (ig != 1 && divv < 0.0) {
+      doplump = -1.0 * dopspeccalc(tinv, A.wlinv, ig - 1) * divv / (spec_ig * 3.0 * pc_c);
+    } else {
+      doplump = 0.0;
+    }
+    if (ix == 1) {
+      o1 = 0.0;
+    } else {
+      const int l = ix - 1;
+      const double capl = CAPd(A, ig, l), sigl = A.sig[l - 1];
+      const double dxl = Xa - A.xarr[ix - 2];
+      if ((capl + sigl) * dxl < A.tauddmc) {
+        const double mfphelp = (capc + sigc) * dist;
+        const double ppl = 4.0 / (3.0 * mfphelp + 6.0 * pc_dext);
+        o1 = 1.5 * ppl * sq(Xa) / dx3;
+      } else {
+        const double mfphelp = (sigc + capc) * dist + (sigl + capl) * dxl;
+        o1 = 2.0 * sq(Xa) / (mfphelp * dx3);
+      }
+    }
+    bool lhelp;
+    double capl = 0.0, sigl = 0.0, dxl = 0.0;
+    if (ix == A.nx) {
+      lhelp = true;
+    } else {
+      const int l = ix + 1;
+      capl = CAPd(A, ig, l);
+      sigl = A.sig[l - 1];
+      dxl = A.xarr[ix + 1] - Xb;
+      lhelp = (capl + sigl) * dxl < A.tauddmc;
+    }
+    if (lhelp) {
+      const double mfphelp = (capc + sigc) * dist;
+      const double ppr = 4.0 / (3.0 * mfphelp + 6.0 * pc_dext);
+      o2 = 1.5 * ppr * sq(Xb) / dx3;
+    } else {
+      const double mfphelp = (sigc + capc) * dist + (sigl + capl) * dxl;
+      o2 = 2.0 * sq(Xb) / (mfphelp * dx3);
+    }
+  }
+  double denom = (o1 + o2) + (1.0 - emitlump) * caplump + doplump;
+  denom = 1.0 / denom;
+  r1 = rng.draw();
+  const double ddmct = fabs(log(r1) * denom * cinv);
+  eraddens = e * ddmct;
+  jrad = pc_c * eraddens;
+  r1 = rng.draw();
+  const double pl0 = o1 * denom, pl1 = o2 * denom;
+  const double pa = 0.0;
+  const double pdop = doplump * denom;
+  const int16_t* glumps = A.T.glumps + off;
+  int iiig;
+  if (r1 >= pa && r1 < pa + pdop) {
+    // Doppler shift (:283-355)
+    if (glump == 0) {
+      iiig = ig;
+    } else {
+      r1 = rng.draw();
+      const int q = first_gt(A.T.cdf_dop + off, glump, r1);
+      iiig = divv >= 0.0 ? glumps[q] : glumps[glump - 1 - q];
+    }
+    if (divv >= 0.0) {
+      ig = iiig + 1;
+      wl = A.wl[ig - 1];
+      ig = ig < ng ? ig : ng;
+    } else {
+      ig = iiig - 1;
+      wl = A.wl[ig];
+      ig = ig > 1 ? ig : 1;
+    }
+    if ((sigc + CAPd(A, ig, ic)) * dist < A.tauddmc) {
+      p.itype = 1;
+      r1 = rng.draw();
+      mu = 1.0 - 2.0 * r1;
+      r1 = rng.draw();
+      x = pow(r1 * cube(Xb) + (1.0 - r1) * cube(Xa), third_r4);
+      x = x < Xb ? x : Xb;
+      x = x > Xa ? x : Xa;
+      vx = (A.vxarr[ix - 1] * (Xb - x) + A.vxarr[ix] * (x - Xa)) / dist;
+      mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
+      wl = wl * (1.0 - vx * mu * cinv);
+      help = 1.0 / (1.0 - vx * mu * cinv);
+      totevelo = totevelo + e * (1.0 - help);
+      e = e * help;
+      e0 = e0 * help;
+    }
+  } else if (r1 >= pa + pdop && r1 < pa + pdop + pl0) {
+    // left leakage (:358-430)
+    p.idist = -3;
+    if (ix == 1) return;
+    const int l = ix - 1;
+    if (glump == 0) {
+      iiig = ig;
+    } else {
+      r1 = rng.draw();
+      iiig = glumps[first_gt(A.T.cdf_left + off, glump, r1)];
+    }
+    const double dxl = Xa - A.xarr[ix - 2];
+    if ((A.sig[l - 1] + CAPd(A, iiig, l)) * dxl < A.tauddmc) {
+      p.itype = 1;
+      r1 = rng.draw();
+      wl = 1.0 / (r1 * A.wlinv[iiig] + (1.0 - r1) * A.wlinv[iiig - 1]);
+      x = Xa;
+      vx = A.vxarr[ix - 1];
+      r1 = rng.draw();
+      r2 = rng.draw();
+      mu = -(r1 > r2 ? r1 : r2);
+      mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
+      help = 1.0 / (1.0 - vx * mu * cinv);
+      totevelo = totevelo + e * (1.0 - help);
+      e = e * help;
+      e0 = e0 * help;
+      wl = wl * (1.0 - vx * mu * cinv);
+    }
+    ix = ix - 1;
+    ig = iiig;
+  } else if (r1 >= pa + pdop + pl0 && r1 < pa + pdop + (pl0 + pl1)) {
+    // right leakage (:434-545)
+    p.idist = -4;
+    if (ix == A.nx) {
+      p.stat = 1;
+      r1 = rng.draw();
+      r2 = rng.draw();
+      mu = r1 > r2 ? r1 : r2;
+      if (glump != 0) {
+        r1 = rng.draw();
+        ig = glumps[first_gt(A.T.cdf_right + off, glump, r1)];
+      }
+      r1 = rng.draw();
+      wl = 1.0 / (r1 * A.wlinv[ig] + (1.0 - r1) * A.wlinv[ig - 1]);
+      x = A.xarr[A.nx];
+      vx = A.vxarr[A.nx];
+      mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
+      mu = mu < 1.0 ? mu : 1.0;
+      help = 1.0 / (1.0 - mu * vx * cinv);
+      totevelo = totevelo + e * (1.0 - help);
+      wl = wl / help;
+      e = e * help;
+      e0 = e0 * help;
+      return;
+    }
+    const int l = ix + 1;
+    if (glump == 0) {
+      iiig = ig;
+    } else {
+      r1 = rng.draw();
+      iiig = glumps[first_gt(A.T.cdf_right + off, glump, r1)];
+    }
+    const double dxl = A.xarr[ix + 1] - Xb;
+    if ((A.sig[l - 1] + CAPd(A, iiig, l)) * dxl < A.tauddmc) {
+      p.itype = 1;
+      r1 = rng.draw();
+      wl = 1.0 / (r1 * A.wlinv[iiig] + (1.0 - r1) * A.wlinv[iiig - 1]);
+      x = Xb;
+      vx = A.vxarr[ix];
+      r1 = rng.draw();
+      r2 = rng.draw();
+      mu = r1 > r2 ? r1 : r2;
+      mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
+      help = 1.0 / (1.0 - vx * mu * cinv);
+      totevelo = totevelo + e * (1.0 - help);
+      e = e * help;
+      e0 = e0 * help;
+      wl = wl * (1.0 - vx * mu * cinv);
+    }
+    ix = ix + 1;
+    ig = iiig;
+  } else {
+    // effective scattering (:549-620)
+    p.idist = -2;
+    if (glump == ng) { ierr = 102; return; }
+    if (glump == 0) {
+      r1 = rng.draw();
+      iiig = emitgroup_dev(A, r1, ic);
+    } else {
+      r1 = rng.draw();
+      const int q = first_gt(A.T.cdf_scat + off, ng - glump, r1);
+      iiig = glumps[ng - 1 - q];
+    }
+    ig = iiig;
+    if ((sigc + CAPd(A, ig, ic)) * dist < A.tauddmc) {
+      p.itype = 1;
+      r1 = rng.draw();
+      wl = 1.0 / ((1.0 - r1) * A.wlinv[ig - 1] + r1 * A.wlinv[ig]);
+      r1 = rng.draw();
+      mu = 1.0 - 2.0 * r1;
+      r1 = rng.draw();
+      x = pow(r1 * cube(Xb) + (1.0 - r1) * cube(Xa), third_r4);
+      x = x < Xb ? x : Xb;
+      x = x > Xa ? x : Xa;
+      vx = (A.vxarr[ix - 1] * (Xb - x) + A.vxarr[ix] * (x - Xa)) / dist;
+      mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
+      help = 1.0 / (1.0 - vx * mu * cinv);
+      totevelo = totevelo + e * (1.0 - help);
+      e = e * help;
+      e0 = e0 * help;
+      wl = wl * (1.0 - vx * mu * cinv);
+    }
+  }
+  if (x < A.xarr[0]) { p.stat = 2; return; }
+  const double dv = A.divv[ix - 1];
+  totevelo = totevelo + e * (1.0 - exp(-dv * ddmct / 3.0));
+  e = e * exp(-dv * ddmct / 3.0);
+  e0 = e0 * exp(-dv * ddmct / 3.0);
+}
+
+}  // namespace slg

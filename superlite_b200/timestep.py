@@ -1,0 +1,129 @@
+"""Device-resident driver of one SuperLite hot-path timestep.
+
+Mirrors the order of the reference's iteration (superlite.f90:157-222):
+physical_opacity -> opacity_planckmean/rossmean (gas_update.f:147-152) ->
+leakage_opacity + emission_probability (superlite.f90:177-178) ->
+sourcetally (:193) -> particle_advance (:202) -> fluxtally (:219).
+
+All buffers are allocated once; one ``step()`` queues only libslg kernels on
+the context's stream (plus one device-to-device restore of the source
+particles, which stands in for the source generation that precedes the hot
+path in the reference).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import capi
+from .api import HotPath, PACKET_DTYPE
+from .capi import ptr
+
+# libslg kernels queued by one step (see DESIGN.md for the list)
+KERNELS_PER_STEP = 15
+
+
+class DeviceTimestep:
+    def __init__(self, hot: HotPath, case, particles: np.ndarray, isvacant: np.ndarray, params,
+                 flx_wl=None, precision=0):
+        self.hot = hot
+        self.params = params
+        self.precision = precision
+        dev = torch.device("cuda", hot.device)
+        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)
+        g = case.gas
+        nc, ng = case.grid.nx, case.groups.ng
+        self.nc, self.ng = nc, ng
+        hot.set_groups(case.groups.wl)
+        hot.set_grid(case.grid.xarr, case.grid.vxarr, case.grid.vol, case.grid.divv)
+        hot.set_atomic_data(g.ion_ni, g.oc.shape[1], case.lines, case.bf_ph1, case.bf_ph2, case.ff_gff)
+        self.gas = dict(temp=f64(g.temp), natom=f64(g.natom), nelec=f64(g.nelec), vol=f64(case.grid.vol),
+                        mass=f64(g.mass), natomfr=f64(g.natomfr), oc=f64(g.oc), ginv=f64(g.ginv))
+        self.tempinv = 1.0 / self.gas["temp"]
+        self.sig = torch.empty(nc, dtype=torch.float64, device=dev)
+        self.cap = torch.empty((nc, ng), dtype=torch.float32, device=dev)
+        self.emiss = torch.empty((nc, ng), dtype=torch.float32, device=dev)
+        self.capgrey = torch.empty(nc, dtype=torch.float64, device=dev)
+        self.capross = torch.empty(nc, dtype=torch.float64, device=dev)
+        self.opaclump = torch.empty((nc, 11), dtype=torch.float64, device=dev)
+        self.emitprob = torch.empty((nc, hot.nep), dtype=torch.float64, device=dev)
+        self.tally = torch.empty(nc, dtype=torch.float64, device=dev)
+        self.jrad = torch.empty((nc, ng), dtype=torch.float64, device=dev)
+        self.eamp = torch.empty(nc, dtype=torch.float64, device=dev)
+        self.mswap = torch.empty(nc, dtype=torch.int32, device=dev)
+        self.src_energy = torch.empty((ng, nc), dtype=torch.float64, device=dev)
+        self.src_number = torch.empty((ng, nc), dtype=torch.int32, device=dev)
+        fw = case.groups.wl if flx_wl is None else flx_wl
+        self.flx_wl = f64(fw)
+        self.flx_ng = len(fw) - 1
+        self.lum = torch.empty(self.flx_ng, dtype=torch.float64, device=dev)
+        self.lumdev = torch.empty_like(self.lum)
+        self.lumnum = torch.empty(self.flx_ng, dtype=torch.int32, device=dev)
+        assert particles.dtype == PACKET_DTYPE
+        raw = torch.as_tensor(particles.view(np.float64).reshape(-1, 8))
+        self.prt0 = raw.to(dev)
+        self.prt = torch.empty_like(self.prt0)
+        self.isv0 = torch.as_tensor(np.ascontiguousarray(isvacant, dtype=np.int32)).to(dev)
+        self.isv = torch.empty_like(self.isv0)
+        self.npart = particles.shape[0]
+        gp = capi.SlgGas(*[ptr(self.gas[k]) for k in ("temp", "natom", "nelec", "vol", "mass", "natomfr", "oc", "ginv")])
+        self._gas = gp
+        self._flags = capi.SlgOpacityFlags(0, 0, 0, 0, 1, 0.0)
+        self._tin = HotPath.transport_in(self.tempinv, self.sig, self.capgrey, self.emitprob, self.opaclump, self.cap,
+                                         params, precision)
+        self._tout = capi.SlgTransportOut(ptr(self.tally), ptr(self.jrad), ptr(self.eamp), ptr(self.mswap), 0.0, 0.0, 0.0)
+        self.stream = torch.cuda.ExternalStream(hot.stream(), device=dev)
+
+    def _chk(self, rc):
+        self.hot._check(rc)
+
+    def opacity(self):
+        L, h = self.hot.lib, self.hot.h
+        self._chk(L.slg_dev_physical_opacity(h, C.byref(self._gas), C.byref(self._flags), ptr(self.sig), ptr(self.cap),
+                                             ptr(self.emiss), None))
+        self._chk(L.slg_dev_opacity_means(h, ptr(self.gas["temp"]), ptr(self.sig), ptr(self.cap), ptr(self.capgrey),
+                                          ptr(self.capross)))
+
+    def coefficients(self):
+        L, h = self.hot.lib, self.hot.h
+        p = self.params
+        self._chk(L.slg_dev_leakage_opacity11(h, ptr(self.tempinv), ptr(self.sig), ptr(self.cap), None, p.tauddmc,
+                                              p.taulump, ptr(self.opaclump)))
+        self._chk(L.slg_dev_emission_probability(h, ptr(self.tempinv), ptr(self.cap), ptr(self.capgrey),
+                                                 ptr(self.emitprob)))
+
+    def restore_particles(self):
+        with torch.cuda.stream(self.stream):
+            self.prt.copy_(self.prt0)
+            self.isv.copy_(self.isv0)
+
+    def transport(self, seed):
+        L, h = self.hot.lib, self.hot.h
+        self._chk(L.slg_dev_sourcetally(h, self.npart, ptr(self.prt), ptr(self.isv), ptr(self.src_energy),
+                                        ptr(self.src_number)))
+        self._tout.tot_evelo = self._tout.tot_eout = self._tout.tot_sflux = 0.0
+        self._chk(L.slg_dev_particle_advance(h, C.byref(self._tin), ptr(self.prt), ptr(self.isv), self.npart, seed,
+                                             C.byref(self._tout)))
+
+    def fluxtally(self):
+        L, h = self.hot.lib, self.hot.h
+        self._chk(L.slg_dev_fluxtally(h, self.npart, ptr(self.prt), ptr(self.isv), self.flx_ng, ptr(self.flx_wl),
+                                      ptr(self.lum), ptr(self.lumdev), ptr(self.lumnum)))
+
+    def step(self, seed):
+        """Queue one full timestep; call sync() to complete the transport counters."""
+        self.restore_particles()
+        self.opacity()
+        self.coefficients()
+        self.transport(seed)
+        self.fluxtally()
+
+    def sync(self):
+        self.hot.sync()  # also folds the transport counters into self._tout
+        return self.counters()
+
+    def counters(self):
+        from .api import transport_out_dict
+        return transport_out_dict(self._tout)
