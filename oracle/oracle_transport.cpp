@@ -197,7 +197,9 @@ void transport11(const Ctx& C, orc_packet& p, Ptcl2& p2, double& vx, Rng& rng, d
     }
     mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
   } else if (d == db) {
-    bool lout = mu >= 0.0 && ix == C.nx;
+    // A grazing exit through the outer edge can leave mu a rounding error
+    // below 0; the reference would then index shell nx+1 (guarded here).
+    bool lout = (mu >= 0.0 && ix == C.nx) || ixnext > C.nx;
     if (lout) { p2.stat = 1; return; }
   }
   if (d == dthm) {
@@ -733,6 +735,11 @@ int orc_particle_advance(const orc_trn_in* in, orc_packet* prt, int32_t* isvacan
       p2.ix = orc::binsrch(p.x, in->xarr, nx + 1, false);
       p2.ic = p2.ix;
       p2.ig = orc::binsrch(p.wl, in->wl, ng + 1, false);
+      if (p2.ix < 1 || p2.ig < 1) {  // NaN position or wavelength (library code 1002)
+        if (in->errorfatal && L.ierr == 0) { L.ierr = 1002; L.ierr_part = ipart; }
+        isvacant[ipart - 1] = 1;
+        continue;
+      }
       const double help = C.dx(p2.ix);
       const double tau = (C.SIG(p2.ic) + C.CAP(p2.ig, p2.ic)) * help;
       p2.itype = (in->puretran || tau < in->tauddmc) ? 1 : 2;
@@ -845,6 +852,7 @@ void orc_fluxtally(int64_t npart, const orc_packet* prt, int32_t* isvacant, int 
     const orc_packet& p = prt[ip];
     if (p.x != DBL_MAX) continue;
     int ig = orc::binsrch(p.wl, flx_wl, flx_ng + 1, false);
+    if (ig < 1) continue;  // NaN wavelength (the reference indexes out of bounds)
     luminos[ig - 1] = luminos[ig - 1] + p.e;
     lumdev[ig - 1] = lumdev[ig - 1] + sq(p.e);
     lumnum[ig - 1] = lumnum[ig - 1] + 1;

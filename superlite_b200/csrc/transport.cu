@@ -95,6 +95,13 @@ __global__ void __launch_bounds__(TRN_BLOCK) particle_advance_kernel(const TrnAr
             p.x = x; p.mu = mu; p.e = e; p.e0 = e0; p.wl = wl; p.dist = 0.0;
             p.ix = binsrch(x, A.xarr, A.nx + 1, false);
             p.ig = binsrch(wl, A.wl, A.ng + 1, false);
+            if (p.ix < 1 || p.ig < 1) {  // NaN position or wavelength: library code 1002
+              if (A.errorfatal) atomicMin(&A.acc->ierr_key, ((unsigned long long)(ip + 1) << 32) | 1002u);
+              A.isvacant[ip] = 1;
+              p.ix = 1;
+              p.ig = 1;
+            }
+            const bool bad = A.isvacant[ip] != 0;
             const double help = dxd(A, p.ix);
             const double tau = (A.sig[p.ix - 1] + CAPd(A, p.ig, p.ix)) * help;
             p.itype = (A.puretran || tau < A.tauddmc) ? 1 : 2;
@@ -111,7 +118,7 @@ __global__ void __launch_bounds__(TRN_BLOCK) particle_advance_kernel(const TrnAr
             istep = 0;
             rng.init(A.seed, (uint64_t)ip, 0u);
             if (TRACE) h = 1469598103934665603ull;
-            have = true;
+            have = !bad;
           }
         }
       }
@@ -244,6 +251,7 @@ __global__ void fluxtally_kernel(long long npart, const slg_packet* __restrict__
     if (q->x != DBL_MAX) continue;
     const double e = q->e;
     const int ig = binsrch(q->wl, flx_wl, flx_ng + 1, false);
+    if (ig < 1) continue;  // NaN wavelength
     if (use_smem) {
       atomicAdd(&s_lum[ig - 1], e);
       atomicAdd(&s_dev[ig - 1], sq(e));

@@ -207,7 +207,9 @@ __device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
     }
     mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
   } else if (d == db) {
-    if (mu >= 0.0 && ix == A.nx) { p.stat = 1; return; }
+    // transport11.f90:290-295.  A grazing exit through the outer edge can leave
+    // mu a rounding error below 0; the reference would then index shell nx+1.
+    if ((mu >= 0.0 && ix == A.nx) || ixnext > A.nx) { p.stat = 1; return; }
   }
   if (d == dthm) {
     wl = wl * (1.0 - mu * vx * cinv) / elabfact;
