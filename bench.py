@@ -1,0 +1,380 @@
+"""Benchmark of SuperLite's per-timestep hot path on B200.
+
+Workload (default): one full IMC/DDMC timestep on the physical opacities of
+256 shells x 2000 groups x 5e5 lines, 5e7 source particles, FP64 transport
+(particle_advance.f90 with transport11/diffusion11):
+
+    source particles (GPU)  -> physical_opacity + Planck/Rosseland means
+    -> leakage_opacity11 + emission_probability -> sourcetally
+    -> particle_advance -> fluxtally
+
+metric: particle-steps/s = (IMC + DDMC events, particle_advance.f90:209,219)
+        / wall time of the whole timestep.  The opacity build is reported
+        beside it as cell-group evaluations per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 (torchrun): every rank runs its own independent particles on the same
+grid (weak scaling) and the grid/flux tallies are summed with one NCCL
+all-reduce, as the reference's reduce_gridtally / reduce_fluxtally do.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s"
+T_DAYS = 10.0
+SEED_CASE = 2
+L_BOL = 1e42
+# SURVEY-defined algorithmic bytes of one particle-step (event-based SoA traffic)
+BYTES_PER_STEP = 128.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--npart", type=float, default=5e7)
+    ap.add_argument("--ncell", type=int, default=256)
+    ap.add_argument("--ng", type=int, default=2000)
+    ap.add_argument("--nline", type=float, default=5e5)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=0, help="particles in the CPU-baseline sample (0: auto)")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_case(a):
+    from superlite_b200 import workloads as W
+    return W.opacity_case(ncell=a.ncell, ng=a.ng, nline=int(a.nline), seed=SEED_CASE, t_days=T_DAYS)
+
+
+def config_dict(a, world):
+    return {"workload": "IMC-DDMC timestep on physical LTE opacities (configs[2])",
+            "shells": a.ncell, "groups": a.ng, "lines": int(a.nline), "particles_per_gpu": int(a.npart),
+            "snapshot_days": T_DAYS, "tauddmc": 5.0, "taulump": 10.0, "transport_precision": "fp64",
+            "parallelism": f"particles{world}", "l2": "inputs larger than L2 (particle array 3.2 GB per GPU)"}
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for ln in fh:
+                parts = [x.strip() for x in ln.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(a):
+    import torch
+    from superlite_b200 import HotPath, workloads as W
+    from superlite_b200.timestep import DeviceTimestep
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    case = make_case(a)
+    npart = int(a.npart)
+    params = W.TransportParams()
+    hot = HotPath(local)
+    radtemp = case.gas.temp.copy()
+    ts = DeviceTimestep(hot, case, params, npart=npart)
+    emit, _ = hot.sourceenergy(radtemp, L_BOL)
+    nvol, nnew = hot.sourcenumbers(emit, npart, npart)
+    d_radtemp = ts.gas["temp"]
+    ts.isv.fill_(1)
+    stream = ts.stream
+    seed0 = 1000 * (rank + 1)
+
+    def one_step(k):
+        hot.interior_source(d_radtemp, emit, nvol, ts.prt, ts.isv, seed=seed0 + 2 * k)
+        ts.opacity()
+        ts.coefficients()
+        ts.transport(seed0 + 2 * k + 1)
+        ts.fluxtally()
+
+    # warm-up
+    for k in range(a.warmup):
+        one_step(k)
+        ts.sync()
+    # timed region
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev_op = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    ev_tr = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    steps_total = 0
+    counters = []
+    ev[0].record(stream)
+    for k in range(a.steps):
+        kk = a.warmup + k
+        hot.interior_source(d_radtemp, emit, nvol, ts.prt, ts.isv, seed=seed0 + 2 * kk)
+        ev_op[k][0].record(stream)
+        ts.opacity()
+        ev_op[k][1].record(stream)
+        ts.coefficients()
+        ev_tr[k][0].record(stream)
+        ts.transport(seed0 + 2 * kk + 1)
+        ev_tr[k][1].record(stream)
+        ts.fluxtally()
+        c = ts.sync()
+        counters.append(c)
+        steps_total += c["nstepimc"] + c["nstepddmc"]
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = ev[0].elapsed_time(ev[1])
+    t_op = [s.elapsed_time(e) for s, e in ev_op]
+    t_tr = [s.elapsed_time(e) for s, e in ev_tr]
+    ms_max = ms
+    steps_all = steps_total
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        s = torch.tensor([steps_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(s)
+        steps_all = int(s.item())
+        # reduce_gridtally / reduce_fluxtally (mpimod_mpi.f:797-948): one exchange per step
+        for buf in (ts.tally, ts.jrad, ts.lum, ts.lumdev):
+            dist.all_reduce(buf)
+    value = steps_all / (ms_max / 1e3)
+    peak, peak_kind = measured_peaks()
+    tr_ms = statistics.mean(t_tr)
+    steps_per_launch = steps_total / a.steps
+    achieved = BYTES_PER_STEP * steps_per_launch / (tr_ms / 1e3) / 1e9
+    opac_evals = a.ncell * a.ng / (statistics.mean(t_op) / 1e3)
+    res = {
+        "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, superlite_b200/workloads.py)",
+        "config": config_dict(a, world),
+        "opacity_cell_group_evals_per_s": opac_evals,
+        "transport_particle_steps_per_s": steps_per_launch / (tr_ms / 1e3),
+        "phase_ms": {"opacity+means": statistics.mean(t_op), "particle_advance": tr_ms},
+        "counters_last_step": {k: counters[-1][k] for k in ("npckt", "nflux", "nstepimc", "nstepddmc", "nstepmax",
+                                                            "nmethodswap")},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "particle_advance_kernel",
+                     "basis": f"{BYTES_PER_STEP:.0f} B per particle-step x steps per launch / launch time; "
+                              f"peak {peak_kind}"},
+        "clocks": clocks,
+        "gpu_launches": 20 * a.steps,
+    }
+    if not a.no_e2e:
+        res["e2e"] = run_e2e(a, hot, case, emit, nvol, params, seed0)
+    if rank == 0 and world == 1 and not a.no_cpu:
+        res["cpu_baseline"] = cpu_baseline(a, case, hot, ts, emit, nvol, params)
+    hot.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(res))
+
+
+def run_e2e(a, hot, case, emit, nvol, params, seed0):
+    """Same timestep through the host-pointer C ABI: every phase takes and returns
+    host arrays (module arrays of the Fortran driver), copies included."""
+    from superlite_b200.api import PACKET_DTYPE
+    g = case.gas
+    npart = int(a.npart)
+    prt = np.zeros(npart, dtype=PACKET_DTYPE)
+    isv = np.ones(npart, dtype=np.int32)
+    radtemp = g.temp.copy()
+    tinv = 1.0 / g.temp
+    times, steps = [], 0
+    h2d = d2h = 0
+    for k in range(1 + a.steps):
+        t0 = time.perf_counter()
+        hot.interior_source(radtemp, emit, nvol, prt, isv, seed=seed0 + 7 + k)
+        op = hot.physical_opacity(g.temp, g.natom, g.nelec, case.grid.vol, g.mass, g.natomfr, g.oc, g.ginv)
+        grey, ross = hot.opacity_means(g.temp, op["sig"], op["cap"])
+        ol = hot.leakage_opacity(tinv, op["sig"], op["cap"], tauddmc=params.tauddmc, taulump=params.taulump)
+        ep = hot.emission_probability(tinv, op["cap"], grey)
+        en, num = hot.sourcetally(prt, isv)
+        tables = dict(tempinv=tinv, sig=op["sig"], capgrey=grey, emitprob=ep, opaclump=ol, cap=op["cap"])
+        r = hot.particle_advance(tables, prt, isv, params, seed=seed0 + 11 + k)
+        lum, dev, n = hot.fluxtally(prt, isv, case.groups.wl)
+        t1 = time.perf_counter()
+        if k > 0:  # first pass warms the staging buffers
+            times.append(t1 - t0)
+            steps += r["nstepimc"] + r["nstepddmc"]
+    P = npart * 64 + npart * 4
+    nc, ng = case.grid.nx, case.groups.ng
+    gas_b = (5 * nc + 31 * nc + 2 * g.oc.size) * 8
+    h2d = P * 4 + gas_b + 3 * nc * ng * 4 + nc * 8 * 20
+    d2h = P * 3 + 2 * nc * ng * 4 + nc * ng * 8 * 2 + nc * 8 * 20
+    return {"value": steps / sum(times), "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "steps": a.steps,
+            "path": "host-pointer C ABI per phase (slg_interior_source .. slg_fluxtally)"}
+
+
+def cpu_baseline(a, case, hot, ts, emit, nvol, params, budget_s=20.0):
+    """The oracle (C++ restatement of the Fortran) on the host cores, timed on a
+    bounded sample: the full opacity build once, transport of a particle sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    op = po.physical_opacity(case)
+    grey = po.planckmean(case.groups.wlinv, case.gas.temp, op["cap"])
+    t_opac = time.perf_counter() - t0
+    tinv = 1.0 / case.gas.temp
+    t0 = time.perf_counter()
+    ol = po.leakage_opacity11(case.grid, case.groups.wlinv, tinv, op["sig"], op["cap"], tauddmc=params.tauddmc,
+                              taulump=params.taulump)
+    ep = po.emission_probability(case.groups.wlinv, tinv, op["cap"], grey, case.groups.nep, case.groups.nepg)
+    t_coef = time.perf_counter() - t0
+    tt = po.TransportTables(case.grid, case.groups, tinv, op["sig"], op["cap"], grey, ep, ol, params)
+    npart = int(a.npart)
+    sample = a.cpu_sample or 20000
+    while True:
+        prt, isv, _, _, _ = po.make_source_particles(case.grid, case.groups, case.gas.temp, L_BOL, sample)
+        st = po.rnd_init(cores, 0)
+        t0 = time.perf_counter()
+        r = po.particle_advance(tt, prt, isv, rngmode=0, nthreads=cores, rnd_states=st)
+        dt = time.perf_counter() - t0
+        if dt > 2.0 or a.cpu_sample or sample >= npart:
+            break
+        sample = min(npart, int(sample * max(2.0, budget_s / max(dt, 1e-3) * 0.5)))
+    steps = r["nstepimc"] + r["nstepddmc"]
+    scale = npart / sample
+    t_step = t_opac + t_coef + dt * scale
+    return {"value": steps * scale / t_step, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "sample": f"{sample} particles of the {npart}-particle timestep (mzran, OpenMP static,1), "
+                      f"full opacity build ({t_opac:.2f} s, 1 thread) + coefficients; transport time scaled "
+                      f"by {scale:.1f}",
+            "transport_particle_steps_per_s": steps / dt}
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(a):
+    """The reference's CPU path as restated by the oracle (the Fortran itself has
+    no compiler here), on the host cores, same workload, bounded sample per step."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    from superlite_b200 import workloads as W
+    case = make_case(a)
+    params = W.TransportParams()
+    cores = os.cpu_count() or 1
+    npart = int(a.npart)
+    sample = a.cpu_sample or 40000
+    tinv = 1.0 / case.gas.temp
+    rates, tsteps = [], []
+    for k in range(a.warmup + a.steps):
+        t0 = time.perf_counter()
+        op = po.physical_opacity(case)
+        grey = po.planckmean(case.groups.wlinv, case.gas.temp, op["cap"])
+        po.rossmean(case.groups.wlinv, case.gas.temp, op["sig"], op["cap"])
+        ol = po.leakage_opacity11(case.grid, case.groups.wlinv, tinv, op["sig"], op["cap"],
+                                  tauddmc=params.tauddmc, taulump=params.taulump)
+        ep = po.emission_probability(case.groups.wlinv, tinv, op["cap"], grey, case.groups.nep, case.groups.nepg)
+        t_fixed = time.perf_counter() - t0
+        prt, isv, _, _, _ = po.make_source_particles(case.grid, case.groups, case.gas.temp, L_BOL, sample,
+                                                     ioffset=k)
+        tt = po.TransportTables(case.grid, case.groups, tinv, op["sig"], op["cap"], grey, ep, ol, params)
+        st = po.rnd_init(cores, k)
+        t0 = time.perf_counter()
+        po.sourcetally(prt, isv, case.grid, case.groups)
+        r = po.particle_advance(tt, prt, isv, rngmode=0, nthreads=cores, rnd_states=st)
+        po.fluxtally(prt, isv, case.groups.wl)
+        dt = time.perf_counter() - t0
+        scale = npart / sample
+        t_step = t_fixed + dt * scale
+        if k >= a.warmup:
+            rates.append((r["nstepimc"] + r["nstepddmc"]) * scale / t_step)
+            tsteps.append(t_step)
+    value = statistics.mean(rates)
+    res = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": 1e3 * statistics.mean(tsteps), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded generator, superlite_b200/workloads.py)", "config": config_dict(a, world),
+           "impl": "reference",
+           "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+                            "sample": f"per step: full opacity build + coefficients, transport of {sample} of "
+                                      f"{npart} particles (mzran, OpenMP static,1), transport time scaled"},
+           "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(res))
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -195,6 +195,30 @@ int slg_fluxtally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, int32_t* i
 int slg_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, const int32_t* isvacant,
                     double* src_energy, int32_t* src_number);
 
+/* ------------------------------------------------------------------ sources */
+
+/* sourceenergy (SOURCE/sourceenergy.f90:21-29): grd_emit (ncell) of the
+ * surface-like thermal source, renormalised to L_bol; tot_sthermal optional.
+ * Host arrays, host computation (O(ncell)). */
+int slg_sourceenergy(slg_ctx* ctx, const double* radtemp, double L_bol, double* emit,
+                     double* tot_sthermal);
+
+/* sourcenumbers (SOURCE/sourcenumbers.f90:3-94, one rank, no surface source):
+ * grd_nvol (ncell) for src_ns particles.  Returns src_nnew (>= 0) or a negative
+ * error (vacancies < emitting cells, no particles, surplus > ncell). */
+int64_t slg_sourcenumbers(slg_ctx* ctx, const double* emit, double srcepwr, int64_t src_ns,
+                          int64_t nvacant, int32_t* nvol);
+
+/* vacancies + interior_source + source_transformdirection
+ * (SOURCE/vacancies.f90, SOURCE/interior_source.f90:3-172,
+ * SOURCE/source_transformdirection.f90:3-47): fills the first src_nnew vacant
+ * slots of prt/isvacant with thermal source particles (lab-frame direction,
+ * comoving energy and wavelength).  Random numbers: Philox4x32-10, one stream
+ * per particle slot keyed by `seed` (stream 1).  *nnew receives src_nnew. */
+int slg_interior_source(slg_ctx* ctx, const double* radtemp, const double* emit,
+                        const int32_t* nvol, slg_packet* prt, int32_t* isvacant, int64_t npart,
+                        uint64_t seed, int64_t* nnew);
+
 /* ------------------------------------------------------------------ device-pointer forms */
 /* Same semantics as above; every array argument is a device pointer, work is
  * queued on the context's stream, and the call returns after queueing (the
@@ -216,6 +240,10 @@ int slg_dev_fluxtally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, int32_
                       int32_t* lumnum);
 int slg_dev_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt,
                         const int32_t* isvacant, double* src_energy, int32_t* src_number);
+/* radtemp, prt and isvacant on the device; emit and nvol are host arrays. */
+int slg_dev_interior_source(slg_ctx* ctx, const double* radtemp, const double* emit,
+                            const int32_t* nvol, slg_packet* prt, int32_t* isvacant,
+                            int64_t npart, uint64_t seed, int64_t* nnew);
 /* Wait for the context's stream; returns a pending error if any. */
 int slg_sync(slg_ctx* ctx);
 /* The context's cudaStream_t, as an opaque handle. */

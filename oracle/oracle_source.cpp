@@ -81,7 +81,7 @@ int64_t orc_sourcenumbers(int nx, const double* emit, double pwr, int64_t src_ns
 int orc_interior_source(int nx, int ng, const double* xarr, const double* vxarr,
                         const double* wlinv, const double* radtemp, const double* emit, double pwr,
                         const int32_t* nvol, int64_t npart, orc_packet* prt, int32_t* isvacant,
-                        orc_rnd* state) {
+                        orc_rnd* state, int rngmode, uint64_t seed) {
   int64_t nnew = 0;
   for (int l = 0; l < nx; ++l)
     if (emit[l] != 0.0) nnew += nvol[l];
@@ -108,9 +108,16 @@ int orc_interior_source(int nx, int ng, const double* xarr, const double* vxarr,
     const int icnb1 = i - 1 > 1 ? i - 1 : 1;
     const int icnb2 = i + 1 < nx ? i + 1 : nx;
     for (int ii = 1; ii <= nhere; ++ii) {
-      orc_packet& p = prt[ivacant[ipart]];
-      isvacant[ivacant[ipart]] = 0;
+      const int64_t ivac = ivacant[ipart];
+      orc_packet& p = prt[ivac];
+      isvacant[ivac] = 0;
       ipart++;
+      // rngmode 0: the single mzran stream rnd_state; 1: Philox stream
+      // (seed, pid = slot, stream 1) shared with the GPU source kernel
+      uint32_t kdraw = 0;
+      auto mzran_real = [&](orc_rnd* st) {
+        return rngmode == 0 ? orc::mzran_real(st) : orc::philox_real(seed, (uint64_t)ivac, 1u, kdraw++);
+      };
       double denom2 = 0.0;
       double r1 = mzran_real(state);
       int iig = 1;

@@ -106,7 +106,7 @@ def lib():
         L.orc_sourcenumbers.argtypes = [C.c_int, dp, C.c_double, C.c_int64, C.c_int64, ip]
         L.orc_interior_source.restype = C.c_int
         L.orc_interior_source.argtypes = [C.c_int, C.c_int, dp, dp, dp, dp, dp, C.c_double, ip,
-                                          C.c_int64, C.c_void_p, ip, C.c_void_p]
+                                          C.c_int64, C.c_void_p, ip, C.c_void_p, C.c_int, C.c_uint64]
         _LIB = L
     return _LIB
 
@@ -311,9 +311,11 @@ def sourcetally(prt, isvacant, grid, groups):
 
 
 # ---------------------------------------------------------------- sources
-def make_source_particles(grid, groups, radtemp, L_bol, src_ns, npart=None, ioffset=0):
+def make_source_particles(grid, groups, radtemp, L_bol, src_ns, npart=None, ioffset=0, rngmode=0, seed=0,
+                          isvacant=None):
     """sourceenergy + sourcenumbers + vacancies + interior_source +
-    source_transformdirection with the reference's mzran stream."""
+    source_transformdirection with the reference's mzran stream (rngmode 0)
+    or the per-particle Philox streams of the GPU source kernel (rngmode 1)."""
     nx, ng = grid.nx, groups.ng
     emit = np.zeros(nx)
     tot = np.zeros(1)
@@ -321,16 +323,17 @@ def make_source_particles(grid, groups, radtemp, L_bol, src_ns, npart=None, ioff
     lib().orc_sourceenergy(nx, _ptr(xarr, dp), _ptr(f64(radtemp), dp), L_bol, _ptr(emit, dp), _ptr(tot, dp))
     npart = src_ns if npart is None else npart
     nvol = np.zeros(nx, dtype=np.int32)
-    nnew = lib().orc_sourcenumbers(nx, _ptr(emit, dp), 1.0, src_ns, npart, _ptr(nvol, ip))
+    nnew = lib().orc_sourcenumbers(nx, _ptr(emit, dp), 1.0, src_ns, src_ns if isvacant is None else
+                                   int(isvacant.sum()), _ptr(nvol, ip))
     if nnew < 0:
         raise RuntimeError(f"sourcenumbers failed: {nnew}")
     prt = np.zeros(npart, dtype=PACKET_DTYPE)
-    isv = np.ones(npart, dtype=np.int32)
+    isv = np.ones(npart, dtype=np.int32) if isvacant is None else isvacant.copy()
     st = rnd_init(1, ioffset)
     rc = lib().orc_interior_source(nx, ng, _ptr(xarr, dp), _ptr(f64(grid.vxarr), dp),
                                    _ptr(f64(groups.wlinv), dp), _ptr(f64(radtemp), dp), _ptr(emit, dp), 1.0,
                                    _ptr(nvol, ip), npart, prt.ctypes.data_as(C.c_void_p), _ptr(isv, ip),
-                                   st.ctypes.data_as(C.c_void_p))
+                                   st.ctypes.data_as(C.c_void_p), rngmode, seed)
     if rc != 0:
         raise RuntimeError(f"interior_source failed: {rc}")
     return prt, isv, emit, nvol, float(tot[0])

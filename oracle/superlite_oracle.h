@@ -168,11 +168,14 @@ void orc_sourceenergy(int nx, const double* xarr, const double* radtemp, double 
 /* sourcenumbers.f90 for one rank, no surface source: returns src_nnew. */
 int64_t orc_sourcenumbers(int nx, const double* emit, double srcepwr, int64_t src_ns,
                           int64_t nvacant, int32_t* nvol);
-/* vacancies + interior_source + source_transformdirection (mzran, one stream). */
+/* vacancies + interior_source + source_transformdirection.  rngmode 0: the
+ * reference's single mzran stream `state`; 1: one Philox stream per particle
+ * (seed, pid = slot index, stream 1), as the GPU source kernel draws. */
 int orc_interior_source(int nx, int ng, const double* xarr, const double* vxarr,
                         const double* wlinv, const double* radtemp, const double* emit,
                         double srcepwr, const int32_t* nvol, int64_t npart,
-                        orc_packet* prt, int32_t* isvacant, orc_rnd* state);
+                        orc_packet* prt, int32_t* isvacant, orc_rnd* state, int rngmode,
+                        uint64_t seed);
 
 #ifdef __cplusplus
 }

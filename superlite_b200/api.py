@@ -254,6 +254,40 @@ class HotPath:
                                            ptr(num)))
         return lum, dev, num
 
+    # ------------------------------------------------------------- sources
+    def sourceenergy(self, radtemp, L_bol):
+        """SOURCE/sourceenergy.f90: grd_emit (ncell) and tot_sthermal."""
+        t = _f64(radtemp)
+        emit = np.zeros(self.nx)
+        tot = np.zeros(1)
+        self._check(self.lib.slg_sourceenergy(self.h, ptr(t), float(L_bol), ptr(emit), ptr(tot)))
+        return emit, float(tot[0])
+
+    def sourcenumbers(self, emit, src_ns, nvacant=None, srcepwr=1.0):
+        """SOURCE/sourcenumbers.f90 (one rank): grd_nvol and src_nnew."""
+        e = _f64(emit)
+        nvol = np.zeros(self.nx, dtype=np.int32)
+        n = self.lib.slg_sourcenumbers(self.h, ptr(e), float(srcepwr), int(src_ns),
+                                       int(src_ns if nvacant is None else nvacant), ptr(nvol))
+        if n < 0:
+            self._check(int(n))
+        return nvol, int(n)
+
+    def interior_source(self, radtemp, emit, nvol, prt, isvacant, seed=0):
+        """vacancies + interior_source + source_transformdirection.  numpy arrays are
+        updated in place (host path); torch CUDA tensors use the device path."""
+        e = _f64(emit)
+        nv = np.ascontiguousarray(nvol, dtype=np.int32)
+        nnew = C.c_int64(0)
+        if _is_torch(prt):
+            self._check(self.lib.slg_dev_interior_source(self.h, ptr(radtemp), ptr(e), ptr(nv), ptr(prt),
+                                                         ptr(isvacant), int(prt.shape[0]), seed, C.byref(nnew)))
+            return int(nnew.value)
+        t = _f64(radtemp)
+        self._check(self.lib.slg_interior_source(self.h, ptr(t), ptr(e), ptr(nv), ptr(prt), ptr(isvacant), len(prt),
+                                                 seed, C.byref(nnew)))
+        return int(nnew.value)
+
     def sourcetally(self, prt, isvacant):
         """Returns src_energy, src_number as (ng, ncell) arrays (Fortran (ncell, ng))."""
         if _is_torch(prt):

@@ -73,6 +73,10 @@ SIGNATURES = {
                                            C.POINTER(SlgTransportOut)]),
     "slg_dev_fluxtally": (C.c_int, [vp, C.c_int64, vp, vp, C.c_int32, vp, vp, vp, vp]),
     "slg_dev_sourcetally": (C.c_int, [vp, C.c_int64, vp, vp, vp, vp]),
+    "slg_sourceenergy": (C.c_int, [vp, vp, C.c_double, vp, vp]),
+    "slg_sourcenumbers": (C.c_int64, [vp, vp, C.c_double, C.c_int64, C.c_int64, vp]),
+    "slg_interior_source": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_int64, C.c_uint64, vp]),
+    "slg_dev_interior_source": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_int64, C.c_uint64, vp]),
     "slg_sync": (C.c_int, [vp]),
     "slg_stream": (vp, [vp]),
 }

@@ -51,6 +51,13 @@ void* scratch(slg_ctx* ctx, int slot, size_t bytes) {
 
 int opacity_flags(slg_ctx* ctx, int32_t* sanity, int32_t* binning);
 int sourcetally_error(slg_ctx* ctx, int* err);
+void host_sourceenergy(int nx, const double* xarr, const double* radtemp, double L_bol, double* emit,
+                       double* tot_sthermal);
+long long host_sourcenumbers(int nx, const double* emit, double pwr, long long src_ns, long long nvacant,
+                             int32_t* nvol);
+int launch_interior_source(slg_ctx* ctx, const double* d_radtemp, const double* h_emit, const int32_t* h_nvol,
+                           long long npart, slg_packet* prt, int32_t* isvacant, uint64_t seed, long long* nnew_out);
+int interior_source_check(slg_ctx* ctx, long long nnew);
 
 }  // namespace slg
 
@@ -512,6 +519,56 @@ int slg_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, const in
     if (!rc && (e & 1)) rc = set_error(ctx, SLG_ERR_ARG, "sourcetally: ic outside range");
     if (!rc && (e & 2)) rc = set_error(ctx, SLG_ERR_ARG, "sourcetally: ig outside range");
   }
+  return rc;
+}
+
+// ------------------------------------------------------------------ sources
+int slg_sourceenergy(slg_ctx* ctx, const double* radtemp, double L_bol, double* emit, double* tot_sthermal) {
+  if (!ctx || !radtemp || !emit) return set_error(ctx, SLG_ERR_ARG, "null argument");
+  if (ctx->nx < 1) return set_error(ctx, SLG_ERR_STATE, "grid not set");
+  host_sourceenergy(ctx->nx, ctx->h_xarr.data(), radtemp, L_bol, emit, tot_sthermal);
+  return SLG_OK;
+}
+
+int64_t slg_sourcenumbers(slg_ctx* ctx, const double* emit, double srcepwr, int64_t src_ns, int64_t nvacant,
+                          int32_t* nvol) {
+  if (!ctx || !emit || !nvol || src_ns < 1) return set_error(ctx, SLG_ERR_ARG, "bad argument");
+  if (ctx->nx < 1) return set_error(ctx, SLG_ERR_STATE, "grid not set");
+  const long long r = host_sourcenumbers(ctx->nx, emit, srcepwr, src_ns, nvacant, nvol);
+  if (r < 0) return set_error(ctx, SLG_ERR_ARG, "sourcenumbers failed (%lld)", r);
+  return r;
+}
+
+int slg_dev_interior_source(slg_ctx* ctx, const double* radtemp, const double* emit, const int32_t* nvol,
+                            slg_packet* prt, int32_t* isvacant, int64_t npart, uint64_t seed, int64_t* nnew) {
+  if (!ctx || !radtemp || !emit || !nvol || npart < 0 || (npart > 0 && (!prt || !isvacant)))
+    return set_error(ctx, SLG_ERR_ARG, "bad argument");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  cudaSetDevice(ctx->device);
+  long long n = 0;
+  const int rc = launch_interior_source(ctx, radtemp, emit, nvol, npart, prt, isvacant, seed, &n);
+  if (nnew) *nnew = n;
+  return rc;
+}
+
+int slg_interior_source(slg_ctx* ctx, const double* radtemp, const double* emit, const int32_t* nvol,
+                        slg_packet* prt, int32_t* isvacant, int64_t npart, uint64_t seed, int64_t* nnew) {
+  if (!ctx || !radtemp || !emit || !nvol || npart < 0 || (npart > 0 && (!prt || !isvacant)))
+    return set_error(ctx, SLG_ERR_ARG, "bad argument");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  cudaSetDevice(ctx->device);
+  const size_t np = (size_t)npart;
+  int rc = 0;
+  const double* dt = up(ctx, H_A, radtemp, (size_t)ctx->nx, &rc);
+  slg_packet* dp = up(ctx, H_G, prt, np, &rc);
+  int32_t* dv = up(ctx, H_H, isvacant, np, &rc);
+  long long n = 0;
+  if (!rc) rc = launch_interior_source(ctx, dt, emit, nvol, npart, dp, dv, seed, &n);
+  down(ctx, prt, dp, np, &rc);
+  down(ctx, isvacant, dv, np, &rc);
+  rc = finish(ctx, rc);
+  if (!rc) rc = interior_source_check(ctx, n);
+  if (nnew) *nnew = n;
   return rc;
 }
 

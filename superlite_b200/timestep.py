@@ -26,8 +26,8 @@ KERNELS_PER_STEP = 15
 
 
 class DeviceTimestep:
-    def __init__(self, hot: HotPath, case, particles: np.ndarray, isvacant: np.ndarray, params,
-                 flx_wl=None, precision=0):
+    def __init__(self, hot: HotPath, case, params, npart: int = 0, particles: np.ndarray = None,
+                 isvacant: np.ndarray = None, flx_wl=None, precision=0):
         self.hot = hot
         self.params = params
         self.precision = precision
@@ -61,13 +61,17 @@ class DeviceTimestep:
         self.lum = torch.empty(self.flx_ng, dtype=torch.float64, device=dev)
         self.lumdev = torch.empty_like(self.lum)
         self.lumnum = torch.empty(self.flx_ng, dtype=torch.int32, device=dev)
-        assert particles.dtype == PACKET_DTYPE
-        raw = torch.as_tensor(particles.view(np.float64).reshape(-1, 8))
-        self.prt0 = raw.to(dev)
-        self.prt = torch.empty_like(self.prt0)
-        self.isv0 = torch.as_tensor(np.ascontiguousarray(isvacant, dtype=np.int32)).to(dev)
-        self.isv = torch.empty_like(self.isv0)
-        self.npart = particles.shape[0]
+        if particles is not None:
+            assert particles.dtype == PACKET_DTYPE
+            raw = torch.as_tensor(particles.view(np.float64).reshape(-1, 8))
+            self.prt0 = raw.to(dev)
+            self.isv0 = torch.as_tensor(np.ascontiguousarray(isvacant, dtype=np.int32)).to(dev)
+            npart = particles.shape[0]
+        else:
+            self.prt0 = self.isv0 = None  # particles are made on the device (interior_source)
+        self.prt = torch.empty((npart, 8), dtype=torch.float64, device=dev)
+        self.isv = torch.ones(npart, dtype=torch.int32, device=dev)
+        self.npart = npart
         gp = capi.SlgGas(*[ptr(self.gas[k]) for k in ("temp", "natom", "nelec", "vol", "mass", "natomfr", "oc", "ginv")])
         self._gas = gp
         self._flags = capi.SlgOpacityFlags(0, 0, 0, 0, 1, 0.0)
@@ -95,6 +99,8 @@ class DeviceTimestep:
                                                  ptr(self.emitprob)))
 
     def restore_particles(self):
+        if self.prt0 is None:
+            return
         with torch.cuda.stream(self.stream):
             self.prt.copy_(self.prt0)
             self.isv.copy_(self.isv0)

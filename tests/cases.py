@@ -16,7 +16,10 @@ def transport_case(oracle, t_days=5.0, nx=64, ng=100, npart=4000, seed=3, kind="
     groups = W.group_grid(ng)
     rho, mass = W.broken_powerlaw_rho(grid)
     temp = rng.uniform(6000.0, 14000.0, nx)
-    sig, cap = oracle.analytic_opacity(groups.wlinv, temp, rho, kind=1 if kind == "grey" else 2)
+    if kind == "mono":  # group-dependent: ~70% of (shell, group) pairs optically thick at 6 d
+        sig, cap = oracle.analytic_opacity(groups.wlinv, temp, rho, kind=2, capcoef=1e33)
+    else:
+        sig, cap = oracle.analytic_opacity(groups.wlinv, temp, rho, kind=1)
     if kind == "grey+sig":
         sig = 0.3 * cap[:, 0].astype(np.float64)
     tinv = 1.0 / temp
