@@ -244,6 +244,40 @@ int slg_dev_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt,
 int slg_dev_interior_source(slg_ctx* ctx, const double* radtemp, const double* emit,
                             const int32_t* nvol, slg_packet* prt, int32_t* isvacant,
                             int64_t npart, uint64_t seed, int64_t* nnew);
+/* ------------------------------------------------------------------ no device allocation */
+
+/* Size limits of slg_particle_advance_static (see below). */
+#define SLG_STATIC_MAX_CELLGROUPS 131072 /* ncell * ng */
+#define SLG_STATIC_MAX_CELLS 4096
+#define SLG_ERR_TOO_LARGE (-7)           /* grid larger than the static limits */
+
+/* Grid and group arrays on the device (grd_xarr, grd_vxarr (nx+1), grd_divv
+ * (nx), grp_wl, grp_wlinv (ng+1)), for the entry point below. */
+typedef struct slg_grid_dev {
+  int32_t nx, ng;
+  const double* xarr;
+  const double* vxarr;
+  const double* divv;
+  const double* wl;
+  const double* wlinv;
+} slg_grid_dev;
+
+/* particle_advance for callers that cannot allocate device memory (no
+ * counterpart in the reference: an addition of this library).  Same semantics
+ * as slg_dev_particle_advance, but needs no context and calls no allocator:
+ * every input and output is a caller-owned device pointer, and the per-cell
+ * tables and counters live in one fixed 6.5 MiB __device__ array that every GPU
+ * loading the library holds until exit.  Grids beyond SLG_STATIC_MAX_CELLS
+ * shells or SLG_STATIC_MAX_CELLGROUPS (shells x groups) return
+ * SLG_ERR_TOO_LARGE.  Runs on `stream` (a cudaStream_t, NULL = default) on the
+ * current device and returns after the stream has finished it.  The first
+ * call on a device looks up the array's device address; make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race, so serialise them. */
+int slg_particle_advance_static(const slg_grid_dev* grid, const slg_transport_in* in,
+                                slg_packet* prt, int32_t* isvacant, int64_t npart,
+                                uint64_t seed, slg_transport_out* out, void* stream);
+
 /* Wait for the context's stream; returns a pending error if any. */
 int slg_sync(slg_ctx* ctx);
 /* The context's cudaStream_t, as an opaque handle. */

@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libslg.so")
 
 SLG_OK = 0
 ERRORS = {-1: "SLG_ERR_CUDA", -2: "SLG_ERR_ARG", -3: "SLG_ERR_STATE", -4: "SLG_ERR_UNSORTED",
-          -5: "SLG_ERR_OOM", -6: "SLG_ERR_NOT_BUILT"}
+          -5: "SLG_ERR_OOM", -6: "SLG_ERR_NOT_BUILT", -7: "SLG_ERR_TOO_LARGE"}
 
 vp = C.c_void_p
 
@@ -44,6 +44,11 @@ class SlgTransportOut(C.Structure):
                 ("nstepimc", C.c_int64), ("nstepddmc", C.c_int64), ("nmethodswap", C.c_int64),
                 ("nstepmax", C.c_int64), ("ndist", C.c_int64 * 11), ("nposwarn", C.c_int64),
                 ("ierr", C.c_int32), ("ierr_part", C.c_int32)]
+
+
+class SlgGridDev(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ng", C.c_int32), ("xarr", vp), ("vxarr", vp), ("divv", vp), ("wl", vp),
+                ("wlinv", vp)]
 
 
 # name -> (restype, argtypes); every symbol declared in include/slg.h
@@ -77,6 +82,8 @@ SIGNATURES = {
     "slg_sourcenumbers": (C.c_int64, [vp, vp, C.c_double, C.c_int64, C.c_int64, vp]),
     "slg_interior_source": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_int64, C.c_uint64, vp]),
     "slg_dev_interior_source": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_int64, C.c_uint64, vp]),
+    "slg_particle_advance_static": (C.c_int, [C.POINTER(SlgGridDev), C.POINTER(SlgTransportIn), vp, vp, C.c_int64,
+                                              C.c_uint64, C.POINTER(SlgTransportOut), vp]),
     "slg_sync": (C.c_int, [vp]),
     "slg_stream": (vp, [vp]),
 }

@@ -448,3 +448,20 @@ int build_cell_tables(slg_ctx* ctx, const slg_transport_in* in) {
 }
 
 }  // namespace slg
+
+namespace slg {
+// Launch of cell_tables_kernel on caller-provided tables and stream (used by
+// the entry point that allocates nothing).
+int launch_cell_tables_raw(cudaStream_t st, int nx, int ng, int nep, int nepg, const double* xarr,
+                           const double* vxarr, const double* divv, const double* wlinv,
+                           const slg_transport_in* in, const CellTables& T) {
+  TabArgs A;
+  A.nx = nx; A.ng = ng; A.nep = nep; A.nepg = nepg;
+  A.xarr = xarr; A.vxarr = vxarr; A.divv = divv; A.wlinv = wlinv;
+  A.tempinv = in->tempinv; A.sig = in->sig; A.capgrey = in->capgrey; A.opaclump = in->opaclump;
+  A.emitprob = in->emitprob; A.cap = in->cap; A.tauddmc = in->tauddmc; A.taulump = in->taulump;
+  A.T = T;
+  cell_tables_kernel<<<nx, GB, 0, st>>>(A);
+  return cudaGetLastError() == cudaSuccess ? SLG_OK : SLG_ERR_CUDA;
+}
+}  // namespace slg

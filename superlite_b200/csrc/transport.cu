@@ -412,3 +412,36 @@ int sourcetally_error(slg_ctx* ctx, int* err) {
 }
 
 }  // namespace slg
+
+namespace slg {
+// Launch of particle_advance_kernel with every buffer supplied by the caller
+// (used by the entry point that allocates nothing).  nblk is the grid size.
+int launch_particle_advance_raw(cudaStream_t st, const TrnArgs& A, int nblk) {
+  particle_advance_kernel<false><<<(unsigned)nblk, TRN_BLOCK, 0, st>>>(A);
+  return cudaGetLastError() == cudaSuccess ? SLG_OK : SLG_ERR_CUDA;
+}
+int particle_advance_blocks_per_sm() {
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_kernel<false>, TRN_BLOCK, 0);
+  return occ > 0 ? occ : 4;
+}
+int particle_advance_block_size() { return TRN_BLOCK; }
+
+// Fold device counters read back by the caller into *out (totals accumulate).
+int finish_particle_advance_acc(const TransportAcc& a, slg_transport_out* out) {
+  out->tot_evelo += a.evelo;
+  out->tot_eout += a.eout;
+  out->tot_sflux += a.sflux;
+  out->npckt = (int64_t)a.npckt;
+  out->nflux = (int64_t)a.nflux;
+  out->nstepimc = (int64_t)a.nimc;
+  out->nstepddmc = (int64_t)a.nddmc;
+  out->nmethodswap = (int64_t)a.nswap;
+  out->nstepmax = (int64_t)a.nmax;
+  for (int k = 0; k < 11; ++k) out->ndist[k] = (int64_t)a.ndist[k];
+  out->nposwarn = (int64_t)a.nwarn;
+  out->ierr = a.ierr_key != ~0ull ? (int32_t)(a.ierr_key & 0xffffffffu) : 0;
+  out->ierr_part = a.ierr_key != ~0ull ? (int32_t)(a.ierr_key >> 32) : 0;
+  return out->ierr;
+}
+}  // namespace slg
