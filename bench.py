@@ -157,7 +157,14 @@ def run_ours(a):
         ts.transport(seed0 + 2 * k + 1)
         ts.fluxtally()
 
-    # warm-up
+    # autotune the transport kernel on this workload's particles, then warm up
+    hot.interior_source(d_radtemp, emit, nvol, ts.prt, ts.isv, seed=seed0 - 1)
+    ts.opacity()
+    ts.coefficients()
+    variant, tune_ms = ts.autotune(seed=seed0 - 1, nsample=min(npart, 200_000))
+    ts.transport(seed0 - 1)  # one untimed step with the chosen variant
+    ts.fluxtally()           # leaves every slot vacant again
+    ts.sync()
     for k in range(a.warmup):
         one_step(k)
         ts.sync()
@@ -226,6 +233,7 @@ def run_ours(a):
                      "basis": f"{BYTES_PER_STEP:.0f} B per particle-step x steps per launch / launch time; "
                               f"peak {peak_kind}"},
         "clocks": clocks,
+        "autotune": {"variant": variant, "sample_ms": tune_ms},
         "gpu_launches": 20 * a.steps,
     }
     if not a.no_e2e:

@@ -240,6 +240,16 @@ int slg_dev_fluxtally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, int32_
                       int32_t* lumnum);
 int slg_dev_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt,
                         const int32_t* isvacant, double* src_energy, int32_t* src_number);
+/* Transport autotuner (library addition): runs each compiled variant of the
+ * particle-loop kernel (register budget / resident blocks per SM) on a copy of
+ * the first nsample particles (device pointers; inputs are left unchanged),
+ * times it and keeps the fastest for this context.  *best (optional) receives
+ * the variant, ms (optional, 4 entries) the times. */
+int slg_autotune_transport(slg_ctx* ctx, const slg_transport_in* in, const slg_packet* prt,
+                           const int32_t* isvacant, int64_t npart, uint64_t seed,
+                           int64_t nsample, int32_t* best, float* ms);
+/* Select a transport kernel variant (0..3) explicitly. */
+int slg_set_transport_variant(slg_ctx* ctx, int32_t variant);
 /* radtemp, prt and isvacant on the device; emit and nvol are host arrays. */
 int slg_dev_interior_source(slg_ctx* ctx, const double* radtemp, const double* emit,
                             const int32_t* nvol, slg_packet* prt, int32_t* isvacant,

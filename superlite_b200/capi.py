@@ -84,6 +84,9 @@ SIGNATURES = {
     "slg_dev_interior_source": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_int64, C.c_uint64, vp]),
     "slg_particle_advance_static": (C.c_int, [C.POINTER(SlgGridDev), C.POINTER(SlgTransportIn), vp, vp, C.c_int64,
                                               C.c_uint64, C.POINTER(SlgTransportOut), vp]),
+    "slg_autotune_transport": (C.c_int, [vp, C.POINTER(SlgTransportIn), vp, vp, C.c_int64, C.c_uint64, C.c_int64,
+                                         vp, vp]),
+    "slg_set_transport_variant": (C.c_int, [vp, C.c_int32]),
     "slg_sync": (C.c_int, [vp]),
     "slg_stream": (vp, [vp]),
 }

@@ -58,6 +58,8 @@ long long host_sourcenumbers(int nx, const double* emit, double pwr, long long s
 int launch_interior_source(slg_ctx* ctx, const double* d_radtemp, const double* h_emit, const int32_t* h_nvol,
                            long long npart, slg_packet* prt, int32_t* isvacant, uint64_t seed, long long* nnew_out);
 int interior_source_check(slg_ctx* ctx, long long nnew);
+int autotune_transport(slg_ctx* ctx, const slg_transport_in* in, const slg_packet* prt, const int32_t* isvacant,
+                       int64_t npart, uint64_t seed, int64_t nsample, int* best, float* ms);
 
 }  // namespace slg
 
@@ -520,6 +522,27 @@ int slg_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, const in
     if (!rc && (e & 2)) rc = set_error(ctx, SLG_ERR_ARG, "sourcetally: ig outside range");
   }
   return rc;
+}
+
+// ------------------------------------------------------------------ autotuning
+int slg_autotune_transport(slg_ctx* ctx, const slg_transport_in* in, const slg_packet* prt, const int32_t* isvacant,
+                           int64_t npart, uint64_t seed, int64_t nsample, int32_t* best, float* ms) {
+  if (!ctx || !in || npart < 0 || (npart > 0 && (!prt || !isvacant))) return set_error(ctx, SLG_ERR_ARG, "bad argument");
+  if (!in->tempinv || !in->sig || !in->capgrey || !in->emitprob || !in->opaclump || !in->cap)
+    return set_error(ctx, SLG_ERR_ARG, "slg_transport_in has a null array");
+  if (!need_grid(ctx) || ctx->nx < 2) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  if (in->precision != 0) return set_error(ctx, SLG_ERR_NOT_BUILT, "precision %d not available", in->precision);
+  cudaSetDevice(ctx->device);
+  int b = 0;
+  const int rc = autotune_transport(ctx, in, prt, isvacant, npart, seed, nsample, &b, ms);
+  if (best) *best = b;
+  return rc;
+}
+
+int slg_set_transport_variant(slg_ctx* ctx, int32_t variant) {
+  if (!ctx || variant < 0 || variant > 3) return set_error(ctx, SLG_ERR_ARG, "variant must be 0..3");
+  ctx->trn_variant = variant;
+  return SLG_OK;
 }
 
 // ------------------------------------------------------------------ sources

@@ -80,7 +80,7 @@ struct slg_ctx {
   uint64_t* trace_hash = nullptr;
   int32_t* trace_nstep = nullptr;
   // launch configuration chosen by the autotuner (0 = defaults)
-  int trn_block = 0, trn_grid_per_sm = 0;
+  int trn_variant = 0;  // transport kernel variant (see launch_transport_variant)
   // transport_out of a queued slg_dev_particle_advance, completed by slg_sync
   slg_transport_out* pending_out = nullptr;
   int num_sms = 0;

@@ -43,8 +43,12 @@ __device__ inline void store_packet(slg_packet* p, double x, double y, double z,
   q[3] = make_double2(e0, wl);
 }
 
-template <bool TRACE>
-__global__ void __launch_bounds__(TRN_BLOCK) particle_advance_kernel(const TrnArgs A) {
+// MINB = minimum resident blocks per SM requested from the register
+// allocator: 1 -> up to 255 registers (the compiler settles on 128),
+// 5 -> 96, 6 -> 80, 8 -> 64 registers with some spilling.  The autotuner
+// (slg_autotune_transport) picks the fastest on the caller's workload.
+template <bool TRACE, int MINB>
+__global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const TrnArgs A) {
   __shared__ unsigned long long s_cnt[20];
   __shared__ double s_sum[3];
   if (threadIdx.x < 20) s_cnt[threadIdx.x] = 0ull;
@@ -294,7 +298,29 @@ __global__ void sourcetally_kernel(long long npart, const slg_packet* __restrict
   }
 }
 
+template <bool TRACE, int MINB>
+int launch_one(int num_sms, long long npart, cudaStream_t st, const TrnArgs& A) {
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_kernel<TRACE, MINB>, TRN_BLOCK, 0);
+  long long nblk = (long long)num_sms * (occ > 0 ? occ : 4);
+  const long long need = (npart + TRN_BLOCK - 1) / TRN_BLOCK;
+  if (need < nblk) nblk = need > 0 ? need : 1;
+  particle_advance_kernel<TRACE, MINB><<<(unsigned)nblk, TRN_BLOCK, 0, st>>>(A);
+  return cudaPeekAtLastError() == cudaSuccess ? SLG_OK : SLG_ERR_CUDA;
+}
+
 }  // namespace
+
+// Transport kernel variants (register budget / resident blocks), see MINB.
+constexpr int kTransportVariants = 4;
+int launch_transport_variant(int v, bool trace, int num_sms, long long npart, cudaStream_t st, const TrnArgs& A) {
+  switch (v) {
+    case 1: return trace ? launch_one<true, 5>(num_sms, npart, st, A) : launch_one<false, 5>(num_sms, npart, st, A);
+    case 2: return trace ? launch_one<true, 6>(num_sms, npart, st, A) : launch_one<false, 6>(num_sms, npart, st, A);
+    case 3: return trace ? launch_one<true, 8>(num_sms, npart, st, A) : launch_one<false, 8>(num_sms, npart, st, A);
+    default: return trace ? launch_one<true, 1>(num_sms, npart, st, A) : launch_one<false, 1>(num_sms, npart, st, A);
+  }
+}
 
 int launch_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packet* prt, int32_t* isvacant,
                             int64_t npart, uint64_t seed, slg_transport_out* out, uint64_t* d_trace_hash,
@@ -319,22 +345,8 @@ int launch_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packet
   A.T = ctx->tables; A.prt = prt; A.isvacant = isvacant; A.npart = npart; A.seed = seed;
   A.tally = out->tally; A.jrad = out->jrad; A.eamp = out->eamp; A.methodswap = out->methodswap;
   A.acc = ctx->d_acc; A.trace_hash = d_trace_hash; A.trace_nstep = d_trace_nstep;
-  const int block = TRN_BLOCK;
-  int per_sm = ctx->trn_grid_per_sm > 0 ? ctx->trn_grid_per_sm : 0;
-  if (per_sm == 0) {
-    int occ = 0;
-    if (d_trace_hash) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_kernel<true>, block, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_kernel<false>, block, 0);
-    per_sm = occ > 0 ? occ : 4;
-  }
-  long long nblk = (long long)ctx->num_sms * per_sm;
-  const long long need = (npart + block - 1) / block;
-  if (need < nblk) nblk = need > 0 ? need : 1;
-  if (d_trace_hash)
-    particle_advance_kernel<true><<<(unsigned)nblk, block, 0, st>>>(A);
-  else
-    particle_advance_kernel<false><<<(unsigned)nblk, block, 0, st>>>(A);
-  if ((rc = cuda_check(ctx, cudaGetLastError(), "particle_advance launch"))) return rc;
+  if ((rc = launch_transport_variant(ctx->trn_variant, d_trace_hash != nullptr, ctx->num_sms, npart, st, A)))
+    return set_error(ctx, rc, "particle_advance launch: %s", cudaGetErrorString(cudaGetLastError()));
   return cuda_check(ctx, cudaMemcpyAsync(ctx->h_acc, ctx->d_acc, sizeof(TransportAcc), cudaMemcpyDeviceToHost, st),
                     "transport counters download");
 }
@@ -417,15 +429,71 @@ namespace slg {
 // Launch of particle_advance_kernel with every buffer supplied by the caller
 // (used by the entry point that allocates nothing).  nblk is the grid size.
 int launch_particle_advance_raw(cudaStream_t st, const TrnArgs& A, int nblk) {
-  particle_advance_kernel<false><<<(unsigned)nblk, TRN_BLOCK, 0, st>>>(A);
+  particle_advance_kernel<false, 1><<<(unsigned)nblk, TRN_BLOCK, 0, st>>>(A);
   return cudaGetLastError() == cudaSuccess ? SLG_OK : SLG_ERR_CUDA;
 }
 int particle_advance_blocks_per_sm() {
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_kernel<false>, TRN_BLOCK, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_kernel<false, 1>, TRN_BLOCK, 0);
   return occ > 0 ? occ : 4;
 }
 int particle_advance_block_size() { return TRN_BLOCK; }
+
+// Autotuner of the transport kernel: runs every variant of
+// launch_transport_variant on the same copy of (a sample of) the caller's
+// particles, times each with CUDA events and keeps the fastest for this
+// context.  Device pointers; results are discarded.
+int autotune_transport(slg_ctx* ctx, const slg_transport_in* in, const slg_packet* prt, const int32_t* isvacant,
+                       int64_t npart, uint64_t seed, int64_t nsample, int* best, float* ms) {
+  const int nx = ctx->nx, ng = ctx->ng;
+  cudaStream_t st = ctx->stream;
+  int rc = build_cell_tables(ctx, in);
+  if (rc) return rc;
+  const long long n = nsample > 0 && nsample < npart ? nsample : npart;
+  slg_packet* p = (slg_packet*)scratch(ctx, 40, sizeof(slg_packet) * (n > 0 ? n : 1));
+  int32_t* v = (int32_t*)scratch(ctx, 41, sizeof(int32_t) * (n > 0 ? n : 1));
+  double* tally = (double*)scratch(ctx, 42, sizeof(double) * nx);
+  double* jrad = (double*)scratch(ctx, 43, sizeof(double) * (size_t)nx * ng);
+  double* eamp = (double*)scratch(ctx, 44, sizeof(double) * nx);
+  int32_t* msw = (int32_t*)scratch(ctx, 45, sizeof(int32_t) * nx);
+  if (!p || !v || !tally || !jrad || !eamp || !msw) return SLG_ERR_OOM;
+  TrnArgs A;
+  A.nx = nx; A.ng = ng; A.nep = ctx->nep; A.nepg = ctx->nepg;
+  A.xarr = ctx->d_xarr; A.vxarr = ctx->d_vxarr; A.divv = ctx->d_divv; A.wl = ctx->d_wl; A.wlinv = ctx->d_wlinv;
+  A.tempinv = in->tempinv; A.sig = in->sig; A.capgrey = in->capgrey; A.emitprob = in->emitprob;
+  A.opaclump = in->opaclump; A.cap = in->cap; A.tauddmc = in->tauddmc; A.taulump = in->taulump;
+  A.puretran = in->puretran; A.noampfact = in->noampfact; A.errorfatal = in->errorfatal;
+  A.thm_aniso = in->thm_aniso; A.dogrdtally = in->dogrdtally; A.max_steps = in->max_steps;
+  A.T = ctx->tables; A.prt = p; A.isvacant = v; A.npart = n; A.seed = seed;
+  A.tally = tally; A.jrad = jrad; A.eamp = eamp; A.methodswap = msw;
+  A.acc = ctx->d_acc; A.trace_hash = nullptr; A.trace_nstep = nullptr;
+  cudaEvent_t e0, e1;
+  if ((rc = cuda_check(ctx, cudaEventCreate(&e0), "event"))) return rc;
+  if ((rc = cuda_check(ctx, cudaEventCreate(&e1), "event"))) { cudaEventDestroy(e0); return rc; }
+  float bestms = 0.f;
+  int bestv = 0;
+  for (int var = 0; var < kTransportVariants && !rc; ++var) {
+    cudaMemcpyAsync(p, prt, sizeof(slg_packet) * n, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(v, isvacant, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st);
+    cudaMemsetAsync(tally, 0, sizeof(double) * nx, st);
+    cudaMemsetAsync(jrad, 0, sizeof(double) * (size_t)nx * ng, st);
+    cudaMemsetAsync(ctx->d_acc, 0, sizeof(TransportAcc), st);
+    cudaEventRecord(e0, st);
+    rc = launch_transport_variant(var, false, ctx->num_sms, n, st, A);
+    cudaEventRecord(e1, st);
+    if (!rc) rc = cuda_check(ctx, cudaEventSynchronize(e1), "autotune sync");
+    float t = 0.f;
+    if (!rc) cudaEventElapsedTime(&t, e0, e1);
+    if (ms) ms[var] = t;
+    if (!rc && (var == 0 || t < bestms)) { bestms = t; bestv = var; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  ctx->trn_variant = bestv;
+  if (best) *best = bestv;
+  return SLG_OK;
+}
 
 // Fold device counters read back by the caller into *out (totals accumulate).
 int finish_particle_advance_acc(const TransportAcc& a, slg_transport_out* out) {

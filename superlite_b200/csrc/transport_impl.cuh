@@ -38,15 +38,32 @@ struct Ptcl {
 };
 
 // first position q in [0,n) with a[q] > r, else n-1 (the last position a
-// linear scan visits)
+// linear scan visits).  a is non-decreasing, so the count of entries <= r
+// is a prefix; an 8-ary search issues the 7 probes of a round together,
+// which needs 4 dependent rounds of loads for n = 2000 instead of 11.
 __device__ inline int first_gt(const double* __restrict__ a, int n, double r) {
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (a[mid] > r) hi = mid;
-    else lo = mid + 1;
+  int lo = 0, hi = n;  // answer in [lo, hi]
+  while (hi - lo > 8) {
+    const int step = (hi - lo) >> 3;
+    double v[7];
+#pragma unroll
+    for (int j = 0; j < 7; ++j) v[j] = __ldg(a + lo + (j + 1) * step);
+    int c = 0;
+#pragma unroll
+    for (int j = 0; j < 7; ++j) c += v[j] <= r;
+    const int nlo = c == 0 ? lo : lo + c * step + 1;
+    const int nhi = c == 7 ? hi : lo + (c + 1) * step;
+    lo = nlo;
+    hi = nhi;
   }
-  return lo < n ? lo : n - 1;
+  double v[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) v[j] = lo + j < hi ? __ldg(a + lo + j) : 0.0;
+  int c = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) c += (lo + j < hi) && v[j] <= r;
+  const int q = lo + c;
+  return q < n ? q : n - 1;
 }
 
 __device__ inline double CAPd(const TrnArgs& A, int ig, int ic) {
@@ -468,40 +485,16 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       e = e * help;
       e0 = e0 * help;
     }
-  } else if (r1 >= pa + pdop && r1 < pa + pdop + pl0) {
-    // left leakage (:358-430)
-    p.idist = -3;
-    if (ix == 1) return;
-    const int l = ix - 1;
-    if (glump == 0) {
-      iiig = ig;
-    } else {
-      r1 = rng.draw();
-      iiig = glumps[first_gt(A.T.cdf_left + off, glump, r1)];
-    }
-    const double dxl = Xa - A.xarr[ix - 2];
-    if ((A.sig[l - 1] + CAPd(A, iiig, l)) * dxl < A.tauddmc) {
-      p.itype = 1;
-      r1 = rng.draw();
-      wl = 1.0 / (r1 * A.wlinv[iiig] + (1.0 - r1) * A.wlinv[iiig - 1]);
-      x = Xa;
-      vx = A.vxarr[ix - 1];
-      r1 = rng.draw();
-      r2 = rng.draw();
-      mu = -(r1 > r2 ? r1 : r2);
-      mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
-      help = 1.0 / (1.0 - vx * mu * cinv);
-      totevelo = totevelo + e * (1.0 - help);
-      e = e * help;
-      e0 = e0 * help;
-      wl = wl * (1.0 - vx * mu * cinv);
-    }
-    ix = ix - 1;
-    ig = iiig;
-  } else if (r1 >= pa + pdop + pl0 && r1 < pa + pdop + (pl0 + pl1)) {
-    // right leakage (:434-545)
-    p.idist = -4;
-    if (ix == A.nx) {
+  } else if (r1 >= pa + pdop && r1 < pa + pdop + (pl0 + pl1)) {
+    // leakage to a neighbour: left (:358-430) or right (:434-545).  Both
+    // directions run one code path (same draws, same arithmetic as each
+    // branch of the reference) so lanes of a warp leaking either way stay
+    // together.
+    const bool right = r1 >= pa + pdop + pl0;
+    p.idist = right ? -4 : -3;
+    if (!right && ix == 1) return;
+    if (right && ix == A.nx) {
+      // escape through the outer edge (:438-478)
       p.stat = 1;
       r1 = rng.draw();
       r2 = rng.draw();
@@ -523,23 +516,24 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       e0 = e0 * help;
       return;
     }
-    const int l = ix + 1;
+    const int l = right ? ix + 1 : ix - 1;
     if (glump == 0) {
       iiig = ig;
     } else {
       r1 = rng.draw();
-      iiig = glumps[first_gt(A.T.cdf_right + off, glump, r1)];
+      iiig = glumps[first_gt((right ? A.T.cdf_right : A.T.cdf_left) + off, glump, r1)];
     }
-    const double dxl = A.xarr[ix + 1] - Xb;
+    const double dxl = right ? A.xarr[ix + 1] - Xb : Xa - A.xarr[ix - 2];
     if ((A.sig[l - 1] + CAPd(A, iiig, l)) * dxl < A.tauddmc) {
       p.itype = 1;
       r1 = rng.draw();
       wl = 1.0 / (r1 * A.wlinv[iiig] + (1.0 - r1) * A.wlinv[iiig - 1]);
-      x = Xb;
-      vx = A.vxarr[ix];
+      x = right ? Xb : Xa;
+      vx = A.vxarr[right ? ix : ix - 1];
       r1 = rng.draw();
       r2 = rng.draw();
-      mu = r1 > r2 ? r1 : r2;
+      const double m = r1 > r2 ? r1 : r2;
+      mu = right ? m : -m;
       mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
       help = 1.0 / (1.0 - vx * mu * cinv);
       totevelo = totevelo + e * (1.0 - help);
@@ -547,7 +541,7 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       e0 = e0 * help;
       wl = wl * (1.0 - vx * mu * cinv);
     }
-    ix = ix + 1;
+    ix = l;
     ig = iiig;
   } else {
     // effective scattering (:549-620)

@@ -113,6 +113,16 @@ class DeviceTimestep:
         self._chk(L.slg_dev_particle_advance(h, C.byref(self._tin), ptr(self.prt), ptr(self.isv), self.npart, seed,
                                              C.byref(self._tout)))
 
+    def autotune(self, seed=0, nsample=200_000):
+        """Pick the fastest transport-kernel variant on a copy of the current
+        particles (call after the particles are in place).  Returns (variant, ms)."""
+        L, h = self.hot.lib, self.hot.h
+        best = C.c_int32(0)
+        ms = (C.c_float * 4)()
+        self._chk(L.slg_autotune_transport(h, C.byref(self._tin), ptr(self.prt), ptr(self.isv), self.npart, seed,
+                                           int(nsample), C.byref(best), ms))
+        return int(best.value), [float(m) for m in ms]
+
     def fluxtally(self):
         L, h = self.hot.lib, self.hot.h
         self._chk(L.slg_dev_fluxtally(h, self.npart, ptr(self.prt), ptr(self.isv), self.flx_ng, ptr(self.flx_wl),
