@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--ncell", type=int, default=256)
     ap.add_argument("--ng", type=int, default=2000)
     ap.add_argument("--nline", type=float, default=5e5)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=0, help="particles in the CPU-baseline sample (0: auto)")
@@ -74,7 +75,7 @@ def make_case(a):
 def config_dict(a, world):
     return {"workload": "IMC-DDMC timestep on physical LTE opacities (configs[2])",
             "shells": a.ncell, "groups": a.ng, "lines": int(a.nline), "particles_per_gpu": int(a.npart),
-            "snapshot_days": T_DAYS, "tauddmc": 5.0, "taulump": 10.0, "transport_precision": "fp64",
+            "snapshot_days": T_DAYS, "tauddmc": 5.0, "taulump": 10.0, "transport_precision": a.precision,
             "parallelism": f"particles{world}", "l2": "inputs larger than L2 (particle array 3.2 GB per GPU)"}
 
 
@@ -142,7 +143,8 @@ def run_ours(a):
     params = W.TransportParams()
     hot = HotPath(local)
     radtemp = case.gas.temp.copy()
-    ts = DeviceTimestep(hot, case, params, npart=npart)
+    prec = 1 if a.precision == "mixed" else 0
+    ts = DeviceTimestep(hot, case, params, npart=npart, precision=prec)
     emit, _ = hot.sourceenergy(radtemp, L_BOL)
     nvol, nnew = hot.sourcenumbers(emit, npart, npart)
     d_radtemp = ts.gas["temp"]
@@ -161,7 +163,7 @@ def run_ours(a):
     hot.interior_source(d_radtemp, emit, nvol, ts.prt, ts.isv, seed=seed0 - 1)
     ts.opacity()
     ts.coefficients()
-    variant, tune_ms = ts.autotune(seed=seed0 - 1, nsample=min(npart, 200_000))
+    variant, tune_ms = ts.autotune(seed=seed0 - 1, nsample=min(npart, 1_000_000))
     ts.transport(seed0 - 1)  # one untimed step with the chosen variant
     ts.fluxtally()           # leaves every slot vacant again
     ts.sync()

@@ -76,6 +76,26 @@ int slg_set_groups(slg_ctx* ctx, int32_t ng, const double* grp_wl);
 int slg_set_grid(slg_ctx* ctx, int32_t nx, const double* xarr, const double* vxarr,
                  const double* vol, const double* divv);
 
+/* Many independent ejecta models in one context (no counterpart in the
+ * reference, which runs one model per process).  Model m has nx[m] >= 2
+ * shells and npart[m] particle slots.  xarr and vxarr hold each model's
+ * nx[m]+1 shell edges, one model after the other; vol and divv each model's
+ * nx[m] cells.  Every per-cell array of the other calls (temperatures, gas,
+ * opacities, tallies ...) then runs over the sum of nx[m] cells in model
+ * order, and the particle arrays over the sum of npart[m] slots in model order
+ * (model m owns slots [npart[0] + ... + npart[m-1], + npart[m])).  Shell
+ * neighbours never cross a model.  Per-model behaviour: sourceenergy
+ * renormalises each model to L_bol, slg_models_sourcenumbers fills each
+ * model's slots, interior_source writes each model's particles into its own
+ * slots, fluxtally returns one row of flx_ng groups per model, and transport
+ * (precision 1 only) advances all models' particles in one persistent launch.
+ * Random numbers: model m draws under the key seed + m * SLG_MODEL_SEED_STRIDE
+ * with slot numbers counted from the model's first slot, so each model
+ * reproduces its own single-model run under that key. */
+#define SLG_MODEL_SEED_STRIDE 0x9E3779B97F4A7C15ULL
+int slg_set_models(slg_ctx* ctx, int32_t nmodel, const int32_t* nx, const int64_t* npart,
+                   const double* xarr, const double* vxarr, const double* vol, const double* divv);
+
 /* Permanent atomic data after bcast_permanent (mpimod_mpi.f:23-501):
  * ion_el(iz)%ni (nelem), the bb line list sorted by wl0 (read_bbxs_data.f:84),
  * bf_ph1(6,7,30,30), bf_ph2(7,30,30) (bfxsmod.f:14) and ff_gff(81,41)
@@ -83,6 +103,36 @@ int slg_set_grid(slg_ctx* ctx, int32_t nx, const double* xarr, const double* vxa
 int slg_set_atomic_data(slg_ctx* ctx, int32_t nelem, int32_t nstage, const int32_t* ion_ni,
                         int64_t nline, const slg_bbxs* bb_xs, const float* bf_ph1,
                         const float* bf_ph2, const double* ff_gff);
+
+/* ------------------------------------------------------------------ equation of state */
+
+/* Partition functions of ions_solve_eos (ionsmod.f:206-215) at temperature
+ * temp (host computation): q(ii,iz) = sum_k glev(k,ii,iz) exp(-elev(k,ii,iz)/kT)
+ * for stages 1..ni-1 and 1 for stage ni.  glev, elev (nlev, nstage, nelem) with
+ * elev in erg, nlevel (nstage, nelem), q (nstage, nelem).  The reference
+ * evaluates them once, at the temperature of the first cell of its first EOS
+ * call, and keeps them. */
+void slg_partition_functions(int32_t nelem, int32_t nstage, int32_t nlev, const int32_t* ni,
+                             const int32_t* nlevel, const double* glev, const double* elev,
+                             double temp, double* q);
+
+/* Ion data of the equation of state (ionsmod.f ion_el after ions_read_data):
+ * ni (nelem) stages including the bare ion, and (nstage, nelem) each: e the
+ * ionisation energy of stage ii to ii+1 [erg], q the partition functions,
+ * g1 the ground-level weights glev(1).  nelem <= 32, nstage <= 32. */
+int slg_set_ions(slg_ctx* ctx, int32_t nelem, int32_t nstage, const int32_t* ni, const double* e,
+                 const double* q, const double* g1);
+
+/* ions_solve_eos (ionsmod.f:160-356) for every cell, then eos_update's ground
+ * states (GAS/eos_update.f:37-45).  nelec (ncell) is the start value on entry
+ * (the previous step's, as in the reference) and the converged electrons per
+ * atom on return; acc is the convergence limit on |nelec/nelec_new - 1|
+ * (reference 1e-8).  oc, ginv (ncell, noc, nelem) for stages 1..noc (0 and 1
+ * beyond ni); iconv (ncell, optional) the iteration count (41: not converged,
+ * -1: a cell where the reference stops).  natomfr is (0:nelem, ncell). */
+int slg_saha_eos(slg_ctx* ctx, const double* temp, const double* natom, const double* vol,
+                 const double* natomfr, double acc, double* nelec, int32_t noc, double* oc,
+                 double* ginv, int32_t* iconv);
 
 /* ------------------------------------------------------------------ opacity */
 
@@ -208,6 +258,11 @@ int slg_sourceenergy(slg_ctx* ctx, const double* radtemp, double L_bol, double* 
  * error (vacancies < emitting cells, no particles, surplus > ncell). */
 int64_t slg_sourcenumbers(slg_ctx* ctx, const double* emit, double srcepwr, int64_t src_ns,
                           int64_t nvacant, int32_t* nvol);
+/* sourcenumbers for each model of slg_set_models: src_ns[m] particles and
+ * nvacant[m] vacancies for model m; nvol over all cells.  Returns the total
+ * src_nnew or a negative error. */
+int64_t slg_models_sourcenumbers(slg_ctx* ctx, const double* emit, double srcepwr,
+                                 const int64_t* src_ns, const int64_t* nvacant, int32_t* nvol);
 
 /* vacancies + interior_source + source_transformdirection
  * (SOURCE/vacancies.f90, SOURCE/interior_source.f90:3-172,
@@ -227,6 +282,9 @@ int slg_dev_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity
                              double* gas_sig, float* gas_cap, float* gas_emiss, double* cap64);
 int slg_dev_opacity_means(slg_ctx* ctx, const double* temp, const double* sig,
                           const float* gas_cap, double* capgrey, double* capross);
+int slg_dev_saha_eos(slg_ctx* ctx, const double* temp, const double* natom, const double* vol,
+                     const double* natomfr, double acc, double* nelec, int32_t noc, double* oc,
+                     double* ginv, int32_t* iconv);
 int slg_dev_leakage_opacity11(slg_ctx* ctx, const double* tempinv, const double* sig,
                               const float* cap, const float* capemit, double tauddmc,
                               double taulump, double* opaclump);
@@ -241,10 +299,11 @@ int slg_dev_fluxtally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, int32_
 int slg_dev_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt,
                         const int32_t* isvacant, double* src_energy, int32_t* src_number);
 /* Transport autotuner (library addition): runs each compiled variant of the
- * particle-loop kernel (register budget / resident blocks per SM) on a copy of
- * the first nsample particles (device pointers; inputs are left unchanged),
- * times it and keeps the fastest for this context.  *best (optional) receives
- * the variant, ms (optional, 4 entries) the times. */
+ * particle-loop kernel of in->precision (register budget / resident blocks
+ * per SM) on a copy of the first nsample particles (device pointers; inputs
+ * are left unchanged), times it and keeps the fastest for this context and
+ * precision.  *best (optional) receives the variant, ms (optional, 4
+ * entries) the times. */
 int slg_autotune_transport(slg_ctx* ctx, const slg_transport_in* in, const slg_packet* prt,
                            const int32_t* isvacant, int64_t npart, uint64_t seed,
                            int64_t nsample, int32_t* best, float* ms);
@@ -287,6 +346,29 @@ typedef struct slg_grid_dev {
 int slg_particle_advance_static(const slg_grid_dev* grid, const slg_transport_in* in,
                                 slg_packet* prt, int32_t* isvacant, int64_t npart,
                                 uint64_t seed, slg_transport_out* out, void* stream);
+
+/* ------------------------------------------------------------------ CUDA graphs */
+/* Capture the work that slg_dev_* calls queue on the context's stream
+ * between slg_graph_begin and slg_graph_end into one executable CUDA graph
+ * held by the context (no counterpart in the reference).  Make one
+ * uncaptured pass of the same calls first: a call that needs a new device
+ * buffer, an upload of changed host data (interior_source re-uploads its
+ * set-up only when emit/nvol change) or a host wait makes slg_graph_end
+ * fail.  slg_graph_launch replays the graph nlaunch times.  Replay r, counted
+ * from 0 after slg_graph_end, draws every random number of the captured
+ * transport and source calls from the Philox counter word
+ * 3 = stream | r << 2, so replay 0 equals the same calls made directly and
+ * later replays draw fresh numbers.  Transport counters of replays are read
+ * with slg_transport_totals. */
+int slg_graph_begin(slg_ctx* ctx);
+int slg_graph_end(slg_ctx* ctx);
+int slg_graph_launch(slg_ctx* ctx, int32_t nlaunch);
+/* Counters of every particle_advance (direct or replayed) since the context
+ * was made or last reset, summed (nstepmax: maximum; ierr/ierr_part: the
+ * lowest error key), written to the scalar fields of *out (tot_* are set, not
+ * added); arrays of *out are not touched.  Waits for the stream; reset != 0
+ * zeroes the sums.  Returns the first transport error code (0 if none). */
+int slg_transport_totals(slg_ctx* ctx, slg_transport_out* out, int32_t reset);
 
 /* Wait for the context's stream; returns a pending error if any. */
 int slg_sync(slg_ctx* ctx);

@@ -50,6 +50,11 @@ class TrnOut(C.Structure):
                 ("ierr_part", C.c_int32)]
 
 
+class OrcIon(C.Structure):
+    _fields_ = [("nelem", C.c_int32), ("nstage", C.c_int32), ("ni", C.c_void_p), ("e", C.c_void_p),
+                ("q", C.c_void_p), ("g1", C.c_void_p)]
+
+
 def _ptr(a, t):
     if a is None:
         return None
@@ -107,6 +112,9 @@ def lib():
         L.orc_interior_source.restype = C.c_int
         L.orc_interior_source.argtypes = [C.c_int, C.c_int, dp, dp, dp, dp, dp, C.c_double, ip,
                                           C.c_int64, C.c_void_p, ip, C.c_void_p, C.c_int, C.c_uint64]
+        L.orc_partition.argtypes = [C.c_int, C.c_int, C.c_int, ip, ip, dp, dp, C.c_double, dp]
+        L.orc_saha_eos.restype = C.c_int
+        L.orc_saha_eos.argtypes = [C.POINTER(OrcIon), C.c_int, dp, dp, dp, dp, C.c_double, dp, C.c_int32, dp, dp, ip]
         _LIB = L
     return _LIB
 
@@ -337,3 +345,34 @@ def make_source_particles(grid, groups, radtemp, L_bol, src_ns, npart=None, ioff
     if rc != 0:
         raise RuntimeError(f"interior_source failed: {rc}")
     return prt, isv, emit, nvol, float(tot[0])
+
+
+# ---------------------------------------------------------------- equation of state
+def partition(ion, temp):
+    """ionsmod.f:206-215 at one temperature: q (nelem, nstage)."""
+    ni = np.ascontiguousarray(ion.ni, dtype=np.int32)
+    nl = np.ascontiguousarray(ion.nlevel, dtype=np.int32)
+    g, e = f64(ion.glev), f64(ion.elev)
+    q = np.zeros(ion.e.shape)
+    lib().orc_partition(len(ni), ion.e.shape[1], g.shape[2], _ptr(ni, ip), _ptr(nl, ip), _ptr(g, dp), _ptr(e, dp),
+                        float(temp), _ptr(q, dp))
+    return q
+
+
+def saha_eos(ion, q, temp, natom, vol, natomfr, nelec0, acc=1e-8, noc=4):
+    """ions_solve_eos + eos_update for every cell.  Returns nelec, oc and ginv
+    as numpy (nelem, noc, ncell), iconv."""
+    ni = np.ascontiguousarray(ion.ni, dtype=np.int32)
+    e, qq, g1 = f64(ion.e), f64(q), f64(ion.g1)
+    st = OrcIon(len(ni), e.shape[1], ni.ctypes.data, e.ctypes.data, qq.ctypes.data, g1.ctypes.data)
+    t, na, v, fr = f64(temp), f64(natom), f64(vol), f64(natomfr)
+    nc = len(t)
+    nel = f64(nelec0).copy()
+    oc = np.zeros((len(ni), noc, nc))
+    ginv = np.zeros((len(ni), noc, nc))
+    it = np.zeros(nc, dtype=np.int32)
+    rc = lib().orc_saha_eos(C.byref(st), nc, _ptr(t, dp), _ptr(na, dp), _ptr(v, dp), _ptr(fr, dp), float(acc),
+                            _ptr(nel, dp), int(noc), _ptr(oc, dp), _ptr(ginv, dp), _ptr(it, ip))
+    if rc != 0:
+        raise RuntimeError(f"orc_saha_eos stopped at cell {-rc - 1}")
+    return nel, oc, ginv, it

@@ -49,6 +49,31 @@ void orc_spectintv(double tempinv, const double* wlinv, int ng, int n, int offse
 double orc_planck(double wl, double temp);
 int orc_binsrch(double x, const double* arr, int n, int widerange);
 
+/* ---------------- LTE equation of state ---------------- */
+/* Ion data of ions_read_data (ionsmod.f:652-829) for nelem elements, stage
+ * slots per element nstage (>= every ni): ni (nelem) stages including the bare
+ * ion; e (nstage, nelem) ionisation energy of stage ii to ii+1 [erg]; q
+ * (nstage, nelem) partition functions; g1 (nstage, nelem) ground-level weights. */
+typedef struct orc_ion {
+  int32_t nelem, nstage;
+  const int32_t* ni;
+  const double* e;
+  const double* q;
+  const double* g1;
+} orc_ion;
+/* Partition functions as ions_solve_eos evaluates them (ionsmod.f:206-215) at
+ * one temperature: q = sum_k glev exp(-elev/(kb temp)) for stages 1..ni-1,
+ * 1 for stage ni.  glev, elev (nlev, nstage, nelem), nlevel (nstage, nelem). */
+void orc_partition(int nelem, int nstage, int nlev, const int32_t* ni, const int32_t* nlevel,
+                   const double* glev, const double* elev, double temp, double* q);
+/* ions_solve_eos (ionsmod.f:160-356) and eos_update (GAS/eos_update.f:20-45)
+ * for every cell: nelec (ncell) in/out, accuracy acc (reference 1e-8), oc and
+ * ginv (ncell, noc, nelem) for stages 1..noc, iconv (ncell, optional) the
+ * iteration count.  Returns 0, or -(cell+1) where the reference stops. */
+int orc_saha_eos(const orc_ion* ion, int ncell, const double* temp, const double* natom, const double* vol,
+                 const double* natomfr, double acc, double* nelec, int32_t noc, double* oc, double* ginv,
+                 int32_t* iconv);
+
 /* ---------------- opacity ---------------- */
 double orc_bfxs(const float* bf_ph1, const float* bf_ph2, int nz, int ne, double e);
 

@@ -104,6 +104,22 @@ class HotPath:
         self._check(self.lib.slg_set_grid(self.h, len(x) - 1, ptr(x), ptr(vx), ptr(v), ptr(dv)))
         self.nx = len(x) - 1
         self.xarr = x
+        self.nmodel = 1
+
+    def set_models(self, nx, npart, xarr, vxarr, vol, divv):
+        """Several independent models in this context (slg_set_models): nx[m]
+        shells and npart[m] particle slots each; xarr/vxarr concatenate each
+        model's nx[m]+1 edges, vol/divv each model's cells."""
+        n = np.ascontiguousarray(nx, dtype=np.int32)
+        npt = np.ascontiguousarray(npart, dtype=np.int64)
+        x, vx, v, dv = _f64(xarr), _f64(vxarr), _f64(vol), _f64(divv)
+        assert len(x) == n.sum() + len(n) and len(v) == n.sum() and len(npt) == len(n)
+        self._check(self.lib.slg_set_models(self.h, len(n), ptr(n), ptr(npt), ptr(x), ptr(vx), ptr(v), ptr(dv)))
+        self.nx = int(n.sum())
+        self.xarr = x
+        self.nmodel = len(n)
+        self.model_nx = n
+        self.model_npart = npt
 
     def set_atomic_data(self, ion_ni, nstage, lines, bf_ph1, bf_ph2, ff_gff):
         ni = np.ascontiguousarray(ion_ni, dtype=np.int32)
@@ -238,18 +254,21 @@ class HotPath:
         return out
 
     def fluxtally(self, prt, isvacant, flx_wl):
+        rows = getattr(self, "nmodel", 1)  # one row of groups per model
         if _is_torch(prt):
             import torch
             ng = flx_wl.shape[0] - 1
-            lum = torch.empty(ng, dtype=torch.float64, device=prt.device)
+            shape = (rows, ng) if rows > 1 else (ng,)
+            lum = torch.empty(shape, dtype=torch.float64, device=prt.device)
             dev = torch.empty_like(lum)
-            num = torch.empty(ng, dtype=torch.int32, device=prt.device)
+            num = torch.empty(shape, dtype=torch.int32, device=prt.device)
             self._check(self.lib.slg_dev_fluxtally(self.h, int(prt.shape[0]), ptr(prt), ptr(isvacant), ng, ptr(flx_wl),
                                                    ptr(lum), ptr(dev), ptr(num)))
             return lum, dev, num
         w = _f64(flx_wl)
         ng = len(w) - 1
-        lum, dev, num = np.zeros(ng), np.zeros(ng), np.zeros(ng, dtype=np.int32)
+        shape = (rows, ng) if rows > 1 else (ng,)
+        lum, dev, num = np.zeros(shape), np.zeros(shape), np.zeros(shape, dtype=np.int32)
         self._check(self.lib.slg_fluxtally(self.h, len(prt), ptr(prt), ptr(isvacant), ng, ptr(w), ptr(lum), ptr(dev),
                                            ptr(num)))
         return lum, dev, num
@@ -272,6 +291,72 @@ class HotPath:
         if n < 0:
             self._check(int(n))
         return nvol, int(n)
+
+    def models_sourcenumbers(self, emit, src_ns, nvacant=None, srcepwr=1.0):
+        """sourcenumbers per model (slg_models_sourcenumbers)."""
+        e = _f64(emit)
+        ns = np.ascontiguousarray(src_ns, dtype=np.int64)
+        nv = ns if nvacant is None else np.ascontiguousarray(nvacant, dtype=np.int64)
+        nvol = np.zeros(self.nx, dtype=np.int32)
+        n = self.lib.slg_models_sourcenumbers(self.h, ptr(e), float(srcepwr), ptr(ns), ptr(nv), ptr(nvol))
+        if n < 0:
+            self._check(int(n))
+        return nvol, int(n)
+
+    # ------------------------------------------------------------- equation of state
+    def set_ions(self, ion, q_temp: float):
+        """Ion data (workloads.IonTable) with the partition functions frozen at
+        q_temp, as ions_solve_eos evaluates them once (ionsmod.f:206-215)."""
+        ni = np.ascontiguousarray(ion.ni, dtype=np.int32)
+        nl = np.ascontiguousarray(ion.nlevel, dtype=np.int32)
+        g, el = _f64(ion.glev), _f64(ion.elev)
+        q = np.zeros(ion.e.shape)
+        self.lib.slg_partition_functions(len(ni), ion.e.shape[1], g.shape[2], ptr(ni), ptr(nl), ptr(g), ptr(el),
+                                         float(q_temp), ptr(q))
+        e, g1 = _f64(ion.e), _f64(ion.g1)
+        self._check(self.lib.slg_set_ions(self.h, len(ni), e.shape[1], ptr(ni), ptr(e), ptr(q), ptr(g1)))
+        self.ion_nelem = len(ni)
+        return q
+
+    def saha_eos(self, temp, natom, vol, natomfr, nelec0, acc=1e-8, noc=4):
+        """ions_solve_eos + eos_update: returns nelec, oc, ginv ((nelem, noc, ncell)
+        numpy, or torch tensors on the device when the inputs are) and iconv."""
+        if _is_torch(temp):
+            import torch
+            dev = temp.device
+            nel = nelec0.clone()
+            oc = torch.empty((self.ion_nelem, noc, self.nx), dtype=torch.float64, device=dev)
+            ginv = torch.empty_like(oc)
+            it = torch.empty(self.nx, dtype=torch.int32, device=dev)
+            self._check(self.lib.slg_dev_saha_eos(self.h, ptr(temp), ptr(natom), ptr(vol), ptr(natomfr), float(acc),
+                                                  ptr(nel), int(noc), ptr(oc), ptr(ginv), ptr(it)))
+            return nel, oc, ginv, it
+        t, na, v, fr = _f64(temp), _f64(natom), _f64(vol), _f64(natomfr)
+        nel = _f64(nelec0).copy()
+        oc = np.zeros((self.ion_nelem, noc, self.nx))
+        ginv = np.zeros_like(oc)
+        it = np.zeros(self.nx, dtype=np.int32)
+        self._check(self.lib.slg_saha_eos(self.h, ptr(t), ptr(na), ptr(v), ptr(fr), float(acc), ptr(nel), int(noc),
+                                          ptr(oc), ptr(ginv), ptr(it)))
+        return nel, oc, ginv, it
+
+    # ------------------------------------------------------------- CUDA graphs
+    def graph_begin(self):
+        self._check(self.lib.slg_graph_begin(self.h))
+
+    def graph_end(self):
+        self._check(self.lib.slg_graph_end(self.h))
+
+    def graph_launch(self, n=1):
+        self._check(self.lib.slg_graph_launch(self.h, int(n)))
+
+    def transport_totals(self, reset=False):
+        """Counters summed over every particle_advance since the last reset."""
+        out = capi.SlgTransportOut()
+        rc = self.lib.slg_transport_totals(self.h, C.byref(out), 1 if reset else 0)
+        if rc < 0:
+            self._check(rc)
+        return transport_out_dict(out)
 
     def interior_source(self, radtemp, emit, nvol, prt, isvacant, seed=0):
         """vacancies + interior_source + source_transformdirection.  numpy arrays are

@@ -59,6 +59,7 @@ SIGNATURES = {
     "slg_version": (C.c_char_p, []),
     "slg_set_groups": (C.c_int, [vp, C.c_int32, vp]),
     "slg_set_grid": (C.c_int, [vp, C.c_int32, vp, vp, vp, vp]),
+    "slg_set_models": (C.c_int, [vp, C.c_int32, vp, vp, vp, vp, vp, vp]),
     "slg_set_atomic_data": (C.c_int, [vp, C.c_int32, C.c_int32, vp, C.c_int64, vp, vp, vp, vp]),
     "slg_physical_opacity": (C.c_int, [vp, C.POINTER(SlgGas), C.POINTER(SlgOpacityFlags), vp, vp, vp, vp, vp]),
     "slg_analytic_opacity": (C.c_int, [vp, vp, vp, C.c_int32] + [C.c_double] * 8 + [vp, vp]),
@@ -80,6 +81,7 @@ SIGNATURES = {
     "slg_dev_sourcetally": (C.c_int, [vp, C.c_int64, vp, vp, vp, vp]),
     "slg_sourceenergy": (C.c_int, [vp, vp, C.c_double, vp, vp]),
     "slg_sourcenumbers": (C.c_int64, [vp, vp, C.c_double, C.c_int64, C.c_int64, vp]),
+    "slg_models_sourcenumbers": (C.c_int64, [vp, vp, C.c_double, vp, vp, vp]),
     "slg_interior_source": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_int64, C.c_uint64, vp]),
     "slg_dev_interior_source": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_int64, C.c_uint64, vp]),
     "slg_particle_advance_static": (C.c_int, [C.POINTER(SlgGridDev), C.POINTER(SlgTransportIn), vp, vp, C.c_int64,
@@ -88,6 +90,14 @@ SIGNATURES = {
                                          vp, vp]),
     "slg_set_transport_variant": (C.c_int, [vp, C.c_int32]),
     "slg_sync": (C.c_int, [vp]),
+    "slg_partition_functions": (None, [C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, C.c_double, vp]),
+    "slg_set_ions": (C.c_int, [vp, C.c_int32, C.c_int32, vp, vp, vp, vp]),
+    "slg_saha_eos": (C.c_int, [vp, vp, vp, vp, vp, C.c_double, vp, C.c_int32, vp, vp, vp]),
+    "slg_dev_saha_eos": (C.c_int, [vp, vp, vp, vp, vp, C.c_double, vp, C.c_int32, vp, vp, vp]),
+    "slg_graph_begin": (C.c_int, [vp]),
+    "slg_graph_end": (C.c_int, [vp]),
+    "slg_graph_launch": (C.c_int, [vp, C.c_int32]),
+    "slg_transport_totals": (C.c_int, [vp, vp, C.c_int32]),
     "slg_stream": (vp, [vp]),
 }
 

@@ -20,6 +20,7 @@ int set_error(slg_ctx* ctx, int code, const char* fmt, ...) {
   vsnprintf(buf, sizeof(buf), fmt, ap);
   va_end(ap);
   ctx->err = buf;
+  if (ctx->capturing) ctx->capture_failed = 1;  // the graph would miss this call's work
   return code;
 }
 
@@ -51,6 +52,7 @@ void* scratch(slg_ctx* ctx, int slot, size_t bytes) {
 
 int opacity_flags(slg_ctx* ctx, int32_t* sanity, int32_t* binning);
 int sourcetally_error(slg_ctx* ctx, int* err);
+int finish_particle_advance_acc(const TransportAcc& a, slg_transport_out* out);
 void host_sourceenergy(int nx, const double* xarr, const double* radtemp, double L_bol, double* emit,
                        double* tot_sthermal);
 long long host_sourcenumbers(int nx, const double* emit, double pwr, long long src_ns, long long nvacant,
@@ -103,6 +105,116 @@ void free_dev(void* p) {
   if (p) cudaFree(p);
 }
 
+// The grid of one or more models (grid_setup per model, GRID/grid_setup.f:3-62):
+// per-model shell edges one model after another, per-cell arrays over all cells.
+int set_models(slg_ctx* ctx, const char* fn, int nmodel, const int32_t* nx, const int64_t* npart,
+               const double* xarr, const double* vxarr, const double* vol, const double* divv) {
+  if (!ctx || nmodel < 1 || !nx || !xarr || !vxarr || !vol || !divv)
+    return set_error(ctx, SLG_ERR_ARG, "%s: bad arguments", fn);
+  if (ctx->capturing) return set_error(ctx, SLG_ERR_STATE, "%s: a graph capture is open", fn);
+  std::vector<ModelDesc> md(nmodel);
+  long long nc = 0, np = 0;
+  for (int m = 0; m < nmodel; ++m) {
+    if (nx[m] < 1 || (nmodel > 1 && nx[m] < 2))
+      return set_error(ctx, SLG_ERR_ARG, "%s: model %d has %d shells", fn, m, nx[m]);
+    if (npart && npart[m] < 0) return set_error(ctx, SLG_ERR_ARG, "%s: model %d has %lld particles", fn, m,
+                                                (long long)npart[m]);
+    const double* X = xarr + nc + m;
+    for (int k = 0; k < nx[m]; ++k)
+      if (!(X[k + 1] > X[k]))
+        return set_error(ctx, SLG_ERR_ARG, "%s: xarr of model %d not increasing at %d", fn, m, k);
+    md[m].poff = np;
+    md[m].np = npart ? npart[m] : 0;
+    md[m].nx = nx[m];
+    md[m].co = (int)nc;
+    md[m].xo = (int)(nc + m);
+    md[m].pad = 0;
+    nc += nx[m];
+    np += md[m].np;
+    if (nc > (1 << 30)) return set_error(ctx, SLG_ERR_ARG, "%s: too many shells", fn);
+  }
+  const int ncell = (int)nc, nedge = (int)nc + nmodel;
+  std::vector<int4> cmap;
+  if (nmodel > 1) {
+    cmap.resize(ncell);
+    for (int m = 0; m < nmodel; ++m)
+      for (int i = 0; i < nx[m]; ++i) cmap[md[m].co + i] = make_int4(i + 1, nx[m], md[m].co, m);
+  }
+  cudaSetDevice(ctx->device);
+  int rc = SLG_OK;
+  if (ncell != ctx->nx || nmodel != ctx->nmodel) {
+    free_dev(ctx->d_xarr); free_dev(ctx->d_vxarr); free_dev(ctx->d_vol); free_dev(ctx->d_divv);
+    free_dev(ctx->d_models); free_dev(ctx->d_cellmap);
+    ctx->d_xarr = ctx->d_vxarr = ctx->d_vol = ctx->d_divv = nullptr;
+    ctx->d_models = nullptr;
+    ctx->d_cellmap = nullptr;
+    ctx->nx = 0;
+    ctx->nmodel = 0;
+    rc = cuda_check(ctx, cudaMalloc(&ctx->d_xarr, sizeof(double) * nedge), "alloc xarr");
+    if (!rc) rc = cuda_check(ctx, cudaMalloc(&ctx->d_vxarr, sizeof(double) * nedge), "alloc vxarr");
+    if (!rc) rc = cuda_check(ctx, cudaMalloc(&ctx->d_vol, sizeof(double) * ncell), "alloc vol");
+    if (!rc) rc = cuda_check(ctx, cudaMalloc(&ctx->d_divv, sizeof(double) * ncell), "alloc divv");
+    if (!rc) rc = cuda_check(ctx, cudaMalloc(&ctx->d_models, sizeof(ModelDesc) * nmodel), "alloc models");
+    if (!rc && nmodel > 1) rc = cuda_check(ctx, cudaMalloc(&ctx->d_cellmap, sizeof(int4) * ncell), "alloc cellmap");
+    if (rc) return rc;
+  }
+  cudaStream_t st = ctx->stream;
+  rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_xarr, xarr, sizeof(double) * nedge, cudaMemcpyHostToDevice, st), "xarr");
+  if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_vxarr, vxarr, sizeof(double) * nedge, cudaMemcpyHostToDevice, st), "vxarr");
+  if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_vol, vol, sizeof(double) * ncell, cudaMemcpyHostToDevice, st), "vol");
+  if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_divv, divv, sizeof(double) * ncell, cudaMemcpyHostToDevice, st), "divv");
+  if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_models, md.data(), sizeof(ModelDesc) * nmodel, cudaMemcpyHostToDevice, st), "models");
+  if (!rc && nmodel > 1)
+    rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_cellmap, cmap.data(), sizeof(int4) * ncell, cudaMemcpyHostToDevice, st), "cellmap");
+  if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(st), "grid sync");
+  if (rc) return rc;
+  ctx->nx = ncell;
+  ctx->nmodel = nmodel;
+  ctx->h_models = md;
+  ctx->npart_models = npart ? np : 0;
+  ctx->h_xarr.assign(xarr, xarr + nedge);
+  ctx->tables.nx = ctx->tables.ng = 0;
+  ctx->src_emit.clear();
+  ctx->src_nvol.clear();
+  return SLG_OK;
+}
+
+// Zero the running transport counters (first error: none).
+int reset_totals(slg_ctx* ctx) {
+  int rc = cuda_check(ctx, cudaMemsetAsync(ctx->d_totals, 0, sizeof(TransportAcc), ctx->stream), "totals");
+  if (!rc)
+    rc = cuda_check(ctx, cudaMemsetAsync(&ctx->d_totals->ierr_key, 0xff, sizeof(unsigned long long), ctx->stream),
+                    "totals");
+  return rc;
+}
+
+__global__ void epoch_bump_kernel(unsigned long long* e) { *e += 1ull; }
+
+int check_model_particles(slg_ctx* ctx, int64_t npart);
+
+// fluxtally per model: model m's escaped particles go to rows m of
+// luminos/lumdev/lumnum (flx_ng entries each).
+int fluxtally_models(slg_ctx* ctx, int64_t npart, const slg_packet* prt, int32_t* isvacant, int flx_ng,
+                     const double* flx_wl, double* luminos, double* lumdev, int32_t* lumnum) {
+  if (ctx->nmodel <= 1) return launch_fluxtally(ctx, npart, prt, isvacant, flx_ng, flx_wl, luminos, lumdev, lumnum);
+  int rc = check_model_particles(ctx, npart);
+  for (int m = 0; m < ctx->nmodel && !rc; ++m) {
+    const ModelDesc& d = ctx->h_models[m];
+    const size_t o = (size_t)m * flx_ng;
+    rc = launch_fluxtally(ctx, d.np, prt + d.poff, isvacant + d.poff, flx_ng, flx_wl, luminos + o, lumdev + o,
+                          lumnum + o);
+  }
+  return rc;
+}
+
+// Particle count of a call against the models' slot ranges.
+int check_model_particles(slg_ctx* ctx, int64_t npart) {
+  if (ctx->nmodel > 1 && npart != ctx->npart_models)
+    return set_error(ctx, SLG_ERR_ARG, "npart %lld differs from the %lld slots of the models", (long long)npart,
+                     ctx->npart_models);
+  return SLG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -120,7 +232,11 @@ slg_ctx* slg_create(int device) {
   }
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (cudaMalloc(&ctx->d_acc, sizeof(TransportAcc)) != cudaSuccess ||
-      cudaMallocHost(&ctx->h_acc, sizeof(TransportAcc)) != cudaSuccess) {
+      cudaMallocHost(&ctx->h_acc, sizeof(TransportAcc)) != cudaSuccess ||
+      cudaMalloc(&ctx->d_totals, sizeof(TransportAcc)) != cudaSuccess ||
+      cudaMalloc(&ctx->d_epoch, sizeof(unsigned long long)) != cudaSuccess ||
+      reset_totals(ctx) != SLG_OK || cudaMemset(ctx->d_epoch, 0, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
     cudaGetLastError();
     slg_destroy(ctx);
     return nullptr;
@@ -138,6 +254,9 @@ void slg_destroy(slg_ctx* ctx) {
   free_dev(ctx->d_xarr); free_dev(ctx->d_vxarr); free_dev(ctx->d_vol); free_dev(ctx->d_divv);
   free_dev(ctx->d_ion_ni); free_dev(ctx->d_bb); free_dev(ctx->d_ph1); free_dev(ctx->d_ph2);
   free_dev(ctx->d_gff); free_dev(ctx->d_acc);
+  free_dev(ctx->d_totals); free_dev(ctx->d_epoch); free_dev(ctx->d_models); free_dev(ctx->d_cellmap);
+  free_dev(ctx->d_eos_ni); free_dev(ctx->d_eos_e); free_dev(ctx->d_eos_q); free_dev(ctx->d_eos_g1);
+  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
   if (ctx->h_acc) cudaFreeHost(ctx->h_acc);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -149,6 +268,7 @@ void* slg_stream(slg_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 int slg_sync(slg_ctx* ctx) {
   if (!ctx) return SLG_ERR_ARG;
+  if (ctx->capturing) return set_error(ctx, SLG_ERR_STATE, "slg_sync: a graph capture is open");
   int rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "stream sync");
   if (!rc && ctx->pending_out) {
     slg_transport_out* o = ctx->pending_out;
@@ -156,6 +276,79 @@ int slg_sync(slg_ctx* ctx) {
     rc = finish_particle_advance(ctx, nullptr, o);
   }
   return rc;
+}
+
+// ------------------------------------------------------------------ CUDA graphs
+int slg_graph_begin(slg_ctx* ctx) {
+  if (!ctx) return SLG_ERR_ARG;
+  if (ctx->capturing) return set_error(ctx, SLG_ERR_STATE, "slg_graph_begin: a capture is already open");
+  int rc = slg_sync(ctx);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  rc = cuda_check(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  if (!rc) {
+    ctx->capturing = 1;
+    ctx->capture_failed = 0;
+  }
+  return rc;
+}
+
+int slg_graph_end(slg_ctx* ctx) {
+  if (!ctx) return SLG_ERR_ARG;
+  if (!ctx->capturing) return set_error(ctx, SLG_ERR_STATE, "slg_graph_end: no capture is open");
+  cudaSetDevice(ctx->device);
+  epoch_bump_kernel<<<1, 1, 0, ctx->stream>>>(ctx->d_epoch);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  ctx->capturing = 0;
+  ctx->pending_out = nullptr;  // captured calls complete on replay (slg_transport_totals)
+  if (ctx->capture_failed && e == cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return set_error(ctx, SLG_ERR_STATE, "slg_graph_end: a call failed during the capture (%s)", ctx->err.c_str());
+  }
+  if (e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return set_error(ctx, SLG_ERR_CUDA, "slg_graph_end: capture failed (%s); a call during the capture needed "
+                     "an allocation, an upload of changed host data or a host wait", cudaGetErrorString(e));
+  }
+  if (ctx->graph_exec) {
+    cudaGraphExecDestroy(ctx->graph_exec);
+    ctx->graph_exec = nullptr;
+  }
+  int rc = cuda_check(ctx, cudaGraphInstantiate(&ctx->graph_exec, g, 0), "graph instantiate");
+  cudaGraphDestroy(g);
+  if (!rc) rc = cuda_check(ctx, cudaMemsetAsync(ctx->d_epoch, 0, sizeof(unsigned long long), ctx->stream), "epoch");
+  return rc;
+}
+
+int slg_graph_launch(slg_ctx* ctx, int32_t nlaunch) {
+  if (!ctx || nlaunch < 0) return set_error(ctx, SLG_ERR_ARG, "slg_graph_launch: bad argument");
+  if (!ctx->graph_exec || ctx->capturing) return set_error(ctx, SLG_ERR_STATE, "slg_graph_launch: no graph");
+  cudaSetDevice(ctx->device);
+  for (int i = 0; i < nlaunch; ++i) {
+    const int rc = cuda_check(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream), "graph launch");
+    if (rc) return rc;
+  }
+  return SLG_OK;
+}
+
+int slg_transport_totals(slg_ctx* ctx, slg_transport_out* out, int32_t reset) {
+  if (!ctx || !out) return set_error(ctx, SLG_ERR_ARG, "slg_transport_totals: bad argument");
+  int rc = slg_sync(ctx);
+  if (rc > 0) rc = SLG_OK;  // a transport error of the last direct call is reported below as well
+  if (rc) return rc;
+  TransportAcc h;
+  rc = cuda_check(ctx, cudaMemcpy(&h, ctx->d_totals, sizeof(TransportAcc), cudaMemcpyDeviceToHost), "totals");
+  if (rc) return rc;
+  out->tot_evelo = out->tot_eout = out->tot_sflux = 0.0;
+  const int ierr = finish_particle_advance_acc(h, out);
+  if (reset) {
+    rc = reset_totals(ctx);
+    if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "totals reset");
+    if (rc) return rc;
+  }
+  return ierr;
 }
 
 int slg_set_groups(slg_ctx* ctx, int32_t ng, const double* grp_wl) {
@@ -184,30 +377,13 @@ int slg_set_groups(slg_ctx* ctx, int32_t ng, const double* grp_wl) {
 
 int slg_set_grid(slg_ctx* ctx, int32_t nx, const double* xarr, const double* vxarr, const double* vol,
                  const double* divv) {
-  if (!ctx || nx < 1 || !xarr || !vxarr || !vol || !divv)
-    return set_error(ctx, SLG_ERR_ARG, "slg_set_grid: bad arguments");
-  for (int k = 0; k < nx; ++k)
-    if (!(xarr[k + 1] > xarr[k])) return set_error(ctx, SLG_ERR_ARG, "slg_set_grid: xarr not increasing at %d", k);
-  cudaSetDevice(ctx->device);
-  if (nx != ctx->nx) {
-    free_dev(ctx->d_xarr); free_dev(ctx->d_vxarr); free_dev(ctx->d_vol); free_dev(ctx->d_divv);
-    ctx->d_xarr = ctx->d_vxarr = ctx->d_vol = ctx->d_divv = nullptr;
-    int rc = cuda_check(ctx, cudaMalloc(&ctx->d_xarr, sizeof(double) * (nx + 1)), "alloc xarr");
-    if (!rc) rc = cuda_check(ctx, cudaMalloc(&ctx->d_vxarr, sizeof(double) * (nx + 1)), "alloc vxarr");
-    if (!rc) rc = cuda_check(ctx, cudaMalloc(&ctx->d_vol, sizeof(double) * nx), "alloc vol");
-    if (!rc) rc = cuda_check(ctx, cudaMalloc(&ctx->d_divv, sizeof(double) * nx), "alloc divv");
-    if (rc) return rc;
-  }
-  int rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_xarr, xarr, sizeof(double) * (nx + 1), cudaMemcpyHostToDevice, ctx->stream), "xarr");
-  if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_vxarr, vxarr, sizeof(double) * (nx + 1), cudaMemcpyHostToDevice, ctx->stream), "vxarr");
-  if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_vol, vol, sizeof(double) * nx, cudaMemcpyHostToDevice, ctx->stream), "vol");
-  if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(ctx->d_divv, divv, sizeof(double) * nx, cudaMemcpyHostToDevice, ctx->stream), "divv");
-  if (!rc) rc = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "grid sync");
-  if (rc) return rc;
-  ctx->nx = nx;
-  ctx->h_xarr.assign(xarr, xarr + nx + 1);
-  ctx->tables.nx = ctx->tables.ng = 0;
-  return SLG_OK;
+  return set_models(ctx, "slg_set_grid", 1, &nx, nullptr, xarr, vxarr, vol, divv);
+}
+
+int slg_set_models(slg_ctx* ctx, int32_t nmodel, const int32_t* nx, const int64_t* npart, const double* xarr,
+                   const double* vxarr, const double* vol, const double* divv) {
+  if (!npart) return set_error(ctx, SLG_ERR_ARG, "slg_set_models: npart is null");
+  return set_models(ctx, "slg_set_models", nmodel, nx, npart, xarr, vxarr, vol, divv);
 }
 
 int slg_set_atomic_data(slg_ctx* ctx, int32_t nelem, int32_t nstage, const int32_t* ion_ni, int64_t nline,
@@ -299,7 +475,11 @@ int slg_dev_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packe
     return set_error(ctx, SLG_ERR_ARG, "slg_transport_out has a null array");
   if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
   if (ctx->nx < 2) return set_error(ctx, SLG_ERR_ARG, "transport needs at least 2 shells");
-  if (in->precision != 0) return set_error(ctx, SLG_ERR_NOT_BUILT, "precision %d not available", in->precision);
+  if (in->precision != 0 && in->precision != 1)
+    return set_error(ctx, SLG_ERR_NOT_BUILT, "precision %d not available", in->precision);
+  if (ctx->nmodel > 1 && in->precision != 1)
+    return set_error(ctx, SLG_ERR_NOT_BUILT, "transport of several models needs precision 1");
+  if (check_model_particles(ctx, npart)) return SLG_ERR_ARG;
   cudaSetDevice(ctx->device);
   const int rc = launch_particle_advance(ctx, in, prt, isvacant, npart, seed, out, nullptr, nullptr);
   ctx->pending_out = rc ? nullptr : out;
@@ -311,7 +491,7 @@ int slg_dev_fluxtally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, int32_
   if (!ctx || flx_ng < 1 || !flx_wl || !luminos || !lumdev || !lumnum || npart < 0)
     return set_error(ctx, SLG_ERR_ARG, "bad argument");
   cudaSetDevice(ctx->device);
-  return launch_fluxtally(ctx, npart, prt, isvacant, flx_ng, flx_wl, luminos, lumdev, lumnum);
+  return fluxtally_models(ctx, npart, prt, isvacant, flx_ng, flx_wl, luminos, lumdev, lumnum);
 }
 
 int slg_dev_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, const int32_t* isvacant,
@@ -442,7 +622,11 @@ int slg_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packet* p
     return set_error(ctx, SLG_ERR_ARG, "slg_transport_out has a null array");
   if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
   if (ctx->nx < 2) return set_error(ctx, SLG_ERR_ARG, "transport needs at least 2 shells");
-  if (in->precision != 0) return set_error(ctx, SLG_ERR_NOT_BUILT, "precision %d not available", in->precision);
+  if (in->precision != 0 && in->precision != 1)
+    return set_error(ctx, SLG_ERR_NOT_BUILT, "precision %d not available", in->precision);
+  if (ctx->nmodel > 1 && in->precision != 1)
+    return set_error(ctx, SLG_ERR_NOT_BUILT, "transport of several models needs precision 1");
+  if (check_model_particles(ctx, npart)) return SLG_ERR_ARG;
   cudaSetDevice(ctx->device);
   const size_t nc = ctx->nx, ng = ctx->ng, np = (size_t)npart;
   int rc = 0;
@@ -485,17 +669,18 @@ int slg_fluxtally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, int32_t* i
   cudaSetDevice(ctx->device);
   const size_t np = (size_t)npart;
   int rc = 0;
+  const size_t nf = (size_t)flx_ng * (ctx->nmodel > 1 ? ctx->nmodel : 1);  // per model
   const slg_packet* dp = up(ctx, H_G, prt, np, &rc);
   int32_t* dv = up(ctx, H_H, isvacant, np, &rc);
   const double* dw = up(ctx, H_A, flx_wl, (size_t)flx_ng + 1, &rc);
-  double* dl = out_buf<double>(ctx, H_I, flx_ng, &rc);
-  double* dd = out_buf<double>(ctx, H_J, flx_ng, &rc);
-  int32_t* dn = out_buf<int32_t>(ctx, H_K, flx_ng, &rc);
-  if (!rc) rc = launch_fluxtally(ctx, npart, dp, dv, flx_ng, dw, dl, dd, dn);
+  double* dl = out_buf<double>(ctx, H_I, nf, &rc);
+  double* dd = out_buf<double>(ctx, H_J, nf, &rc);
+  int32_t* dn = out_buf<int32_t>(ctx, H_K, nf, &rc);
+  if (!rc) rc = fluxtally_models(ctx, npart, dp, dv, flx_ng, dw, dl, dd, dn);
   down(ctx, isvacant, dv, np, &rc);
-  down(ctx, luminos, dl, flx_ng, &rc);
-  down(ctx, lumdev, dd, flx_ng, &rc);
-  down(ctx, lumnum, dn, flx_ng, &rc);
+  down(ctx, luminos, dl, nf, &rc);
+  down(ctx, lumdev, dd, nf, &rc);
+  down(ctx, lumnum, dn, nf, &rc);
   return finish(ctx, rc);
 }
 
@@ -531,7 +716,10 @@ int slg_autotune_transport(slg_ctx* ctx, const slg_transport_in* in, const slg_p
   if (!in->tempinv || !in->sig || !in->capgrey || !in->emitprob || !in->opaclump || !in->cap)
     return set_error(ctx, SLG_ERR_ARG, "slg_transport_in has a null array");
   if (!need_grid(ctx) || ctx->nx < 2) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
-  if (in->precision != 0) return set_error(ctx, SLG_ERR_NOT_BUILT, "precision %d not available", in->precision);
+  if (in->precision != 0 && in->precision != 1)
+    return set_error(ctx, SLG_ERR_NOT_BUILT, "precision %d not available", in->precision);
+  if (ctx->nmodel > 1 && in->precision != 1)
+    return set_error(ctx, SLG_ERR_NOT_BUILT, "transport of several models needs precision 1");
   cudaSetDevice(ctx->device);
   int b = 0;
   const int rc = autotune_transport(ctx, in, prt, isvacant, npart, seed, nsample, &b, ms);
@@ -549,14 +737,36 @@ int slg_set_transport_variant(slg_ctx* ctx, int32_t variant) {
 int slg_sourceenergy(slg_ctx* ctx, const double* radtemp, double L_bol, double* emit, double* tot_sthermal) {
   if (!ctx || !radtemp || !emit) return set_error(ctx, SLG_ERR_ARG, "null argument");
   if (ctx->nx < 1) return set_error(ctx, SLG_ERR_STATE, "grid not set");
-  host_sourceenergy(ctx->nx, ctx->h_xarr.data(), radtemp, L_bol, emit, tot_sthermal);
+  double tot = 0.0;
+  for (const ModelDesc& d : ctx->h_models) {  // each model renormalised to L_bol
+    double t = 0.0;
+    host_sourceenergy(d.nx, ctx->h_xarr.data() + d.xo, radtemp + d.co, L_bol, emit + d.co, &t);
+    tot += t;
+  }
+  if (tot_sthermal) *tot_sthermal = tot;
   return SLG_OK;
+}
+
+int64_t slg_models_sourcenumbers(slg_ctx* ctx, const double* emit, double srcepwr, const int64_t* src_ns,
+                                 const int64_t* nvacant, int32_t* nvol) {
+  if (!ctx || !emit || !nvol || !src_ns || !nvacant) return set_error(ctx, SLG_ERR_ARG, "bad argument");
+  if (ctx->nx < 1) return set_error(ctx, SLG_ERR_STATE, "grid not set");
+  long long tot = 0;
+  for (int m = 0; m < ctx->nmodel; ++m) {
+    const ModelDesc& d = ctx->h_models[m];
+    if (src_ns[m] < 1) return set_error(ctx, SLG_ERR_ARG, "model %d: src_ns %lld", m, (long long)src_ns[m]);
+    const long long r = host_sourcenumbers(d.nx, emit + d.co, srcepwr, src_ns[m], nvacant[m], nvol + d.co);
+    if (r < 0) return set_error(ctx, SLG_ERR_ARG, "sourcenumbers failed for model %d (%lld)", m, r);
+    tot += r;
+  }
+  return tot;
 }
 
 int64_t slg_sourcenumbers(slg_ctx* ctx, const double* emit, double srcepwr, int64_t src_ns, int64_t nvacant,
                           int32_t* nvol) {
   if (!ctx || !emit || !nvol || src_ns < 1) return set_error(ctx, SLG_ERR_ARG, "bad argument");
   if (ctx->nx < 1) return set_error(ctx, SLG_ERR_STATE, "grid not set");
+  if (ctx->nmodel > 1) return set_error(ctx, SLG_ERR_STATE, "several models: use slg_models_sourcenumbers");
   const long long r = host_sourcenumbers(ctx->nx, emit, srcepwr, src_ns, nvacant, nvol);
   if (r < 0) return set_error(ctx, SLG_ERR_ARG, "sourcenumbers failed (%lld)", r);
   return r;

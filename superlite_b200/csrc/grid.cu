@@ -40,15 +40,36 @@ struct LeakArgs {
   const float *cap, *capemit;
   double tauddmc, taulump;
   double* opaclump;
+  const int4* cellmap;  // {shell, model shells, model first cell, model} per cell; null: one model
 };
+
+// Arguments seen from cell c (0-based over all models): per-cell arrays start
+// at the cell's model, nx is the model's, *i the 1-based shell in the model.
+__device__ inline LeakArgs leak_view(LeakArgs A, int c, int* i) {
+  *i = c + 1;
+  if (A.cellmap) {
+    const int4 m = A.cellmap[c];
+    const int co = m.z;
+    *i = m.x;
+    A.nx = m.y;
+    A.xarr += co + m.w;
+    A.vol += co; A.divv += co; A.tempinv += co; A.sig += co;
+    A.cap += (size_t)co * A.ng;
+    if (A.capemit) A.capemit += (size_t)co * A.ng;
+    A.opaclump += (size_t)11 * co;
+  }
+  return A;
+}
 
 // leakage_opacity11.f90:30-171, one block per cell.  Sums are fixed-shape
 // tree reductions (the reference sums sequentially).
-__global__ void __launch_bounds__(GB) leakage_kernel(const LeakArgs A) {
+__global__ void __launch_bounds__(GB) leakage_kernel(const LeakArgs A0) {
   __shared__ double sh[GB];
   __shared__ double shv[GB];
   __shared__ int shi[GB];
-  const int i = blockIdx.x + 1;  // 1-based cell
+  int i0;
+  const LeakArgs A = leak_view(A0, blockIdx.x, &i0);
+  const int i = i0;  // 1-based cell
   const int l = i, ng = A.ng;
   const double* X = A.xarr - 1;  // 1-based view
   auto dx = [&](int k) { return A.xarr[k] - A.xarr[k - 1]; };
@@ -206,15 +227,40 @@ struct TabArgs {
   const float* cap;
   double tauddmc, taulump;
   CellTables T;
+  const int4* cellmap = nullptr;  // as LeakArgs::cellmap
 };
+
+// Arguments seen from cell c (see leak_view); *ic is the 1-based shell.
+__device__ inline TabArgs tab_view(TabArgs A, int c, int* ic) {
+  *ic = c + 1;
+  if (A.cellmap) {
+    const int4 m = A.cellmap[c];
+    const int co = m.z;
+    const size_t cg = (size_t)co * A.ng;
+    *ic = m.x;
+    A.nx = m.y;
+    A.xarr += co + m.w; A.vxarr += co + m.w;
+    A.divv += co; A.tempinv += co; A.sig += co; A.capgrey += co;
+    A.opaclump += (size_t)11 * co;
+    A.emitprob += (size_t)A.nep * co;
+    A.cap += cg;
+    A.T.specarr += cg; A.T.glumps += cg; A.T.cdf_dop += cg; A.T.cdf_left += cg; A.T.cdf_right += cg;
+    A.T.cdf_scat += cg; A.T.emitcum += cg;
+    A.T.nlump += co;
+    A.T.scal += (size_t)SCAL_N * co;
+  }
+  return A;
+}
 
 // Per-cell transport tables (see CellTables).  Phase A computes every term in
 // parallel; phase B forms the running sums sequentially, one thread per table,
 // in the order of the reference's loops.
-__global__ void __launch_bounds__(GB) cell_tables_kernel(const TabArgs A) {
+__global__ void __launch_bounds__(GB) cell_tables_kernel(const TabArgs A0) {
   __shared__ int warp_l[GB / 32], warp_u[GB / 32];
   __shared__ int base_l, base_u;
-  const int ic = blockIdx.x + 1, ix = ic;
+  int ic0;
+  const TabArgs A = tab_view(A0, blockIdx.x, &ic0);
+  const int ic = ic0, ix = ic;
   const int ng = A.ng;
   const size_t off = (size_t)(ic - 1) * ng;
   const float* capc = A.cap + off;
@@ -402,7 +448,7 @@ __global__ void __launch_bounds__(GB) cell_tables_kernel(const TabArgs A) {
 int launch_leakage(slg_ctx* ctx, const double* tempinv, const double* sig, const float* cap,
                    const float* capemit, double tauddmc, double taulump, double* opaclump) {
   LeakArgs A{ctx->nx, ctx->ng, ctx->d_xarr, ctx->d_vol, ctx->d_divv, tempinv, sig, ctx->d_wlinv,
-             cap, capemit, tauddmc, taulump, opaclump};
+             cap, capemit, tauddmc, taulump, opaclump, ctx->nmodel > 1 ? ctx->d_cellmap : nullptr};
   leakage_kernel<<<ctx->nx, GB, 0, ctx->stream>>>(A);
   return cuda_check(ctx, cudaGetLastError(), "leakage launch");
 }
@@ -443,6 +489,7 @@ int build_cell_tables(slg_ctx* ctx, const slg_transport_in* in) {
   A.tempinv = in->tempinv; A.sig = in->sig; A.capgrey = in->capgrey; A.opaclump = in->opaclump;
   A.emitprob = in->emitprob; A.cap = in->cap; A.tauddmc = in->tauddmc; A.taulump = in->taulump;
   A.T = T;
+  A.cellmap = ctx->nmodel > 1 ? ctx->d_cellmap : nullptr;
   cell_tables_kernel<<<nx, GB, 0, ctx->stream>>>(A);
   return cuda_check(ctx, cudaGetLastError(), "cell tables launch");
 }

@@ -532,7 +532,11 @@ int launch_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_
     const size_t shm = 16 + sizeof(double) * nedge_pad + sizeof(unsigned int) * (nedge + 1);
     if (shm > 220 * 1024)
       return set_error(ctx, SLG_ERR_ARG, "too many sub-groups for line binning (%d)", ngsub);
-    cudaFuncSetAttribute(bin_lines_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    static size_t shm_set = 0;  // raised only when needed (no attribute calls on repeated launches)
+    if (shm > shm_set) {
+      cudaFuncSetAttribute(bin_lines_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+      shm_set = 220 * 1024;
+    }
     const int64_t per_block = 256 * 8;
     const int nb = (int)((ctx->nline + per_block - 1) / per_block);
     bin_lines_kernel<<<nb, 256, shm, st>>>(ctx->d_bb, ctx->nline, d_wlsub, nedge, nedge_pad, d_counts,

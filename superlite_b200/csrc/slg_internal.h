@@ -43,6 +43,17 @@ struct TransportAcc {
   unsigned long long next;      // persistent-kernel work counter
 };
 
+// One ejecta model of a multi-model context: particle slots [poff, poff+np),
+// cells [co, co+nx) of every per-cell array, shell edges [xo, xo+nx] of
+// xarr/vxarr (xo = co + model index).
+struct ModelDesc {
+  long long poff, np;
+  int nx, co, xo, pad;
+};
+
+// Random-number key of model m: seed + m * kModelSeedStride (SLG_MODEL_SEED_STRIDE).
+constexpr unsigned long long kModelSeedStride = 0x9E3779B97F4A7C15ULL;
+
 }  // namespace slg
 
 struct slg_ctx {
@@ -71,6 +82,13 @@ struct slg_ctx {
   float* d_ph2 = nullptr;
   double* d_gff = nullptr;
   std::vector<float> h_ph1, h_ph2;
+  // ion data of the equation of state: stages, ionisation energies,
+  // partition functions and ground-level weights, (nstage, nelem) each
+  int eos_nelem = 0, eos_nstage = 0;
+  int32_t* d_eos_ni = nullptr;
+  double* d_eos_e = nullptr;
+  double* d_eos_q = nullptr;
+  double* d_eos_g1 = nullptr;
   // derived per-call scratch
   slg::DevBuf scratch[64];
   slg::CellTables tables;
@@ -80,9 +98,29 @@ struct slg_ctx {
   uint64_t* trace_hash = nullptr;
   int32_t* trace_nstep = nullptr;
   // launch configuration chosen by the autotuner (0 = defaults)
-  int trn_variant = 0;  // transport kernel variant (see launch_transport_variant)
+  int trn_variant = 0;  // FP64 transport kernel variant (see launch_transport_variant)
+  int mix_variant = 0;  // mixed-precision variant (see launch_transport_mixed)
   // transport_out of a queued slg_dev_particle_advance, completed by slg_sync
   slg_transport_out* pending_out = nullptr;
+  // models (one for slg_set_grid): host descriptors, device copies, and the
+  // per-cell map {local 1-based shell, model nx, model first cell, model}
+  int nmodel = 0;
+  std::vector<slg::ModelDesc> h_models;
+  slg::ModelDesc* d_models = nullptr;
+  int4* d_cellmap = nullptr;  // null for a single model
+  long long npart_models = 0;  // sum of the models' particle slots (0: one unranged model)
+  // running sums of the transport counters over launches (device; they
+  // survive graph replays), the replay counter that offsets the random
+  // streams of captured launches, and the captured graph
+  slg::TransportAcc* d_totals = nullptr;
+  unsigned long long* d_epoch = nullptr;
+  int capturing = 0;
+  int capture_failed = 0;  // a call failed during the open capture
+  cudaGraphExec_t graph_exec = nullptr;
+  // host copies of the last uploaded source set-up (an unchanged set-up is
+  // not uploaded again, so captured steps hold no host copies)
+  std::vector<double> src_emit;
+  std::vector<int32_t> src_nvol;
   int num_sms = 0;
 };
 

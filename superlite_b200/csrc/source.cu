@@ -13,6 +13,7 @@
 // in the reference's draw order, so any number of particles are made in
 // parallel and the CPU oracle reproduces them exactly.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include "slg_device.cuh"
@@ -124,7 +125,34 @@ struct SrcArgs {
   slg_packet* prt;
   int32_t* isvacant;
   int* flags;
+  // several models: per-cell map {shell, model shells, model first cell,
+  // model}, model descriptors and the count of vacant slots before each
+  // model's first slot; null for one model
+  const int4* cellmap;
+  const ModelDesc* models;
+  const unsigned long long* vbase;
+  const unsigned long long* epoch;  // replay counter of a captured graph (may be null)
 };
+
+// Vacant slots before each model's first slot (vbase[nmodel] = all), from the
+// scanned 1024-slot block counts and a count inside the block.
+__global__ void model_vacancy_base_kernel(int nmodel, long long npart, const int32_t* __restrict__ isvacant,
+                                          const ModelDesc* __restrict__ models, int nblk,
+                                          const unsigned int* __restrict__ offsets,
+                                          const unsigned long long* __restrict__ total,
+                                          unsigned long long* __restrict__ vbase) {
+  const int m = blockIdx.x;
+  const long long p0 = m < nmodel ? models[m].poff : npart;
+  const long long b = p0 / 1024;
+  if (b >= nblk) {
+    if (threadIdx.x == 0) vbase[m] = *total;
+    return;
+  }
+  unsigned int n = 0;
+  for (long long ip = b * 1024 + threadIdx.x; ip < p0; ip += 32) n += isvacant[ip] != 0;
+  for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
+  if (threadIdx.x == 0) vbase[m] = offsets[b] + n;
+}
 
 // interior_source.f90:193-268 and source_transformdirection.f90:20-44
 __global__ void __launch_bounds__(SB) source_particle_kernel(const SrcArgs A) {
@@ -137,11 +165,33 @@ __global__ void __launch_bounds__(SB) source_particle_kernel(const SrcArgs A) {
     if (A.cstart[mid] <= k) lo = mid;
     else hi = mid;
   }
-  const int i = lo + 1;
-  const long long ivac = A.ivacant[k];
+  int i = lo + 1;  // shell within the model from here on
+  int nx = A.nx, co = 0, m = 0;
+  long long poff = 0, kv = k;  // kv: rank of the slot among the model's vacancies
+  const double *xarr = A.xarr, *vxarr = A.vxarr, *emit = A.emit;
+  const int32_t* nvol = A.nvol;
+  if (A.cellmap) {
+    const int4 cm = A.cellmap[lo];
+    co = cm.z;
+    m = cm.w;
+    i = cm.x;
+    nx = cm.y;
+    poff = A.models[m].poff;
+    kv = (long long)A.vbase[m] + (k - A.cstart[co]);
+    if (kv >= (long long)A.vbase[m + 1]) {  // fewer vacancies than new particles in the model
+      atomicOr(A.flags, 2);
+      return;
+    }
+    xarr += co + m;
+    vxarr += co + m;
+    emit += co;
+    nvol += co;
+  }
+  const long long ivac = A.ivacant[kv];
   PhiloxStream rng;
-  rng.init(A.seed, (uint64_t)ivac, 1u);
-  const double* c = A.cdf + (size_t)(i - 1) * A.ng;
+  rng.init(A.seed + (unsigned long long)m * kModelSeedStride, (uint64_t)(ivac - poff),
+           1u | (A.epoch ? (uint32_t)(*A.epoch << 2) : 0u));
+  const double* c = A.cdf + (size_t)(co + i - 1) * A.ng;
   double r1 = rng.draw();
   int a = 0, b = A.ng;  // first g with c[g] > r1, else the last group
   while (a < b) {
@@ -152,20 +202,20 @@ __global__ void __launch_bounds__(SB) source_particle_kernel(const SrcArgs A) {
   const int iig = a < A.ng ? a + 1 : A.ng;
   r1 = rng.draw();
   const double wl0 = 1.0 / ((1.0 - r1) * A.wlinv[iig - 1] + r1 * A.wlinv[iig]);
-  const int nemit = A.nvol[i - 1];
-  const double ep0 = A.emit[i - 1] / (double)nemit;
+  const int nemit = nvol[i - 1];
+  const double ep0 = emit[i - 1] / (double)nemit;
   r1 = rng.draw();
   const double mu0 = sqrt(r1);
   r1 = rng.draw();
   const double om0 = pc_pi2 * r1;
-  const int icnb1 = max(i - 1, 1), icnb2 = min(i + 1, A.nx);
-  const double el = A.emit[i - 1];
-  double uul = 0.5 * (A.emit[icnb1 - 1] + el);
-  double uur = 0.5 * (A.emit[icnb2 - 1] + el);
+  const int icnb1 = max(i - 1, 1), icnb2 = min(i + 1, nx);
+  const double el = emit[i - 1];
+  double uul = 0.5 * (emit[icnb1 - 1] + el);
+  double uur = 0.5 * (emit[icnb2 - 1] + el);
   const double uumax = uul > uur ? uul : uur;
   uul = uul / uumax;
   uur = uur / uumax;
-  const double Xa = A.xarr[i - 1], Xb = A.xarr[i];
+  const double Xa = xarr[i - 1], Xb = xarr[i];
   double r3 = 0.0, r2 = 1.0, x0 = Xa;
   int guard = 0;
   while (r2 > r3) {
@@ -177,9 +227,9 @@ __global__ void __launch_bounds__(SB) source_particle_kernel(const SrcArgs A) {
     if (++guard > 100000) { atomicOr(A.flags, 1); break; }  // acceptance is >= 1/4 in practice
   }
   // direction2lab1 on the interpolated velocity (source_transformdirection.f90:309-324)
-  const int ix = binsrch(x0, A.xarr, A.nx + 1, false);
-  const double vx = (A.vxarr[ix - 1] * (A.xarr[ix] - x0) + A.vxarr[ix] * (x0 - A.xarr[ix - 1])) /
-                    (A.xarr[ix] - A.xarr[ix - 1]);
+  const int ix = binsrch(x0, xarr, nx + 1, false);
+  const double vx = (vxarr[ix - 1] * (xarr[ix] - x0) + vxarr[ix] * (x0 - xarr[ix - 1])) /
+                    (xarr[ix] - xarr[ix - 1]);
   const double cmffact = 1.0 + mu0 * vx * cinv;
   double mu = (mu0 + vx * cinv) / cmffact;
   mu = mu < 1.0 ? mu : 1.0;
@@ -261,18 +311,30 @@ long long host_sourcenumbers(int nx, const double* emit, double pwr, long long s
 int launch_interior_source(slg_ctx* ctx, const double* d_radtemp, const double* h_emit, const int32_t* h_nvol,
                            long long npart, slg_packet* prt, int32_t* isvacant, uint64_t seed, long long* nnew_out) {
   const int nx = ctx->nx, ng = ctx->ng;
+  const bool models = ctx->nmodel > 1;
   cudaStream_t st = ctx->stream;
-  long long nnew = 0;
   std::vector<long long> cstart(nx + 1, 0);
   for (int l = 0; l < nx; ++l) {
     const long long n = h_emit[l] != 0.0 ? h_nvol[l] : 0;
     cstart[l + 1] = cstart[l] + n;
   }
-  nnew = cstart[nx];
+  const long long nnew = cstart[nx];
   if (nnew > npart) return set_error(ctx, SLG_ERR_ARG, "interior_source: %lld new particles > %lld slots", nnew, npart);
+  if (models) {
+    if (npart != ctx->npart_models)
+      return set_error(ctx, SLG_ERR_ARG, "interior_source: npart differs from the models' slots");
+    for (int m = 0; m < ctx->nmodel; ++m) {
+      const ModelDesc& d = ctx->h_models[m];
+      const long long nm = cstart[d.co + d.nx] - cstart[d.co];
+      if (nm > d.np)
+        return set_error(ctx, SLG_ERR_ARG, "interior_source: model %d: %lld new particles > %lld slots", m, nm, d.np);
+    }
+  }
   *nnew_out = nnew;
   std::vector<int32_t> nv(nx);
   for (int l = 0; l < nx; ++l) nv[l] = h_emit[l] != 0.0 ? h_nvol[l] : 0;
+  // all vacancies are listed for several models (each model takes its own)
+  const long long nlist = models ? npart : nnew;
   double* d_emit = (double*)scratch(ctx, 22, sizeof(double) * nx);
   int32_t* d_nvol = (int32_t*)scratch(ctx, 23, sizeof(int32_t) * nx);
   long long* d_cstart = (long long*)scratch(ctx, 24, sizeof(long long) * (nx + 1));
@@ -280,24 +342,44 @@ int launch_interior_source(slg_ctx* ctx, const double* d_radtemp, const double* 
   const long long nblk = (npart + 1023) / 1024;
   unsigned int* d_cnt = (unsigned int*)scratch(ctx, 26, sizeof(unsigned int) * (nblk > 0 ? nblk : 1));
   unsigned long long* d_tot = (unsigned long long*)scratch(ctx, 27, 64);
-  long long* d_ivac = (long long*)scratch(ctx, 28, sizeof(long long) * (nnew > 0 ? nnew : 1));
+  long long* d_ivac = (long long*)scratch(ctx, 28, sizeof(long long) * (nlist > 0 ? nlist : 1));
+  unsigned long long* d_vbase =
+      models ? (unsigned long long*)scratch(ctx, 29, sizeof(unsigned long long) * (ctx->nmodel + 1)) : nullptr;
   int* d_flags = (int*)(d_tot + 2);
-  if (!d_emit || !d_nvol || !d_cstart || !d_cdf || !d_cnt || !d_tot || !d_ivac) return SLG_ERR_OOM;
+  if (!d_emit || !d_nvol || !d_cstart || !d_cdf || !d_cnt || !d_tot || !d_ivac || (models && !d_vbase))
+    return SLG_ERR_OOM;
   if (nnew == 0) return SLG_OK;
-  int rc = cuda_check(ctx, cudaMemcpyAsync(d_emit, h_emit, sizeof(double) * nx, cudaMemcpyHostToDevice, st), "emit");
-  if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(d_nvol, nv.data(), sizeof(int32_t) * nx, cudaMemcpyHostToDevice, st), "nvol");
-  if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(d_cstart, cstart.data(), sizeof(long long) * (nx + 1),
-                                                cudaMemcpyHostToDevice, st), "cstart");
-  // (copies from pageable memory return once the host data is staged)
-  if (rc) return rc;
+  if (nblk > 0x7fffffffLL) return set_error(ctx, SLG_ERR_ARG, "too many particle slots");
+  // the set-up is uploaded only when it changed, so repeated (and captured)
+  // steps hold no host-to-device copies
+  const bool same = ctx->src_emit.size() == (size_t)nx && ctx->src_nvol.size() == (size_t)nx &&
+                    std::equal(nv.begin(), nv.end(), ctx->src_nvol.begin()) &&
+                    std::equal(h_emit, h_emit + nx, ctx->src_emit.begin());
+  if (!same) {
+    if (ctx->capturing)
+      return set_error(ctx, SLG_ERR_STATE, "interior_source: the source set-up changed during a graph capture");
+    ctx->src_emit.clear();
+    ctx->src_nvol.clear();
+    int rc = cuda_check(ctx, cudaMemcpyAsync(d_emit, h_emit, sizeof(double) * nx, cudaMemcpyHostToDevice, st), "emit");
+    if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(d_nvol, nv.data(), sizeof(int32_t) * nx, cudaMemcpyHostToDevice, st), "nvol");
+    if (!rc) rc = cuda_check(ctx, cudaMemcpyAsync(d_cstart, cstart.data(), sizeof(long long) * (nx + 1),
+                                                  cudaMemcpyHostToDevice, st), "cstart");
+    // (copies from pageable memory return once the host data is staged)
+    if (rc) return rc;
+    ctx->src_emit.assign(h_emit, h_emit + nx);
+    ctx->src_nvol = nv;
+  }
   cudaMemsetAsync(d_tot, 0, 64, st);
   source_cdf_kernel<<<nx, SB, 0, st>>>(nx, ng, d_radtemp, ctx->d_wlinv, d_nvol, d_cdf);
   vacancy_count_kernel<<<(unsigned)nblk, 256, 0, st>>>(npart, isvacant, d_cnt);
-  if (nblk > 0x7fffffffLL) return set_error(ctx, SLG_ERR_ARG, "too many particle slots");
   vacancy_scan_kernel<<<1, 1024, 0, st>>>((int)nblk, d_cnt, d_tot);
-  vacancy_write_kernel<<<(unsigned)nblk, 32, 0, st>>>(npart, isvacant, d_cnt, nnew, d_ivac);
+  vacancy_write_kernel<<<(unsigned)nblk, 32, 0, st>>>(npart, isvacant, d_cnt, nlist, d_ivac);
+  if (models)
+    model_vacancy_base_kernel<<<ctx->nmodel + 1, 32, 0, st>>>(ctx->nmodel, npart, isvacant, ctx->d_models,
+                                                             (int)nblk, d_cnt, d_tot, d_vbase);
   SrcArgs A{nx, ng, ctx->d_xarr, ctx->d_vxarr, ctx->d_wlinv, d_emit, d_cdf, d_nvol, d_cstart, d_ivac, nnew, seed,
-            prt, isvacant, d_flags};
+            prt, isvacant, d_flags, models ? ctx->d_cellmap : nullptr, models ? ctx->d_models : nullptr, d_vbase,
+            ctx->capturing ? ctx->d_epoch : nullptr};
   source_particle_kernel<<<(unsigned)((nnew + SB - 1) / SB), SB, 0, st>>>(A);
   return cuda_check(ctx, cudaGetLastError(), "interior_source launch");
 }
@@ -310,6 +392,7 @@ int interior_source_check(slg_ctx* ctx, long long nnew) {
   if (rc) return rc;
   if ((long long)h[0] < nnew) return set_error(ctx, SLG_ERR_ARG, "vacancies: %llu vacant slots < %lld new particles", h[0], nnew);
   if ((int)h[2] & 1) return set_error(ctx, SLG_ERR_CUDA, "interior_source: position rejection did not converge");
+  if ((int)h[2] & 2) return set_error(ctx, SLG_ERR_ARG, "interior_source: a model has fewer vacant slots than new particles");
   return SLG_OK;
 }
 

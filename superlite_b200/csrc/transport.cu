@@ -63,6 +63,8 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
   Ptcl p;
   double y = 0, z = 0, om = 0;
   PhiloxStream rng;
+  // replays of a captured graph draw from counter word 3 = stream | replay << 2
+  const uint32_t sw = A.epoch ? (uint32_t)(*A.epoch << 2) : 0u;
   int istep = 0;
   uint64_t h = 0;
   // register caches of the tallies
@@ -120,7 +122,7 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
             p.stat = 0;
             p.idist = 0;
             istep = 0;
-            rng.init(A.seed, (uint64_t)ip, 0u);
+            rng.init(A.seed, (uint64_t)ip, sw);
             if (TRACE) h = 1469598103934665603ull;
             have = !bad;
           }
@@ -284,24 +286,37 @@ __global__ void sourcetally_kernel(long long npart, const slg_packet* __restrict
                                    const int32_t* __restrict__ isvacant, int nx, int ng,
                                    const double* __restrict__ xarr, const double* __restrict__ wl,
                                    double* __restrict__ src_energy, int32_t* __restrict__ src_number,
-                                   int* __restrict__ err) {
+                                   int* __restrict__ err, int nmodel, const ModelDesc* __restrict__ models) {
   for (long long ip = (long long)blockIdx.x * blockDim.x + threadIdx.x; ip < npart;
        ip += (long long)gridDim.x * blockDim.x) {
     if (isvacant[ip]) continue;
     const slg_packet* q = prt + ip;
+    // the slot's model: shells mnx from cell co, edges from xo
+    int mnx = nx, co = 0, xo = 0;
+    if (nmodel > 1) {
+      int lo = 0, hi = nmodel - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (models[mid].poff <= ip) lo = mid;
+        else hi = mid - 1;
+      }
+      mnx = models[lo].nx;
+      co = models[lo].co;
+      xo = models[lo].xo;
+    }
     const int ig = binsrch(q->wl, wl, ng + 1, false);
-    const int ic = binsrch(q->x, xarr, nx + 1, false);
-    if (ic < 1 || ic > nx) { atomicOr(err, 1); continue; }
+    const int ic = binsrch(q->x, xarr + xo, mnx + 1, false);
+    if (ic < 1 || ic > mnx) { atomicOr(err, 1); continue; }
     if (ig < 1 || ig > ng) { atomicOr(err, 2); continue; }
-    atomicAdd(&src_energy[(size_t)(ig - 1) * nx + (ic - 1)], q->e);
-    atomicAdd(&src_number[(size_t)(ig - 1) * nx + (ic - 1)], 1);
+    atomicAdd(&src_energy[(size_t)(ig - 1) * nx + (co + ic - 1)], q->e);
+    atomicAdd(&src_number[(size_t)(ig - 1) * nx + (co + ic - 1)], 1);
   }
 }
 
 template <bool TRACE, int MINB>
 int launch_one(int num_sms, long long npart, cudaStream_t st, const TrnArgs& A) {
-  int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_kernel<TRACE, MINB>, TRN_BLOCK, 0);
+  static int occ = -1;  // resident blocks per SM, queried once (not during a capture)
+  if (occ < 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_kernel<TRACE, MINB>, TRN_BLOCK, 0);
   long long nblk = (long long)num_sms * (occ > 0 ? occ : 4);
   const long long need = (npart + TRN_BLOCK - 1) / TRN_BLOCK;
   if (need < nblk) nblk = need > 0 ? need : 1;
@@ -310,6 +325,9 @@ int launch_one(int num_sms, long long npart, cudaStream_t st, const TrnArgs& A) 
 }
 
 }  // namespace
+
+int launch_transport_mixed(int variant, int num_sms, long long npart, cudaStream_t st, const TrnArgs& A);
+constexpr int kMixedVariants = 4;
 
 // Transport kernel variants (register budget / resident blocks), see MINB.
 constexpr int kTransportVariants = 4;
@@ -320,6 +338,39 @@ int launch_transport_variant(int v, bool trace, int num_sms, long long npart, cu
     case 3: return trace ? launch_one<true, 8>(num_sms, npart, st, A) : launch_one<false, 8>(num_sms, npart, st, A);
     default: return trace ? launch_one<true, 1>(num_sms, npart, st, A) : launch_one<false, 1>(num_sms, npart, st, A);
   }
+}
+
+// Kernel arguments of one particle_advance over the context's grid and models.
+TrnArgs transport_args(slg_ctx* ctx, const slg_transport_in* in, slg_packet* prt, int32_t* isvacant,
+                       long long npart, uint64_t seed, double* tally, double* jrad, double* eamp,
+                       int32_t* methodswap) {
+  TrnArgs A;
+  A.nx = ctx->nx; A.ng = ctx->ng; A.nep = ctx->nep; A.nepg = ctx->nepg;
+  A.xarr = ctx->d_xarr; A.vxarr = ctx->d_vxarr; A.divv = ctx->d_divv; A.wl = ctx->d_wl; A.wlinv = ctx->d_wlinv;
+  A.tempinv = in->tempinv; A.sig = in->sig; A.capgrey = in->capgrey; A.emitprob = in->emitprob;
+  A.opaclump = in->opaclump; A.cap = in->cap; A.tauddmc = in->tauddmc; A.taulump = in->taulump;
+  A.puretran = in->puretran; A.noampfact = in->noampfact; A.errorfatal = in->errorfatal;
+  A.thm_aniso = in->thm_aniso; A.dogrdtally = in->dogrdtally; A.max_steps = in->max_steps;
+  A.T = ctx->tables; A.prt = prt; A.isvacant = isvacant; A.npart = npart; A.seed = seed;
+  A.tally = tally; A.jrad = jrad; A.eamp = eamp; A.methodswap = methodswap;
+  A.acc = ctx->d_acc; A.trace_hash = nullptr; A.trace_nstep = nullptr;
+  A.epoch = ctx->capturing ? ctx->d_epoch : nullptr;
+  A.nmodel = ctx->nmodel > 1 ? ctx->nmodel : 1;
+  A.models = ctx->nmodel > 1 ? ctx->d_models : nullptr;
+  return A;
+}
+
+// Running sums of the transport counters over launches (sums, max of the
+// longest history, first error).
+__global__ void totals_fold_kernel(const TransportAcc* __restrict__ a, TransportAcc* __restrict__ t) {
+  if (threadIdx.x == 0) {
+    t->evelo += a->evelo; t->eout += a->eout; t->sflux += a->sflux;
+    t->npckt += a->npckt; t->nflux += a->nflux; t->nimc += a->nimc; t->nddmc += a->nddmc;
+    t->nswap += a->nswap; t->nwarn += a->nwarn;
+    t->nmax = a->nmax > t->nmax ? a->nmax : t->nmax;
+    if (a->ierr_key < t->ierr_key) t->ierr_key = a->ierr_key;  // all ones: no error
+  }
+  if (threadIdx.x < 11) t->ndist[threadIdx.x] += a->ndist[threadIdx.x];
 }
 
 int launch_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packet* prt, int32_t* isvacant,
@@ -335,18 +386,19 @@ int launch_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packet
   if (in->dogrdtally && out->methodswap) cudaMemsetAsync(out->methodswap, 0, sizeof(int32_t) * nx, st);
   cudaMemsetAsync(ctx->d_acc, 0, sizeof(TransportAcc), st);
   cudaMemsetAsync(&ctx->d_acc->ierr_key, 0xff, sizeof(unsigned long long), st);
-  TrnArgs A;
-  A.nx = nx; A.ng = ng; A.nep = ctx->nep; A.nepg = ctx->nepg;
-  A.xarr = ctx->d_xarr; A.vxarr = ctx->d_vxarr; A.divv = ctx->d_divv; A.wl = ctx->d_wl; A.wlinv = ctx->d_wlinv;
-  A.tempinv = in->tempinv; A.sig = in->sig; A.capgrey = in->capgrey; A.emitprob = in->emitprob;
-  A.opaclump = in->opaclump; A.cap = in->cap; A.tauddmc = in->tauddmc; A.taulump = in->taulump;
-  A.puretran = in->puretran; A.noampfact = in->noampfact; A.errorfatal = in->errorfatal;
-  A.thm_aniso = in->thm_aniso; A.dogrdtally = in->dogrdtally; A.max_steps = in->max_steps;
-  A.T = ctx->tables; A.prt = prt; A.isvacant = isvacant; A.npart = npart; A.seed = seed;
-  A.tally = out->tally; A.jrad = out->jrad; A.eamp = out->eamp; A.methodswap = out->methodswap;
-  A.acc = ctx->d_acc; A.trace_hash = d_trace_hash; A.trace_nstep = d_trace_nstep;
-  if ((rc = launch_transport_variant(ctx->trn_variant, d_trace_hash != nullptr, ctx->num_sms, npart, st, A)))
-    return set_error(ctx, rc, "particle_advance launch: %s", cudaGetErrorString(cudaGetLastError()));
+  TrnArgs A = transport_args(ctx, in, prt, isvacant, npart, seed, out->tally, out->jrad, out->eamp,
+                             out->methodswap);
+  A.trace_hash = d_trace_hash;
+  A.trace_nstep = d_trace_nstep;
+  if (in->precision == 1) {
+    A.trace_hash = nullptr;  // the mixed form has no per-event trace
+    A.trace_nstep = nullptr;
+    rc = launch_transport_mixed(ctx->mix_variant, ctx->num_sms, npart, st, A);
+  } else {
+    rc = launch_transport_variant(ctx->trn_variant, d_trace_hash != nullptr, ctx->num_sms, npart, st, A);
+  }
+  if (rc) return set_error(ctx, rc, "particle_advance launch: %s", cudaGetErrorString(cudaGetLastError()));
+  totals_fold_kernel<<<1, 32, 0, st>>>(ctx->d_acc, ctx->d_totals);
   return cuda_check(ctx, cudaMemcpyAsync(ctx->h_acc, ctx->d_acc, sizeof(TransportAcc), cudaMemcpyDeviceToHost, st),
                     "transport counters download");
 }
@@ -385,7 +437,11 @@ int launch_fluxtally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, int32_t
   cudaMemsetAsync(lumnum, 0, sizeof(int32_t) * flx_ng, st);
   const size_t shm = (size_t)flx_ng * (2 * sizeof(double) + sizeof(int));
   const int use_smem = shm <= 96 * 1024;
-  if (use_smem) cudaFuncSetAttribute(fluxtally_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  static size_t shm_set = 0;  // raised only when needed (no attribute calls on repeated launches)
+  if (use_smem && shm > shm_set) {
+    cudaFuncSetAttribute(fluxtally_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    shm_set = 96 * 1024;
+  }
   long long nb = (npart + 255) / 256;
   const long long cap = (long long)ctx->num_sms * 4;
   if (nb > cap) nb = cap;
@@ -408,8 +464,11 @@ int launch_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, const
   const long long cap = (long long)ctx->num_sms * 8;
   if (nb > cap) nb = cap;
   if (nb < 1) nb = 1;
+  if (ctx->nmodel > 1 && npart != ctx->npart_models)
+    return set_error(ctx, SLG_ERR_ARG, "sourcetally: npart differs from the models' slots");
   sourcetally_kernel<<<(unsigned)nb, 256, 0, st>>>(npart, prt, isvacant, ctx->nx, ctx->ng, ctx->d_xarr, ctx->d_wl,
-                                                   src_energy, src_number, d_err);
+                                                   src_energy, src_number, d_err,
+                                                   ctx->nmodel > 1 ? ctx->nmodel : 1, ctx->d_models);
   return cuda_check(ctx, cudaGetLastError(), "sourcetally launch");
 }
 
@@ -457,29 +516,23 @@ int autotune_transport(slg_ctx* ctx, const slg_transport_in* in, const slg_packe
   double* eamp = (double*)scratch(ctx, 44, sizeof(double) * nx);
   int32_t* msw = (int32_t*)scratch(ctx, 45, sizeof(int32_t) * nx);
   if (!p || !v || !tally || !jrad || !eamp || !msw) return SLG_ERR_OOM;
-  TrnArgs A;
-  A.nx = nx; A.ng = ng; A.nep = ctx->nep; A.nepg = ctx->nepg;
-  A.xarr = ctx->d_xarr; A.vxarr = ctx->d_vxarr; A.divv = ctx->d_divv; A.wl = ctx->d_wl; A.wlinv = ctx->d_wlinv;
-  A.tempinv = in->tempinv; A.sig = in->sig; A.capgrey = in->capgrey; A.emitprob = in->emitprob;
-  A.opaclump = in->opaclump; A.cap = in->cap; A.tauddmc = in->tauddmc; A.taulump = in->taulump;
-  A.puretran = in->puretran; A.noampfact = in->noampfact; A.errorfatal = in->errorfatal;
-  A.thm_aniso = in->thm_aniso; A.dogrdtally = in->dogrdtally; A.max_steps = in->max_steps;
-  A.T = ctx->tables; A.prt = p; A.isvacant = v; A.npart = n; A.seed = seed;
-  A.tally = tally; A.jrad = jrad; A.eamp = eamp; A.methodswap = msw;
-  A.acc = ctx->d_acc; A.trace_hash = nullptr; A.trace_nstep = nullptr;
+  const TrnArgs A = transport_args(ctx, in, p, v, n, seed, tally, jrad, eamp, msw);
+  const bool mixed = in->precision == 1;
+  const int nvar = mixed ? kMixedVariants : kTransportVariants;
   cudaEvent_t e0, e1;
   if ((rc = cuda_check(ctx, cudaEventCreate(&e0), "event"))) return rc;
   if ((rc = cuda_check(ctx, cudaEventCreate(&e1), "event"))) { cudaEventDestroy(e0); return rc; }
   float bestms = 0.f;
   int bestv = 0;
-  for (int var = 0; var < kTransportVariants && !rc; ++var) {
+  for (int var = 0; var < nvar && !rc; ++var) {
     cudaMemcpyAsync(p, prt, sizeof(slg_packet) * n, cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(v, isvacant, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st);
     cudaMemsetAsync(tally, 0, sizeof(double) * nx, st);
     cudaMemsetAsync(jrad, 0, sizeof(double) * (size_t)nx * ng, st);
     cudaMemsetAsync(ctx->d_acc, 0, sizeof(TransportAcc), st);
     cudaEventRecord(e0, st);
-    rc = launch_transport_variant(var, false, ctx->num_sms, n, st, A);
+    rc = mixed ? launch_transport_mixed(var, ctx->num_sms, n, st, A)
+               : launch_transport_variant(var, false, ctx->num_sms, n, st, A);
     cudaEventRecord(e1, st);
     if (!rc) rc = cuda_check(ctx, cudaEventSynchronize(e1), "autotune sync");
     float t = 0.f;
@@ -490,7 +543,8 @@ int autotune_transport(slg_ctx* ctx, const slg_transport_in* in, const slg_packe
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
-  ctx->trn_variant = bestv;
+  if (mixed) ctx->mix_variant = bestv;
+  else ctx->trn_variant = bestv;
   if (best) *best = bestv;
   return SLG_OK;
 }

@@ -30,6 +30,9 @@ struct TrnArgs {
   TransportAcc* acc;
   uint64_t* trace_hash;
   int32_t* trace_nstep;
+  const unsigned long long* epoch = nullptr;  // replay counter of a captured graph
+  int nmodel = 1;                             // models (read by the mixed-precision kernel)
+  const ModelDesc* models = nullptr;
 };
 
 struct Ptcl {

@@ -1,0 +1,657 @@
+// transport_mixed.cu -- mixed-precision form of the IMC/DDMC particle loop.
+//
+// Same algorithm and event logic as transport_impl.cuh (particle_advance.f90,
+// transport11.f90, diffusion11.f90), with a split of precisions:
+//   FP64: particle position x (shell-radius comparisons and the distance to a
+//         shell boundary), energy weights e/e0, and the tally accumulation
+//         (Kahan-compensated register sums flushed with FP64 atomics);
+//   FP32: free-flight distances, Doppler distance, direction cosine mu, fluid
+//         velocity, wavelength, DDMC event time and leak probabilities, with
+//         fast single-precision log/exp, and 24-bit random numbers (four per
+//         Philox4x32-10 call, stream 2 of the particle).
+// Cell factors whose magnitude leaves the FP32 range are formed in FP64 and
+// rounded once: shell volume factors (x_b^3 - x_a^3 reaches 1e43 cm^3 at a
+// few days, above FLT_MAX), Planck group fractions deep in the Wien tail,
+// and 1/capgrey.  The DDMC branch is
+// picked by comparing r * (sum of rates) against running sums of the rates,
+// with the effective-scatter rate exactly zero when every group is lumped
+// (its FP64 value, (1 - emitlump) caplump, is rounding noise of a sum that is
+// one by construction), so single-precision rounding cannot select the
+// impossible scatter branch.
+// Results agree with the FP64 form statistically, not event by event.
+// Compiled with FMA contraction enabled.
+#include <cuda_runtime.h>
+#include <cfloat>
+#include "slg_device.cuh"
+#include "slg_internal.h"
+#include "transport_impl.cuh"
+
+namespace slg {
+namespace {
+
+constexpr int MIX_BLOCK = 128;
+constexpr float cinvf = (float)cinv;
+constexpr float pc_cf = (float)pc_c;
+constexpr float dextf = (float)pc_dext;
+
+// four 23-bit uniforms per Philox call: (m + 1/2) 2^-23, in (0,1)
+struct PhiloxStream32 {
+  uint32_t k0, k1, pid_lo, pid_hi, stream;
+  uint32_t k;
+  uint32_t w[4];
+  __device__ inline void init(uint64_t seed, uint64_t pid, uint32_t s) {
+    k0 = (uint32_t)seed; k1 = (uint32_t)(seed >> 32);
+    pid_lo = (uint32_t)pid; pid_hi = (uint32_t)(pid >> 32);
+    stream = s;
+    k = 0;
+  }
+  __device__ inline float draw() {
+    const uint32_t j = k & 3u;
+    if (j == 0u) {
+      const u32x4 o = philox4x32_10(u32x4{k >> 2, pid_lo, pid_hi, stream}, k0, k1);
+      w[0] = o.a; w[1] = o.b; w[2] = o.c; w[3] = o.d;
+    }
+    ++k;
+    const uint32_t u = j == 0u ? w[0] : (j == 1u ? w[1] : (j == 2u ? w[2] : w[3]));
+    return ((float)(u >> 9) + 0.5f) * 0x1p-23f;
+  }
+};
+
+struct PtclM {
+  double x, e, e0;
+  float mu, wl, vx;
+  int ix, ig, itype, stat, idist;
+};
+
+__device__ inline void kahan_add(double& s, double& c, double v) {
+  const double y = v - c;
+  const double t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+// relativistic aberration of a direction cosine, (mu + b) / (1 + b mu), kept
+// in [-1, 1]: single-precision rounding can leave |mu| a few ulp above 1,
+// which makes the chord through the centre (1 - mu^2 < 0) undefined
+__device__ inline float aberrate(float mu, float b) {
+  const float m = (mu + b) / (1.0f + b * mu);
+  return fminf(fmaxf(m, -1.0f), 1.0f);
+}
+
+// the particle's model: shells nx, first cell co, first shell edge xo
+struct MView {
+  int nx, co, xo;
+};
+
+// opacity of group ig in cell ic (1-based over all models' cells)
+__device__ inline float capf(const TrnArgs& A, int ig, int ic) {
+  return __ldg(A.cap + (size_t)(ic - 1) * A.ng + (ig - 1));
+}
+
+// one IMC event (transport11.f90) in mixed precision
+__device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& p, PhiloxStream32& rng,
+                                       double& eraddens,
+                                       double& totevelo, int& ierr) {
+  int& ix = p.ix;
+  int& ig = p.ig;
+  float& mu = p.mu;
+  float& wl = p.wl;
+  float& vx = p.vx;
+  const int ic = ix;
+  const int gc = v.co + ic - 1;  // 0-based index of the cell over all models
+  const double* X = A.xarr + v.xo;
+  const double* VX = A.vxarr + v.xo;
+  ierr = 0;
+  eraddens = 0.0;
+  float elabfact = 1.0f - mu * vx * cinvf;
+  const float elabfactold = elabfact;
+  const double* sc = A.T.scal + (size_t)SCAL_N * gc;
+  const float far = (float)sc[SCAL_FAR];
+  const double Xa = X[ix - 1], Xb = X[ix];
+  const double x = p.x, mud = (double)mu;
+  double dbd;
+  int ixnext;
+  if (ix == 1 || mud >= -sqrt(1.0 - sq(Xa / x))) {
+    dbd = fabs(sqrt(sq(Xb) - (1.0 - sq(mud)) * sq(x)) - mud * x);
+    ixnext = ix + 1;
+  } else {
+    dbd = fabs(sqrt(sq(Xa) - (1.0 - sq(mud)) * sq(x)) + mud * x);
+    ixnext = ix - 1;
+  }
+  if (dbd != dbd) { ierr = 1; return; }
+  const float db = (float)dbd;
+  const float sigc = (float)A.sig[gc];
+  float dthm, dcol, ddop;
+  if (sigc > 0.f) dthm = -__logf(rng.draw()) / (elabfact * sigc);
+  else dthm = far;
+  const float capc = capf(A, ig, gc + 1);
+  if (capc <= 0.f) dcol = far;
+  else dcol = -__logf(rng.draw()) / (elabfact * capc);
+  const float dvdr = (float)sc[SCAL_DVDR];
+  if (dvdr > 0.f && ig < A.ng) ddop = 3.0f * pc_cf / (float)A.divv[v.co + ix - 1] * (elabfact - wl * (float)A.wlinv[ig]);
+  else if (dvdr < 0.f && ig > 1) ddop = 3.0f * pc_cf / (float)A.divv[v.co + ix - 1] * (elabfact - wl * (float)A.wlinv[ig - 1]);
+  else ddop = far;
+  if (ddop < 0.f) ddop = far;
+  float d = dcol;
+  int im = 1;
+  if (dthm < d) { d = dthm; im = 2; }
+  if (ddop < d) { d = ddop; im = 3; }
+  if (db < d) { d = db; im = 4; }
+  p.idist = im;
+  if (dcol != dcol || dthm != dthm || ddop != ddop) { ierr = 3; return; }
+  if (d < 0.f) { ierr = 4; return; }
+  // position in FP64; an event at the boundary lands exactly on the shell edge
+  // event kind with the reference's precedence (transport11.f90:256-489)
+  const bool is_thm = d == dthm, is_col = !is_thm && d == dcol;
+  const bool is_b = !is_thm && !is_col && d == db;
+  const double dd = is_b ? dbd : (double)d;
+  const double xnew = sqrt(sq(x) + sq(dd) + 2.0 * dd * x * mud);
+  p.x = xnew;
+  vx = (float)((VX[ix - 1] * (Xb - xnew) + VX[ix] * (xnew - Xa)) / (Xb - Xa));
+  mu = xnew == 0.0 ? 1.0f : fminf(fmaxf((float)((x * mud + dd) / xnew), -1.0f), 1.0f);
+  eraddens = p.e * (double)(elabfact * elabfact) * dd * cinv;
+  elabfact = 1.0f - mu * vx * cinvf;
+  if (xnew < X[0]) {
+    p.x = X[0];
+    vx = (float)VX[0];
+    ix = 1;
+    mu = 1.0f - rng.draw();
+    return;
+  }
+  double help;
+  if (is_thm || is_col) {
+    const float r1 = rng.draw();
+    mu = 1.0f - 2.0f * r1;
+    mu = aberrate(mu, vx * cinvf);
+  } else if (is_b) {
+    if ((mu >= 0.f && ix == v.nx) || ixnext > v.nx) { p.stat = 1; return; }
+  }
+  if (is_thm) {
+    const float f = 1.0f - mu * vx * cinvf;
+    wl = wl * f / elabfact;
+    help = (double)(elabfact / f);
+    totevelo = totevelo + p.e * (1.0 - help);
+    p.e = p.e * help;
+    p.e0 = p.e0 * help;
+  } else if (is_col) {
+    rng.draw();  // the reference's unused draw (transport11.f90:313)
+    const float f = 1.0f - mu * vx * cinvf;
+    help = (double)(elabfact / f);
+    totevelo = totevelo + p.e * (1.0 - help);
+    p.e = p.e * help;
+    p.e0 = p.e0 * help;
+    if (A.ng != 1) {
+      ig = emitgroup_dev(A, (double)rng.draw(), gc + 1);
+      if (((sigc + capf(A, ig, gc + 1)) * (float)(Xb - Xa) >= (float)A.tauddmc) && !A.puretran) p.itype = 2;
+    }
+    if (p.itype == 2) {
+      const double g = (double)(vx * mu * cinvf);
+      totevelo = totevelo + p.e * g;
+      p.e = p.e * (1.0 - g);
+      p.e0 = p.e0 * (1.0 - g);
+    } else {
+      const float r1 = rng.draw();
+      wl = 1.0f / ((1.0f - r1) * (float)A.wlinv[ig - 1] + r1 * (float)A.wlinv[ig]);
+      wl = wl * (1.0f - vx * mu * cinvf);
+    }
+  } else if (is_b) {
+    const bool out = ixnext > ix;
+    const int l = out ? ix + 1 : ix - 1;
+    const float capl = capf(A, ig, v.co + l), sigl = (float)A.sig[v.co + l - 1];
+    const float dxl = (float)(X[l] - X[l - 1]);
+    const double edge = out ? Xb : Xa;
+    if ((sigl + capl) * dxl < (float)A.tauddmc || A.puretran) {
+      p.x = edge;
+      vx = (float)VX[out ? ix : ix - 1];
+      ix = l;
+    } else {
+      mu = aberrate(mu, -vx * cinvf);
+      float hp = (capl + sigl) * dxl;
+      hp = 4.0f / (3.0f * hp + 6.0f * dextf);
+      const float r1 = rng.draw();
+      if (r1 < hp * (1.0f + 1.5f * fabsf(mu))) {
+        p.itype = 2;
+        totevelo = totevelo + p.e * (1.0 - (double)elabfact);
+        p.e = p.e * (double)elabfact;
+        p.e0 = p.e0 * (double)elabfact;
+        wl = wl / elabfact;
+        ix = l;
+      } else {
+        const float a = rng.draw(), b = rng.draw();
+        const float m = a > b ? a : b;
+        mu = out ? -m : m;
+        mu = aberrate(mu, vx * cinvf);
+        p.x = edge;
+        vx = (float)VX[out ? ix : ix - 1];
+      }
+    }
+  } else {  // Doppler shift
+    if (dvdr > 0.f) {
+      if (ig < A.ng) {
+        ig = ig + 1;
+        wl = (float)((A.wl[ig - 1] + 1e-6 * (A.wl[ig] - A.wl[ig - 1])) * (double)elabfactold);
+      } else {
+        const float r1 = rng.draw();
+        wl = 1.0f / (r1 * (float)A.wlinv[A.ng] + (1.0f - r1) * (float)A.wlinv[A.ng - 1]) * elabfact;
+      }
+    } else if (dvdr < 0.f) {
+      if (ig > 1) {
+        wl = (float)((A.wl[ig - 1] + 1e-6 * (A.wl[ig - 2] - A.wl[ig - 1])) * (double)elabfactold);
+        ig = ig - 1;
+      } else {
+        const float r1 = rng.draw();
+        wl = 1.0f / (r1 * (float)A.wlinv[0] + (1.0f - r1) * (float)A.wlinv[1]) * elabfact;
+      }
+    }
+    if (((sigc + capf(A, ig, gc + 1)) * (float)(Xb - Xa) >= (float)A.tauddmc) && !A.puretran) {
+      p.itype = 2;
+      totevelo = totevelo + p.e * (double)(vx * mu * cinvf);
+      p.e = p.e * (double)elabfact;
+      p.e0 = p.e0 * (double)elabfact;
+      wl = wl / elabfact;
+    }
+  }
+}
+
+// one DDMC event (diffusion11.f90) in mixed precision
+__device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& p, PhiloxStream32& rng,
+                                       double& eraddens,
+                                       double& totevelo, int& ierr) {
+  const int ng = A.ng;
+  int& ix = p.ix;
+  int& ig = p.ig;
+  float& mu = p.mu;
+  float& wl = p.wl;
+  float& vx = p.vx;
+  const int ic = ix;
+  const int gc = v.co + ic - 1;  // 0-based index of the cell over all models
+  const double* X = A.xarr + v.xo;
+  const double* VX = A.vxarr + v.xo;
+  ierr = 0;
+  eraddens = 0.0;
+  const double Xa = X[ix - 1], Xb = X[ix];
+  const float dist = (float)(Xb - Xa);
+  const size_t off = (size_t)gc * ng;
+  const double* sc = A.T.scal + (size_t)SCAL_N * gc;
+  const double dx3 = sc[SCAL_DX3];
+  const float sigc = (float)A.sig[gc];
+  const float capc = capf(A, ig, gc + 1);
+  const double tinv = A.tempinv[gc];
+  const float divv = (float)A.divv[v.co + ix - 1];
+  const float tau_l = (float)A.taulump, tau_d = (float)A.tauddmc;
+  const int glump = (capc * dist >= tau_l) ? A.T.nlump[gc] : 0;
+  if ((sigc + capc) * dist < tau_d) { ierr = 100; return; }
+  float emitlump, caplump, doplump, o1, o2;
+  if (glump > 0) {
+    emitlump = (float)sc[SCAL_EMITLUMP];
+    caplump = (float)sc[SCAL_CAPLUMP];
+    doplump = (float)sc[SCAL_DOPLUMP];
+    const double* OL = A.opaclump + (size_t)11 * gc;
+    o1 = (float)OL[0];
+    o2 = (float)OL[1];
+  } else {
+    emitlump = (float)(specint0(tinv, A.wlinv, ig) * sc[SCAL_CAPGREYINV] * (double)capc);
+    caplump = capc;
+    const double spec_ig = A.T.specarr[off + ig - 1];
+    const double divvd = A.divv[v.co + ix - 1];
+    if (ig != ng && divv >= 0.f) doplump = (float)(dopspeccalc(tinv, A.wlinv, ig) * divvd / (spec_ig * 3.0 * pc_c));
+    else if (ig != 1 && divv < 0.f) doplump = (float)(-dopspeccalc(tinv, A.wlinv, ig - 1) * divvd / (spec_ig * 3.0 * pc_c));
+    else doplump = 0.f;
+    // x^2 / (x_b^3 - x_a^3) per face, formed in FP64
+    const float fa = (float)(sq(Xa) / dx3), fb = (float)(sq(Xb) / dx3);
+    if (ix == 1) {
+      o1 = 0.f;
+    } else {
+      const float capl = capf(A, ig, v.co + ix - 1), sigl = (float)A.sig[v.co + ix - 2];
+      const float dxl = (float)(Xa - X[ix - 2]);
+      if ((capl + sigl) * dxl < tau_d) {
+        const float ppl = 4.0f / (3.0f * (capc + sigc) * dist + 6.0f * dextf);
+        o1 = 1.5f * ppl * fa;
+      } else {
+        o1 = 2.0f * fa / ((sigc + capc) * dist + (sigl + capl) * dxl);
+      }
+    }
+    bool lhelp = true;
+    float capl = 0.f, sigl = 0.f, dxl = 0.f;
+    if (ix != v.nx) {
+      capl = capf(A, ig, v.co + ix + 1);
+      sigl = (float)A.sig[v.co + ix];
+      dxl = (float)(X[ix + 1] - Xb);
+      lhelp = (capl + sigl) * dxl < tau_d;
+    }
+    if (lhelp) {
+      const float ppr = 4.0f / (3.0f * (capc + sigc) * dist + 6.0f * dextf);
+      o2 = 1.5f * ppr * fb;
+    } else {
+      o2 = 2.0f * fb / ((sigc + capc) * dist + (sigl + capl) * dxl);
+    }
+  }
+  // branch rates: Doppler, left leak, right leak, effective scatter
+  const float s_dop = doplump, s_left = doplump + o1, s_leak = doplump + (o1 + o2);
+  const float r_scat = glump == ng ? 0.0f : (1.0f - emitlump) * caplump;
+  const float total = s_leak + r_scat;
+  const float ddmct = fabsf(__logf(rng.draw()) / total * cinvf);
+  eraddens = p.e * (double)ddmct;
+  const float u = rng.draw() * total;  // < total: r < 1 rounds below
+  const int16_t* glumps = A.T.glumps + off;
+  int iiig;
+  if (u < s_dop) {
+    if (glump == 0) {
+      iiig = ig;
+    } else {
+      const int q = first_gt(A.T.cdf_dop + off, glump, (double)rng.draw());
+      iiig = divv >= 0.f ? glumps[q] : glumps[glump - 1 - q];
+    }
+    if (divv >= 0.f) {
+      ig = iiig + 1;
+      wl = (float)A.wl[ig - 1];
+      ig = ig < ng ? ig : ng;
+    } else {
+      ig = iiig - 1;
+      wl = (float)A.wl[ig];
+      ig = ig > 1 ? ig : 1;
+    }
+    if ((sigc + capf(A, ig, gc + 1)) * dist < tau_d) {
+      p.itype = 1;
+      mu = 1.0f - 2.0f * rng.draw();
+      const double rr = (double)rng.draw();
+      double x = pow(rr * cube(Xb) + (1.0 - rr) * cube(Xa), third_r4);
+      x = x < Xb ? x : Xb;
+      x = x > Xa ? x : Xa;
+      p.x = x;
+      vx = (float)((VX[ix - 1] * (Xb - x) + VX[ix] * (x - Xa)) / (Xb - Xa));
+      mu = aberrate(mu, vx * cinvf);
+      const float f = 1.0f - vx * mu * cinvf;
+      wl = wl * f;
+      const double help = 1.0 / (double)f;
+      totevelo = totevelo + p.e * (1.0 - help);
+      p.e = p.e * help;
+      p.e0 = p.e0 * help;
+    }
+  } else if (u < s_leak) {
+    const bool right = u >= s_left;
+    p.idist = right ? -4 : -3;
+    if (!right && ix == 1) return;
+    if (right && ix == v.nx) {
+      p.stat = 1;
+      const float a = rng.draw(), b = rng.draw();
+      mu = a > b ? a : b;
+      if (glump != 0) ig = glumps[first_gt(A.T.cdf_right + off, glump, (double)rng.draw())];
+      const float r = rng.draw();
+      wl = 1.0f / (r * (float)A.wlinv[ig] + (1.0f - r) * (float)A.wlinv[ig - 1]);
+      p.x = X[v.nx];
+      vx = (float)VX[v.nx];
+      mu = aberrate(mu, vx * cinvf);
+      mu = mu < 1.0f ? mu : 1.0f;
+      const double help = 1.0 / (double)(1.0f - mu * vx * cinvf);
+      totevelo = totevelo + p.e * (1.0 - help);
+      wl = wl / (float)help;
+      p.e = p.e * help;
+      p.e0 = p.e0 * help;
+      return;
+    }
+    const int l = right ? ix + 1 : ix - 1;
+    iiig = glump == 0 ? ig
+                      : glumps[first_gt((right ? A.T.cdf_right : A.T.cdf_left) + off, glump, (double)rng.draw())];
+    const float dxl = (float)(right ? X[ix + 1] - Xb : Xa - X[ix - 2]);
+    if (((float)A.sig[v.co + l - 1] + capf(A, iiig, v.co + l)) * dxl < tau_d) {
+      p.itype = 1;
+      const float r = rng.draw();
+      wl = 1.0f / (r * (float)A.wlinv[iiig] + (1.0f - r) * (float)A.wlinv[iiig - 1]);
+      p.x = right ? Xb : Xa;
+      vx = (float)VX[right ? ix : ix - 1];
+      const float a = rng.draw(), b = rng.draw();
+      const float m = a > b ? a : b;
+      mu = right ? m : -m;
+      mu = aberrate(mu, vx * cinvf);
+      const float f = 1.0f - vx * mu * cinvf;
+      const double help = 1.0 / (double)f;
+      totevelo = totevelo + p.e * (1.0 - help);
+      p.e = p.e * help;
+      p.e0 = p.e0 * help;
+      wl = wl * f;
+    }
+    ix = l;
+    ig = iiig;
+  } else {
+    p.idist = -2;
+    if (glump == ng) { ierr = 102; return; }
+    if (glump == 0) {
+      iiig = emitgroup_dev(A, (double)rng.draw(), gc + 1);
+    } else {
+      const int q = first_gt(A.T.cdf_scat + off, ng - glump, (double)rng.draw());
+      iiig = glumps[ng - 1 - q];
+    }
+    ig = iiig;
+    if ((sigc + capf(A, ig, gc + 1)) * dist < tau_d) {
+      p.itype = 1;
+      const float r = rng.draw();
+      wl = 1.0f / ((1.0f - r) * (float)A.wlinv[ig - 1] + r * (float)A.wlinv[ig]);
+      mu = 1.0f - 2.0f * rng.draw();
+      const double rr = (double)rng.draw();
+      double x = pow(rr * cube(Xb) + (1.0 - rr) * cube(Xa), third_r4);
+      x = x < Xb ? x : Xb;
+      x = x > Xa ? x : Xa;
+      p.x = x;
+      vx = (float)((VX[ix - 1] * (Xb - x) + VX[ix] * (x - Xa)) / (Xb - Xa));
+      mu = aberrate(mu, vx * cinvf);
+      const float f = 1.0f - vx * mu * cinvf;
+      const double help = 1.0 / (double)f;
+      totevelo = totevelo + p.e * (1.0 - help);
+      p.e = p.e * help;
+      p.e0 = p.e0 * help;
+      wl = wl * f;
+    }
+  }
+  if (p.x < X[0]) { p.stat = 2; return; }
+  const float dv = (float)A.divv[v.co + ix - 1];
+  const double decay = (double)__expf(-dv * ddmct * (1.0f / 3.0f));
+  totevelo = totevelo + p.e * (1.0 - decay);
+  p.e = p.e * decay;
+  p.e0 = p.e0 * decay;
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(MIX_BLOCK, MINB) particle_advance_mixed_kernel(const TrnArgs A) {
+  __shared__ unsigned long long s_cnt[20];
+  __shared__ double s_sum[3];
+  if (threadIdx.x < 20) s_cnt[threadIdx.x] = 0ull;
+  if (threadIdx.x < 3) s_sum[threadIdx.x] = 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  double evelo = 0.0, eout = 0.0, sflux = 0.0;
+  unsigned long long nimc = 0, nddmc = 0, nswap = 0, npckt = 0, nflux = 0, nwarn = 0, nmax = 0;
+  long long ip = -1;
+  bool have = false, queue_done = false;
+  PtclM p;
+  double y = 0, z = 0, om = 0;
+  PhiloxStream32 rng;
+  // replays of a captured graph draw from counter word 3 = 2 | replay << 2
+  const uint32_t sw = 2u | (A.epoch ? (uint32_t)(*A.epoch << 2) : 0u);
+  // the current particle's model (plain integers: a struct updated member by
+  // member in the refill branch lost its shell count on sm_100a builds)
+  int vnx = A.nx, vco = 0, vxo = 0;
+  int istep = 0;
+  int t_ic = 0, j_ic = 0, j_ig = 0;
+  double t_acc = 0.0, t_c = 0.0, j_acc = 0.0, j_c = 0.0;
+  while (true) {
+    __syncwarp();
+    const bool need = !have && !queue_done;
+    const unsigned needm = __ballot_sync(0xffffffffu, need);
+    if (needm) {
+      const int leader = __ffs(needm) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(&A.acc->next, (unsigned long long)__popc(needm));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        const long long cand = (long long)base + __popc(needm & ((1u << lane) - 1u));
+        if (cand >= A.npart) {
+          queue_done = true;
+        } else if (!A.isvacant[cand]) {
+          ip = cand;
+          const double2* q = reinterpret_cast<const double2*>(A.prt + ip);
+          const double2 a = q[0], b = q[1], c = q[2], d = q[3];
+          double x = a.x, mu = b.y, e = c.y, e0 = d.x, wl = d.y;
+          y = a.y; z = b.x; om = c.x;
+          npckt++;
+          // the slot's model (models own consecutive slot ranges)
+          int m = 0;
+          long long poff = 0;
+          if (A.nmodel > 1) {
+            int lo = 0, hi = A.nmodel - 1;
+            while (lo < hi) {
+              const int mid = (lo + hi + 1) >> 1;
+              if (__ldg(&A.models[mid].poff) <= ip) lo = mid;
+              else hi = mid - 1;
+            }
+            m = lo;
+            poff = __ldg(&A.models[m].poff);
+            vnx = __ldg(&A.models[m].nx);
+            vco = __ldg(&A.models[m].co);
+            vxo = __ldg(&A.models[m].xo);
+          }
+          const double* X = A.xarr + vxo;
+          const double* VX = A.vxarr + vxo;
+          int ix = binsrch(x, X, vnx + 1, false);
+          int ig = binsrch(wl, A.wl, A.ng + 1, false);
+          if (ix < 1 || ig < 1) {
+            if (A.errorfatal) atomicMin(&A.acc->ierr_key, ((unsigned long long)(ip + 1) << 32) | 1002u);
+            A.isvacant[ip] = 1;
+          } else {
+            const double tau = (A.sig[vco + ix - 1] + CAPd(A, ig, vco + ix)) * (X[ix] - X[ix - 1]);
+            p.itype = (A.puretran || tau < A.tauddmc) ? 1 : 2;
+            const double vx = (VX[ix - 1] * (X[ix] - x) + VX[ix] * (x - X[ix - 1])) / (X[ix] - X[ix - 1]);
+            if (p.itype == 1) {
+              const double labfact = 1.0 - vx * mu / pc_c;
+              wl = wl * labfact;
+              e = e / labfact;
+              e0 = e0 / labfact;
+            }
+            p.x = x; p.e = e; p.e0 = e0; p.mu = (float)mu; p.wl = (float)wl; p.vx = (float)vx;
+            p.ix = ix; p.ig = ig; p.stat = 0; p.idist = 0;
+            istep = 0;
+            rng.init(A.seed + (unsigned long long)m * kModelSeedStride, (uint64_t)(ip - poff), sw);
+            have = true;
+          }
+        }
+      }
+    }
+    if (__all_sync(0xffffffffu, !have && queue_done)) break;
+    if (!have) continue;
+    istep++;
+    const MView v{vnx, vco, vxo};
+    const int icold = v.co + p.ix, igold = p.ig;  // cell over all models, 1-based
+    double eraddens;
+    int ierr;
+    if (p.itype == 1 || A.puretran) {
+      nimc++;
+      transport11_mix(A, v, p, rng, eraddens, evelo, ierr);
+      if (p.itype != 1) {
+        nswap++;
+        if (A.dogrdtally) atomicAdd(&A.methodswap[icold - 1], 1);
+      }
+    } else {
+      nddmc++;
+      diffusion11_mix(A, v, p, rng, eraddens, evelo, ierr);
+      if (p.itype == 1) {
+        nswap++;
+        if (A.dogrdtally) atomicAdd(&A.methodswap[icold - 1], 1);
+      }
+    }
+    atomicAdd(&s_cnt[9 + (p.idist > -3 ? p.idist : -3) + 3], 1ull);
+    if (icold != t_ic) {
+      if (t_ic > 0) atomicAdd(&A.tally[t_ic - 1], t_acc - t_c);
+      t_ic = icold;
+      t_acc = 0.0;
+      t_c = 0.0;
+    }
+    kahan_add(t_acc, t_c, eraddens);
+    if (icold != j_ic || igold != j_ig) {
+      if (j_ic > 0) atomicAdd(&A.jrad[(size_t)(j_ic - 1) * A.ng + (j_ig - 1)], pc_c * (j_acc - j_c));
+      j_ic = icold;
+      j_ig = igold;
+      j_acc = 0.0;
+      j_c = 0.0;
+    }
+    kahan_add(j_acc, j_c, eraddens);
+    if (p.itype == 1 && p.stat == 0) {
+      if (p.x > A.xarr[v.xo + p.ix] || p.x < A.xarr[v.xo + p.ix - 1] || p.x != p.x) {
+        if (ierr == 0) ierr = -99;
+      }
+    }
+    if (ierr == -99) nwarn++;
+    if (ierr == 0 && A.max_steps > 0 && istep >= A.max_steps && p.stat == 0) ierr = 1001;
+    if (ierr > 0) {
+      if (A.errorfatal) atomicMin(&A.acc->ierr_key, ((unsigned long long)(ip + 1) << 32) | (unsigned)ierr);
+      p.stat = 2;
+    }
+    if (p.stat != 0) {
+      if ((unsigned long long)istep > nmax) nmax = istep;
+      if (p.stat == 2) {
+        A.isvacant[ip] = 1;
+      } else {
+        nflux++;
+        sflux = sflux - p.e;
+        eout = eout + p.e;
+        double2* q = reinterpret_cast<double2*>(A.prt + ip);
+        q[0] = make_double2(DBL_MAX, y);
+        q[1] = make_double2(z, (double)p.mu);
+        q[2] = make_double2(om, p.e);
+        q[3] = make_double2(p.e0, (double)p.wl);
+      }
+      have = false;
+    }
+  }
+  if (t_ic > 0) atomicAdd(&A.tally[t_ic - 1], t_acc - t_c);
+  if (j_ic > 0) atomicAdd(&A.jrad[(size_t)(j_ic - 1) * A.ng + (j_ig - 1)], pc_c * (j_acc - j_c));
+  atomicAdd(&s_sum[0], evelo);
+  atomicAdd(&s_sum[1], eout);
+  atomicAdd(&s_sum[2], sflux);
+  atomicAdd(&s_cnt[0], npckt);
+  atomicAdd(&s_cnt[1], nflux);
+  atomicAdd(&s_cnt[2], nimc);
+  atomicAdd(&s_cnt[3], nddmc);
+  atomicAdd(&s_cnt[4], nswap);
+  atomicMax(&s_cnt[5], nmax);
+  atomicAdd(&s_cnt[6], nwarn);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    atomicAdd(&A.acc->evelo, s_sum[0]);
+    atomicAdd(&A.acc->eout, s_sum[1]);
+    atomicAdd(&A.acc->sflux, s_sum[2]);
+    atomicAdd(&A.acc->npckt, s_cnt[0]);
+    atomicAdd(&A.acc->nflux, s_cnt[1]);
+    atomicAdd(&A.acc->nimc, s_cnt[2]);
+    atomicAdd(&A.acc->nddmc, s_cnt[3]);
+    atomicAdd(&A.acc->nswap, s_cnt[4]);
+    atomicMax(&A.acc->nmax, s_cnt[5]);
+    atomicAdd(&A.acc->nwarn, s_cnt[6]);
+  }
+  if (threadIdx.x < 11 && s_cnt[9 + threadIdx.x]) atomicAdd(&A.acc->ndist[threadIdx.x], s_cnt[9 + threadIdx.x]);
+}
+
+template <int MINB>
+int launch_mixed_one(int num_sms, long long npart, cudaStream_t st, const TrnArgs& A) {
+  static int occ = -1;  // resident blocks per SM, queried once (not during a capture)
+  if (occ < 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_mixed_kernel<MINB>, MIX_BLOCK, 0);
+  long long nblk = (long long)num_sms * (occ > 0 ? occ : MINB);
+  const long long need = (npart + MIX_BLOCK - 1) / MIX_BLOCK;
+  if (need < nblk) nblk = need > 0 ? need : 1;
+  particle_advance_mixed_kernel<MINB><<<(unsigned)nblk, MIX_BLOCK, 0, st>>>(A);
+  return cudaPeekAtLastError() == cudaSuccess ? SLG_OK : SLG_ERR_CUDA;
+}
+
+}  // namespace
+
+// Variants: resident 128-thread blocks per SM requested from the compiler
+// (register budget 128 / 102 / 85 / 64 per thread).
+int launch_transport_mixed(int variant, int num_sms, long long npart, cudaStream_t st, const TrnArgs& A) {
+  switch (variant) {
+    case 1: return launch_mixed_one<5>(num_sms, npart, st, A);
+    case 2: return launch_mixed_one<6>(num_sms, npart, st, A);
+    case 3: return launch_mixed_one<8>(num_sms, npart, st, A);
+    default: return launch_mixed_one<4>(num_sms, npart, st, A);
+  }
+}
+
+}  // namespace slg

@@ -217,6 +217,75 @@ def load_sutherland(path: str) -> np.ndarray:
 
 
 # ------------------------------------------------------------- populations
+@dataclasses.dataclass
+class IonTable:
+    """Ion data of ions_read_data (ionsmod.f:652-829) in the layouts of
+    slg_set_ions: per element iz (1..nelem) ni stages including the bare ion;
+    e (nelem, nstage) ionisation energy of stage ii -> ii+1 [erg]; levels
+    glev/elev (nelem, nstage, nlev) [elev in erg], nlevel (nelem, nstage)."""
+    ni: np.ndarray
+    e: np.ndarray
+    nlevel: np.ndarray
+    glev: np.ndarray
+    elev: np.ndarray
+
+    @property
+    def nelem(self) -> int:
+        return len(self.ni)
+
+    @property
+    def nstage(self) -> int:
+        return self.e.shape[1]
+
+    @property
+    def g1(self) -> np.ndarray:
+        return self.glev[:, :, 0]
+
+
+def ion_table(seed: int = 7, nlev: int = 6) -> IonTable:
+    """Synthetic ion data for all NELEM elements with ION_NI stages: the
+    energies of ION_ENERGY for the config-2 elements (seeded hydrogen-like
+    values for the others), a ground level with a small integer weight and
+    nlev-1 excited levels below the ionisation energy; the bare ion has one
+    level of weight 1."""
+    rng = np.random.default_rng(seed)
+    ns = ION_NI
+    ni = np.full(NELEM, ns, dtype=np.int32)
+    e = np.zeros((NELEM, ns))
+    nlevel = np.zeros((NELEM, ns), dtype=np.int32)
+    glev = np.zeros((NELEM, ns, nlev))
+    elev = np.zeros((NELEM, ns, nlev))
+    for iz in range(1, NELEM + 1):
+        if iz in ION_ENERGY:
+            ev = np.array(ION_ENERGY[iz])
+        else:
+            ev = np.sort(rng.uniform(6.0, 14.0) * np.array([1.0, 2.1, 3.4, 4.9]) * rng.uniform(0.9, 1.1, 4))
+        e[iz - 1, :ns - 1] = ev * PC_EV
+        for ii in range(ns - 1):
+            nlevel[iz - 1, ii] = nlev
+            glev[iz - 1, ii, 0] = float(rng.choice([1, 2, 3, 4, 5, 6, 9]))
+            glev[iz - 1, ii, 1:] = rng.integers(1, 16, nlev - 1).astype(np.float64)
+            elev[iz - 1, ii, 1:] = np.sort(rng.uniform(0.05, 0.8, nlev - 1)) * ev[ii] * PC_EV
+        nlevel[iz - 1, ns - 1] = 1
+        glev[iz - 1, ns - 1, 0] = 1.0
+    return IonTable(ni, e, nlevel, glev, elev)
+
+
+def composition_state(rho: np.ndarray, massfr: np.ndarray, vol: np.ndarray):
+    """massfr2natomfr (GAS/gas_setup.f:101-160) for given mass fractions:
+    gas_mass = rho vol, X renormalised to sum 1, number fractions
+    natomfr(0:nelem) ~ X_z / A_z normalised to 1, gas_natom = mass sum(X_z/A_z) / amu.  massfr is (ncell, NELEM) over
+    elements 1..NELEM; elements without a mass in ELEM_MASS take 2 z amu."""
+    A = np.array([ELEM_MASS.get(z, 2.0 * z) for z in range(1, NELEM + 1)])
+    mass = rho * vol
+    y = (massfr / massfr.sum(axis=1, keepdims=True)) / A
+    s = y.sum(axis=1)
+    natomfr = np.zeros((len(rho), NELEM + 1))
+    natomfr[:, 1:] = y / s[:, None]
+    natom = mass * s / PC_AMU
+    return mass, natom, natomfr
+
+
 def _saha_cell(temp: float, ndens: float, natomfr_el: np.ndarray):
     """Synthetic two-level Saha balance: returns (nelec per atom, stage fractions)."""
     kt = PC_KB * temp
@@ -320,6 +389,65 @@ def opacity_case(ncell: int = 256, ng: int = 2000, nline: int = 500_000, seed: i
     else:
         ph1, ph2, gff = tables
     return OpacityCase(grid, groups, gas, lines, ph1, ph2, gff)
+
+
+@dataclasses.dataclass
+class ModelBatch:
+    """Independent ejecta models laid out for slg_set_models: per-model grids
+    and gas, and the concatenations the library reads (edges model after
+    model, per-cell arrays over all cells)."""
+    models: list            # one OpacityCase per model (shared groups, lines, tables)
+    nx: np.ndarray          # shells per model (int32)
+    npart: np.ndarray       # particle slots per model (int64)
+    t_days: np.ndarray
+    xarr: np.ndarray
+    vxarr: np.ndarray
+    vol: np.ndarray
+    divv: np.ndarray
+    gas: Gas                # all cells, model order
+
+    @property
+    def groups(self) -> Groups:
+        return self.models[0].groups
+
+    @property
+    def lines(self) -> np.ndarray:
+        return self.models[0].lines
+
+
+def concat_gas(gases) -> Gas:
+    cat0 = lambda k: np.concatenate([getattr(g, k) for g in gases], axis=0)
+    cat2 = lambda k: np.concatenate([getattr(g, k) for g in gases], axis=2)
+    return Gas(cat0("temp"), cat0("mass"), cat0("rho"), cat0("natom"), cat0("nelec"), cat0("natomfr"),
+               cat0("massfr"), gases[0].ion_ni, cat2("oc"), cat2("ginv"))
+
+
+def model_batch(nmodel: int = 128, seed: int = 4, ng: int = 2000, nline: int = 500_000,
+                nx_range=(50, 400), npart_range=(1e5, 1e7), t_range_days=(1.0, 30.0),
+                nx=None, npart=None) -> ModelBatch:
+    """Batched workload: shells ~ U{nx_range}, particle budgets log-uniform in
+    npart_range, snapshot times log-uniform in t_range_days, and per model
+    seeded T (U(6000, 14000) K), broken-power-law rho (1 Msun) and
+    Dirichlet(1) composition as in opacity_case.  Groups, the line list and
+    the bf/ff tables are shared by every model."""
+    rng = np.random.default_rng(seed)
+    nxs = (rng.integers(nx_range[0], nx_range[1] + 1, nmodel) if nx is None
+           else np.asarray(nx)).astype(np.int32)
+    nps = (np.exp(rng.uniform(math.log(npart_range[0]), math.log(npart_range[1]), nmodel)).astype(np.int64)
+           if npart is None else np.asarray(npart, dtype=np.int64))
+    ts = np.exp(rng.uniform(math.log(t_range_days[0]), math.log(t_range_days[1]), nmodel))
+    groups = group_grid(ng)
+    lines = make_lines(nline, rng)
+    ph1, ph2 = synthetic_verner()
+    gff = synthetic_gaunt()
+    models = []
+    for m in range(nmodel):
+        mr = np.random.default_rng([seed, m])
+        grid = homologous_grid(int(nxs[m]), float(ts[m]) * PC_DAY)
+        models.append(OpacityCase(grid, groups, make_gas(grid, mr), lines, ph1, ph2, gff))
+    cat = lambda k: np.concatenate([getattr(c.grid, k) for c in models])
+    return ModelBatch(models, nxs, nps, ts, cat("xarr"), cat("vxarr"), cat("vol"), cat("divv"),
+                      concat_gas([c.gas for c in models]))
 
 
 def analytic_grey(grid: Grid, temp: np.ndarray, rho: np.ndarray, ng: int):
