@@ -347,6 +347,41 @@ int slg_particle_advance_static(const slg_grid_dev* grid, const slg_transport_in
                                 slg_packet* prt, int32_t* isvacant, int64_t npart,
                                 uint64_t seed, slg_transport_out* out, void* stream);
 
+/* ------------------------------------------------------------------ differentiable opacity */
+/* The opacity build as a differentiable function of shell temperature,
+ * density and mass fractions, with a hand-written reverse mode (no
+ * counterpart in the reference).  Needs groups, grid (one model), atomic data,
+ * ion data for the same nelem elements and their masses.  Device pointers. */
+
+/* Element masses [amu] of elements 1..nelem (elemdatamod elem_data%m). */
+int slg_set_element_masses(slg_ctx* ctx, int32_t nelem, const double* mass_amu);
+
+/* Forward: massfr2natomfr (GAS/gas_setup.f:101-160; massfr (nelem, ncell),
+ * renormalised per shell), the equation of state (slg_saha_eos at accuracy
+ * acc; nelec in/out), physical_opacity with ngs = 1 and the FP64 opacity
+ * returned in cap (ng, ncell) (gas_cap's layout before sngl), sig (ncell),
+ * opacity_planckmean / rossmean and leakage_opacity11 computed on that FP64
+ * opacity: capgrey, capross (ncell), opaclump (11, ncell). */
+int slg_dev_opacity_grad_forward(slg_ctx* ctx, const double* temp, const double* rho,
+                                 const double* massfr, double acc, double tauddmc,
+                                 double taulump, double* nelec, double* cap, double* sig,
+                                 double* capgrey, double* capross, double* opaclump);
+
+/* Reverse mode of slg_dev_opacity_grad_forward: given its inputs, its nelec
+ * and outputs, and dL/d(cap, sig, capgrey, capross, opaclump) (NULL = zero;
+ * opaclump rows 1, 2, 7, 8, 11 carry gradients), writes dL/dtemp, dL/drho
+ * (ncell) and dL/dmassfr (nelem, ncell).  The equation of state enters
+ * through its implicit derivative at the returned solution, so pass acc near
+ * machine precision (1e-14) when the gradient must match finite differences. */
+int slg_dev_opacity_grad_backward(slg_ctx* ctx, const double* temp, const double* rho,
+                                  const double* massfr, double acc, double tauddmc,
+                                  double taulump, const double* nelec, const double* cap,
+                                  const double* sig, const double* capgrey,
+                                  const double* capross, const double* opaclump,
+                                  const double* gcap, const double* gsig, const double* gcapgrey,
+                                  const double* gcapross, const double* gopaclump, double* gtemp,
+                                  double* grho, double* gmassfr);
+
 /* ------------------------------------------------------------------ CUDA graphs */
 /* Capture the work that slg_dev_* calls queue on the context's stream
  * between slg_graph_begin and slg_graph_end into one executable CUDA graph

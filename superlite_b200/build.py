@@ -19,7 +19,8 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT, "libslg.so")
 
-FP64_SOURCES = ["opacity.cu", "grid.cu", "transport.cu", "source.cu", "capi.cu", "noalloc.cu", "eos.cu"]
+FP64_SOURCES = ["opacity.cu", "grid.cu", "transport.cu", "source.cu", "capi.cu", "noalloc.cu", "eos.cu",
+                "adjoint.cu"]
 MIXED_SOURCES = ["transport_mixed.cu"]
 HEADERS = ["slg_device.cuh", "slg_internal.h", "transport_impl.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

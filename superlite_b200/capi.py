@@ -90,6 +90,9 @@ SIGNATURES = {
                                          vp, vp]),
     "slg_set_transport_variant": (C.c_int, [vp, C.c_int32]),
     "slg_sync": (C.c_int, [vp]),
+    "slg_set_element_masses": (C.c_int, [vp, C.c_int32, vp]),
+    "slg_dev_opacity_grad_forward": (C.c_int, [vp, vp, vp, vp, C.c_double, C.c_double, C.c_double] + [vp] * 6),
+    "slg_dev_opacity_grad_backward": (C.c_int, [vp, vp, vp, vp, C.c_double, C.c_double, C.c_double] + [vp] * 14),
     "slg_partition_functions": (None, [C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, C.c_double, vp]),
     "slg_set_ions": (C.c_int, [vp, C.c_int32, C.c_int32, vp, vp, vp, vp]),
     "slg_saha_eos": (C.c_int, [vp, vp, vp, vp, vp, C.c_double, vp, C.c_int32, vp, vp, vp]),

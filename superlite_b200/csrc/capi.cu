@@ -256,6 +256,7 @@ void slg_destroy(slg_ctx* ctx) {
   free_dev(ctx->d_gff); free_dev(ctx->d_acc);
   free_dev(ctx->d_totals); free_dev(ctx->d_epoch); free_dev(ctx->d_models); free_dev(ctx->d_cellmap);
   free_dev(ctx->d_eos_ni); free_dev(ctx->d_eos_e); free_dev(ctx->d_eos_q); free_dev(ctx->d_eos_g1);
+  free_dev(ctx->d_amass);
   if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
   if (ctx->h_acc) cudaFreeHost(ctx->h_acc);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);

@@ -132,6 +132,157 @@ __global__ void __launch_bounds__(EOS_BLOCK) saha_eos_kernel(const EosArgs A) {
   }
 }
 
+// Adjoint of the converged ionisation balance (no reference counterpart).
+// With s = 2 sahac(T) / (nelec ndens) and c_k = exp(-e_k/kT) q_(k+1)/q_k, the
+// stage fractions are f_k ~ s^(k-1) prod_(j<k) c_j (partition functions are
+// constants, as in the reference), and nelec solves nelec = sum_z fr_z ne_z.
+// Inputs: goc (ncell, noc, nelem) and gnelec (ncell) = dL/d(oc, nelec);
+// outputs (added to): gT, gnatom (through ndens = natom/vol and oc), gfr
+// (0:nelem, ncell).  One warp per cell, lane = element.
+__global__ void __launch_bounds__(EOS_BLOCK) saha_eos_bwd_kernel(const EosArgs A, const double* __restrict__ goc,
+                                                                const double* __restrict__ gnelec,
+                                                                double* __restrict__ gT,
+                                                                double* __restrict__ gnatom,
+                                                                double* __restrict__ gfr) {
+  const int lane = threadIdx.x & 31;
+  const int i = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (i >= A.nc) return;
+  const bool act = lane < A.nelem;
+  const int ns = A.nstage;
+  const int nion = act ? A.ni[lane] : 0;
+  const double* e = A.e + (size_t)lane * ns;
+  const double* q = A.q + (size_t)lane * ns;
+  const double* g1 = A.g1 + (size_t)lane * ns;
+  const double fr = act ? A.natomfr[(size_t)i * (A.nelem + 1) + lane + 1] : 0.0;
+  const double T = A.temp[i], vol = A.vol[i];
+  const double D = A.natom[i] / vol;
+  const double kt = pc_kb * T;
+  const double y = A.nelec[i];
+  const double sahac = pow(pc_pi2 * pc_me * pc_kb * T / (pc_h * pc_h), 1.5);
+  const double s = 2.0 / (y * D) * sahac;
+  // stage fractions at the converged nelec, from log-weights phi_k
+  double f[EOS_MAXST], E[EOS_MAXST];
+  double pmax = 0.0;
+  if (act) {
+    f[0] = 0.0;
+    E[0] = 0.0;
+    for (int k = 1; k < nion; ++k) {
+      f[k] = f[k - 1] + log(s) - e[k - 1] / kt + log(q[k]) - log(q[k - 1]);
+      E[k] = E[k - 1] + e[k - 1];
+      pmax = fmax(pmax, f[k]);
+    }
+  }
+  double zs = 0.0;
+  for (int k = 0; k < nion; ++k) zs += exp(f[k] - pmax);
+  double ne = 0.0, me = 0.0;  // <k>, <E_k> over the stages
+  for (int k = 0; k < nion; ++k) {
+    f[k] = exp(f[k] - pmax) / zs;
+    ne += (double)k * f[k];
+    me += E[k] * f[k];
+  }
+  double V = 0.0, Cv = 0.0;
+  for (int k = 0; k < nion; ++k) {
+    V += f[k] * sq((double)k - ne);
+    Cv += f[k] * ((double)k - ne) * (E[k] - me);
+  }
+  Cv = Cv / (kt * T);
+  // oc_k = D fr (g1/q)_k f_k
+  double gD = 0.0, gfr_l = 0.0, gbar = 0.0;
+  double gf[EOS_MAXST];
+  for (int k = 0; k < nion; ++k) {
+    gf[k] = 0.0;
+    if (k < A.noc) {
+      const double go = goc[(size_t)i + (size_t)A.nc * ((size_t)k + (size_t)A.noc * lane)];
+      const double w = g1[k] / q[k];
+      gD += go * fr * w * f[k];
+      gfr_l += go * D * w * f[k];
+      gf[k] = go * D * fr * w;
+    }
+    gbar += gf[k] * f[k];
+  }
+  // through the normalisation: dL/dphi_k = f_k (gf_k - gbar); phi_k = k ln s + E_k/kT + const
+  double glns = 0.0, gt = 0.0;
+  for (int k = 0; k < nion; ++k) {
+    const double gp = f[k] * (gf[k] - gbar);
+    glns += gp * (double)k;
+    gt += gp * E[k] / (kt * T);
+  }
+  // warp sums of the terms every element shares (nelec, T, D)
+  double Gy = fr * V, GT = fr * (V * 1.5 / T + Cv), GD = fr * V;
+  for (int o = 16; o > 0; o >>= 1) {
+    glns += __shfl_xor_sync(0xffffffffu, glns, o);
+    gt += __shfl_xor_sync(0xffffffffu, gt, o);
+    gD += __shfl_xor_sync(0xffffffffu, gD, o);
+    Gy += __shfl_xor_sync(0xffffffffu, Gy, o);
+    GT += __shfl_xor_sync(0xffffffffu, GT, o);
+    GD += __shfl_xor_sync(0xffffffffu, GD, o);
+  }
+  // ln s = ln(2 sahac(T)) - ln nelec - ln D
+  gt += glns * 1.5 / T;
+  const double gy = gnelec[i] - glns / y;
+  gD += -glns / D;
+  // nelec = G(nelec, T, D, fr) with dG/dnelec = -Gy/nelec, dG/dD = -GD/D
+  const double lam = gy / (1.0 + Gy / y);
+  gt += lam * GT;
+  gD += lam * (-GD / D);
+  if (act) gfr[(size_t)i * (A.nelem + 1) + lane + 1] += gfr_l + lam * ne;
+  if (lane == 0) {
+    gT[i] += gt;
+    gnatom[i] += gD / vol;
+  }
+}
+
+// massfr2natomfr (GAS/gas_setup.f:101-160) for differentiable inputs: mass
+// fractions X (nelem, ncell) renormalised to one, gas_mass = rho vol,
+// natomfr(z) ~ X_z/m_z normalised, gas_natom = mass sum(X/m) / amu.
+__global__ void composition_kernel(int nc, int nelem, const double* __restrict__ rho, const double* __restrict__ X,
+                                   const double* __restrict__ vol, const double* __restrict__ amass,
+                                   double* __restrict__ mass, double* __restrict__ natom,
+                                   double* __restrict__ natomfr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nc) return;
+  const double* x = X + (size_t)i * nelem;
+  double sx = 0.0;
+  for (int z = 0; z < nelem; ++z) sx += x[z];
+  double S = 0.0;
+  for (int z = 0; z < nelem; ++z) S += (x[z] / sx) / amass[z];
+  const double m = rho[i] * vol[i];
+  mass[i] = m;
+  natom[i] = m * S / pc_amu;
+  double* fr = natomfr + (size_t)i * (nelem + 1);
+  fr[0] = 0.0;
+  for (int z = 0; z < nelem; ++z) fr[z + 1] = ((x[z] / sx) / amass[z]) / S;
+}
+
+// Adjoint of composition_kernel: gnatom, gfr -> grho, gX.
+__global__ void composition_bwd_kernel(int nc, int nelem, const double* __restrict__ rho,
+                                       const double* __restrict__ X, const double* __restrict__ vol,
+                                       const double* __restrict__ amass, const double* __restrict__ gnatom,
+                                       const double* __restrict__ gfr, double* __restrict__ grho,
+                                       double* __restrict__ gX) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nc) return;
+  const double* x = X + (size_t)i * nelem;
+  const double* g = gfr + (size_t)i * (nelem + 1);
+  double sx = 0.0;
+  for (int z = 0; z < nelem; ++z) sx += x[z];
+  double S = 0.0, gy_fr = 0.0;
+  for (int z = 0; z < nelem; ++z) S += (x[z] / sx) / amass[z];
+  for (int z = 0; z < nelem; ++z) gy_fr += g[z + 1] * ((x[z] / sx) / amass[z]);
+  const double m = rho[i] * vol[i];
+  grho[i] = gnatom[i] * vol[i] * S / pc_amu;
+  // y_z = Xhat_z/m_z, S = sum y, natom = m S/amu, fr_z = y_z/S
+  const double gS = gnatom[i] * m / pc_amu - gy_fr / (S * S);
+  double dot = 0.0;
+  double* gx = gX + (size_t)i * nelem;
+  for (int z = 0; z < nelem; ++z) {
+    const double gxh = (g[z + 1] / S + gS) / amass[z];
+    gx[z] = gxh;
+    dot += gxh * (x[z] / sx);
+  }
+  for (int z = 0; z < nelem; ++z) gx[z] = (gx[z] - dot) / sx;  // Xhat = X / sum X
+}
+
 int launch_saha_eos(slg_ctx* ctx, const double* temp, const double* natom, const double* vol,
                     const double* natomfr, double acc, double* nelec, int noc, double* oc, double* ginv,
                     int32_t* iconv, int* d_flags) {
@@ -150,6 +301,42 @@ int check_eos(slg_ctx* ctx, int noc) {
 }
 
 }  // namespace
+
+// Launchers used by the differentiable opacity (adjoint.cu).
+int launch_composition(slg_ctx* ctx, const double* rho, const double* X, double* mass, double* natom,
+                       double* natomfr) {
+  const int nc = ctx->nx;
+  composition_kernel<<<(nc + 127) / 128, 128, 0, ctx->stream>>>(nc, ctx->eos_nelem, rho, X, ctx->d_vol,
+                                                                ctx->d_amass, mass, natom, natomfr);
+  return cuda_check(ctx, cudaGetLastError(), "composition launch");
+}
+
+int launch_composition_bwd(slg_ctx* ctx, const double* rho, const double* X, const double* gnatom,
+                           const double* gfr, double* grho, double* gX) {
+  const int nc = ctx->nx;
+  composition_bwd_kernel<<<(nc + 127) / 128, 128, 0, ctx->stream>>>(nc, ctx->eos_nelem, rho, X, ctx->d_vol,
+                                                                    ctx->d_amass, gnatom, gfr, grho, gX);
+  return cuda_check(ctx, cudaGetLastError(), "composition adjoint launch");
+}
+
+int launch_saha_eos_dev(slg_ctx* ctx, const double* temp, const double* natom, const double* vol,
+                        const double* natomfr, double acc, double* nelec, int noc, double* oc, double* ginv,
+                        int* d_flags) {
+  return launch_saha_eos(ctx, temp, natom, vol, natomfr, acc, nelec, noc, oc, ginv, nullptr, d_flags);
+}
+
+int launch_saha_eos_bwd(slg_ctx* ctx, const double* temp, const double* natom, const double* vol,
+                        const double* natomfr, const double* nelec, int noc, const double* goc,
+                        const double* gnelec, double* gT, double* gnatom, double* gfr) {
+  EosArgs A{ctx->nx, ctx->eos_nelem, ctx->eos_nstage, noc, ctx->d_eos_ni, ctx->d_eos_e, ctx->d_eos_q,
+            ctx->d_eos_g1, temp, natom, vol, natomfr, 0.0, const_cast<double*>(nelec), nullptr, nullptr,
+            nullptr, nullptr};
+  const long long nthr = (long long)ctx->nx * 32;
+  saha_eos_bwd_kernel<<<(unsigned)((nthr + EOS_BLOCK - 1) / EOS_BLOCK), EOS_BLOCK, 0, ctx->stream>>>(
+      A, goc, gnelec, gT, gnatom, gfr);
+  return cuda_check(ctx, cudaGetLastError(), "saha_eos adjoint launch");
+}
+
 }  // namespace slg
 
 using namespace slg;

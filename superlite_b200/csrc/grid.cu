@@ -34,18 +34,23 @@ __device__ inline double block_sum(double v, double* sh) {
   return r;
 }
 
-struct LeakArgs {
+// CT: opacity type, float (grd_cap) or double (the FP64 opacity of the
+// differentiable path).
+template <class CT>
+struct LeakArgsT {
   int nx, ng;
   const double *xarr, *vol, *divv, *tempinv, *sig, *wlinv;
-  const float *cap, *capemit;
+  const CT *cap, *capemit;
   double tauddmc, taulump;
   double* opaclump;
   const int4* cellmap;  // {shell, model shells, model first cell, model} per cell; null: one model
 };
+using LeakArgs = LeakArgsT<float>;
 
 // Arguments seen from cell c (0-based over all models): per-cell arrays start
 // at the cell's model, nx is the model's, *i the 1-based shell in the model.
-__device__ inline LeakArgs leak_view(LeakArgs A, int c, int* i) {
+template <class CT>
+__device__ inline LeakArgsT<CT> leak_view(LeakArgsT<CT> A, int c, int* i) {
   *i = c + 1;
   if (A.cellmap) {
     const int4 m = A.cellmap[c];
@@ -63,17 +68,18 @@ __device__ inline LeakArgs leak_view(LeakArgs A, int c, int* i) {
 
 // leakage_opacity11.f90:30-171, one block per cell.  Sums are fixed-shape
 // tree reductions (the reference sums sequentially).
-__global__ void __launch_bounds__(GB) leakage_kernel(const LeakArgs A0) {
+template <class CT>
+__global__ void __launch_bounds__(GB) leakage_kernel(const LeakArgsT<CT> A0) {
   __shared__ double sh[GB];
   __shared__ double shv[GB];
   __shared__ int shi[GB];
   int i0;
-  const LeakArgs A = leak_view(A0, blockIdx.x, &i0);
+  const LeakArgsT<CT> A = leak_view(A0, blockIdx.x, &i0);
   const int i = i0;  // 1-based cell
   const int l = i, ng = A.ng;
   const double* X = A.xarr - 1;  // 1-based view
   auto dx = [&](int k) { return A.xarr[k] - A.xarr[k - 1]; };
-  const float* capl = A.cap + (size_t)(l - 1) * ng;
+  const CT* capl = A.cap + (size_t)(l - 1) * ng;
   const double sigl = A.sig[l - 1];
   const double dist = dx(i);
   const double tinv = A.tempinv[l - 1];
@@ -218,6 +224,114 @@ __global__ void __launch_bounds__(GB) emitprob_kernel(int ng, int nep, int nepg,
       ep[iep - 1] = help;
     }
     ep[nep - 1] = capgrey[l];
+  }
+}
+
+// d/dT of specintv_elem and dopspeccalc (groupmod.f:123-143, :189-198) at
+// temperature T: x = hc/(lambda k T) scales as 1/T; zero where x is clamped.
+__device__ inline double dspec_dT(double hct, double T, const double* __restrict__ wlinv, int g0) {
+  const double x1 = hct * wlinv[g0], x2 = hct * wlinv[g0 + 1];
+  const double xm = 0.5 * (x2 + x1), ax = fabs(x2 - x1);
+  double dfp = 0.0;
+  if (xm < 300.0) {
+    const double ex = exp(xm), d = ex - 1.0;
+    dfp = 3.0 * sq(xm) / d - cube(xm) * ex / sq(d);
+  }
+  return -(ftpi4 * ax * (fplanck(xm) + xm * dfp)) / T;
+}
+__device__ inline double ddop_dT(double tinv, const double* __restrict__ wlinv, int ig) {
+  const double x = hck * tinv * wlinv[ig];
+  if (x >= 300.0) return 0.0;
+  const double ex = exp(x);
+  return -dopspeccalc(tinv, wlinv, ig) * tinv * (4.0 - x * ex / (ex - 1.0));
+}
+
+__global__ void __launch_bounds__(GB) leakage_bwd_kernel(const LeakArgsT<double> A0, const double* __restrict__ gol,
+                                                         double* __restrict__ gcap, double* __restrict__ gsig,
+                                                         double* __restrict__ gT) {
+  __shared__ double sh[GB];
+  const int c = blockIdx.x;  // cell over all models, 0-based
+  int i0;
+  const LeakArgsT<double> A = leak_view(A0, c, &i0);
+  const int i = i0, ng = A.ng;
+  const double* X = A.xarr - 1;
+  auto dx = [&](int k) { return A.xarr[k] - A.xarr[k - 1]; };
+  const double* capl = A.cap + (size_t)(i - 1) * ng;
+  const double sigl = A.sig[i - 1];
+  const double dist = dx(i);
+  const double tinv = A.tempinv[i - 1], T = 1.0 / tinv;
+  const double hct = hck * tinv;
+  const double divv = A.divv[i - 1];
+  const double* ol = A.opaclump + (size_t)11 * (i - 1);
+  const double* u = gol + (size_t)11 * c;
+  const double speclump = ol[6], ol1 = ol[0], ol2 = ol[1];
+  const double u1 = u[0], u2 = u[1], u7 = u[6], u8 = u[7], u11 = u[10];
+  const double vterm = 3.0 * A.vol[i - 1] / pc_pi4;
+  double gs = 0.0, gt = 0.0;
+  for (int ig = threadIdx.x + 1; ig <= ng; ig += GB) {
+    const double cg = capl[ig - 1];
+    if (!(cg * dist >= A.taulump && (sigl + cg) * dist >= A.tauddmc)) continue;
+    const double sv = specintv_elem(hct, A.wlinv, ig - 1);
+    // left leakage term a and d a / d(opacity sum) of this cell (da) and the left one (dal)
+    double a, da, dal = 0.0;
+    const bool lint = i != 1 && (A.cap[(size_t)(i - 2) * ng + ig - 1] + A.sig[i - 2]) * dx(i - 1) >= A.tauddmc;
+    if (!lint) {
+      const double q = 3.0 * ((cg + sigl) * dist) + 6.0 * pc_dext;
+      a = 1.5 * (4.0 / q) * sq(X[i]) / vterm;
+      da = -a * 3.0 / q * dist;
+    } else {
+      const double help = (sigl + cg) * dist + (A.sig[i - 2] + A.cap[(size_t)(i - 2) * ng + ig - 1]) * dx(i - 1);
+      a = 2.0 * sq(X[i]) / (help * vterm);
+      da = -a / help * dist;
+      dal = -a / help * dx(i - 1);
+    }
+    double b, db, dbr = 0.0;
+    const bool rint = i != A.nx && (A.cap[(size_t)i * ng + ig - 1] + A.sig[i]) * dx(i + 1) >= A.tauddmc;
+    if (!rint) {
+      const double q = 3.0 * ((cg + sigl) * dist) + 6.0 * pc_dext;
+      b = 1.5 * (4.0 / q) * sq(X[i + 1]) / vterm;
+      db = -b * 3.0 / q * dist;
+    } else {
+      const double help = (sigl + cg) * dist + (A.sig[i] + A.cap[(size_t)i * ng + ig - 1]) * dx(i + 1);
+      b = 2.0 * sq(X[i + 1]) / (help * vterm);
+      db = -b / help * dist;
+      dbr = -b / help * dx(i + 1);
+    }
+    // ol1 = sum w_g a_g with w_g = sv_g speclump and speclump = 1/sum sv: d ol1/d sv_g = speclump (a_g - ol1)
+    const double ua = u1 * sv * speclump, ub = u2 * sv * speclump;
+    const double us = u1 * speclump * (a - ol1) + u2 * speclump * (b - ol2) - u7 * speclump * speclump + u8 * cg;
+    gt += us * dspec_dT(hct, T, A.wlinv, ig - 1);
+    atomicAdd(&gcap[(size_t)c * ng + ig - 1], u8 * sv + ua * da + ub * db);
+    gs += ua * da + ub * db;
+    if (lint) {
+      atomicAdd(&gcap[(size_t)(c - 1) * ng + ig - 1], ua * dal);
+      atomicAdd(&gsig[c - 1], ua * dal);
+    }
+    if (rint) {
+      atomicAdd(&gcap[(size_t)(c + 1) * ng + ig - 1], ub * dbr);
+      atomicAdd(&gsig[c + 1], ub * dbr);
+    }
+  }
+  if (u11 != 0.0) {
+    if (divv >= 0.0) {
+      for (int ig = threadIdx.x + 1; ig <= ng - 1; ig += GB) {
+        if (capl[ig - 1] * dist < A.taulump || capl[ig] * dist >= A.taulump) continue;
+        if ((sigl + capl[ig - 1]) * dist < A.tauddmc) continue;
+        gt += u11 * ddop_dT(tinv, A.wlinv, ig) * divv / (3.0 * pc_c);
+      }
+    } else {
+      for (int ig = threadIdx.x + 2; ig <= ng; ig += GB) {
+        if (capl[ig - 1] * dist < A.taulump || capl[ig - 2] * dist >= A.taulump) continue;
+        if ((sigl + capl[ig - 1]) * dist < A.tauddmc) continue;
+        gt -= u11 * ddop_dT(tinv, A.wlinv, ig - 1) * divv / (3.0 * pc_c);
+      }
+    }
+  }
+  gs = block_sum(gs, sh);
+  gt = block_sum(gt, sh);
+  if (threadIdx.x == 0) {
+    atomicAdd(&gsig[c], gs);
+    gT[c] += gt;
   }
 }
 
@@ -449,8 +563,31 @@ int launch_leakage(slg_ctx* ctx, const double* tempinv, const double* sig, const
                    const float* capemit, double tauddmc, double taulump, double* opaclump) {
   LeakArgs A{ctx->nx, ctx->ng, ctx->d_xarr, ctx->d_vol, ctx->d_divv, tempinv, sig, ctx->d_wlinv,
              cap, capemit, tauddmc, taulump, opaclump, ctx->nmodel > 1 ? ctx->d_cellmap : nullptr};
-  leakage_kernel<<<ctx->nx, GB, 0, ctx->stream>>>(A);
+  leakage_kernel<float><<<ctx->nx, GB, 0, ctx->stream>>>(A);
   return cuda_check(ctx, cudaGetLastError(), "leakage launch");
+}
+
+// leakage_opacity11 on the FP64 opacity (ng, ncell) of the differentiable path.
+int launch_leakage64(slg_ctx* ctx, const double* tempinv, const double* sig, const double* cap, double tauddmc,
+                     double taulump, double* opaclump) {
+  LeakArgsT<double> A{ctx->nx, ctx->ng, ctx->d_xarr, ctx->d_vol, ctx->d_divv, tempinv, sig, ctx->d_wlinv,
+                      cap, nullptr, tauddmc, taulump, opaclump, ctx->nmodel > 1 ? ctx->d_cellmap : nullptr};
+  leakage_kernel<double><<<ctx->nx, GB, 0, ctx->stream>>>(A);
+  return cuda_check(ctx, cudaGetLastError(), "leakage64 launch");
+}
+
+// Adjoint of leakage_kernel<double> for opaclump rows 1, 2 (leakage), 7
+// (speclump), 8 (caplump) and 11 (doplump): gol (11, ncell) in; adds to gcap
+// (ng, ncell) of the cell and its neighbours, gsig and gT.  The lumping masks
+// are piecewise constant and contribute nothing.
+int launch_leakage64_bwd(slg_ctx* ctx, const double* tempinv, const double* sig, const double* cap,
+                         double tauddmc, double taulump, const double* opaclump, const double* gol, double* gcap,
+                         double* gsig, double* gT) {
+  LeakArgsT<double> A{ctx->nx, ctx->ng, ctx->d_xarr, ctx->d_vol, ctx->d_divv, tempinv, sig, ctx->d_wlinv,
+                      cap, nullptr, tauddmc, taulump, const_cast<double*>(opaclump),
+                      ctx->nmodel > 1 ? ctx->d_cellmap : nullptr};
+  leakage_bwd_kernel<<<ctx->nx, GB, 0, ctx->stream>>>(A, gol, gcap, gsig, gT);
+  return cuda_check(ctx, cudaGetLastError(), "leakage adjoint launch");
 }
 
 int launch_emitprob(slg_ctx* ctx, const double* tempinv, const float* cap, const double* capgrey,

@@ -318,6 +318,7 @@ struct OpacArgs {
   float* cap32;             // (ng, ncell)
   float* emiss32;
   double* cap64;            // (ncell, ng) optional
+  double* capg64 = nullptr; // (ng, ncell) optional: cap before sngl() in gas_cap's layout
   int* flags;
 };
 
@@ -388,6 +389,7 @@ __device__ inline double subgroup_opacity(const OpacArgs& A, int i, int igs, boo
 __global__ void __launch_bounds__(OPAC_GT * 32) opacity_fwd_kernel(const OpacArgs A) {
   __shared__ float tcap[OPAC_CT][OPAC_GT + 1];
   __shared__ float tem[OPAC_CT][OPAC_GT + 1];
+  __shared__ double tcapd[OPAC_CT][OPAC_GT + 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ig = blockIdx.y * OPAC_GT + warp + 1;  // 1-based group
   const int i = blockIdx.x * OPAC_CT + lane;       // 0-based shell
@@ -426,6 +428,7 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_fwd_kernel(const OpacArg
   if (valid && A.cap64) A.cap64[(size_t)(ig - 1) * A.nc + i] = cap;
   tcap[lane][warp] = c32;
   tem[lane][warp] = e32;
+  if (A.capg64) tcapd[lane][warp] = cap;
   __syncthreads();
   // write (ng, ncell): each shell's OPAC_GT consecutive groups together
   const int ci = threadIdx.x / OPAC_GT, gj = threadIdx.x % OPAC_GT;
@@ -433,6 +436,7 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_fwd_kernel(const OpacArg
   if (i2 < A.nc && g2 < A.ng) {
     A.cap32[(size_t)i2 * A.ng + g2] = tcap[ci][gj];
     A.emiss32[(size_t)i2 * A.ng + g2] = tem[ci][gj];
+    if (A.capg64) A.capg64[(size_t)i2 * A.ng + g2] = tcapd[ci][gj];
   }
 }
 
@@ -494,11 +498,282 @@ __global__ void __launch_bounds__(256) opacity_means_kernel(int nc, int ng, cons
   }
 }
 
+// ------------------------------------------------------------ adjoint (no reference counterpart)
+// Derivatives of the Planck-weight integrands of groupmod.f with respect to
+// x = hc/(lambda k T); both weights are constant where the reference clamps x
+// at 300, and spectintv's NaN guard (groupmod.f:390-392) gives zero.
+__device__ inline double dfplanck(double x) {
+  if (x >= 300.0) return 0.0;
+  const double ex = exp(x), d = ex - 1.0;
+  return 3.0 * sq(x) / d - cube(x) * ex / sq(d);
+}
+__device__ inline double dfross(double x) {
+  if (x >= 300.0) return 0.0;
+  const double ex = exp(x);
+  const double r = (pow4(x) * ex) / sq(ex - 1.0);
+  const double v = r * (4.0 / x + 1.0 - 2.0 * ex / (ex - 1.0));
+  return v != v ? 0.0 : v;
+}
+// d/dT of specintv_elem / spectintv_elem at temperature T (hct = hck/T).
+__device__ inline double dspecintv_dT(double hct, double T, const double* __restrict__ wlinv, int g0) {
+  const double x1 = hct * wlinv[g0], x2 = hct * wlinv[g0 + 1];
+  const double xm = 0.5 * (x2 + x1), ax = fabs(x2 - x1);
+  return -(ftpi4 * ax * (fplanck(xm) + xm * dfplanck(xm))) / T;
+}
+__device__ inline double dspectintv_dT(double hct, double T, const double* __restrict__ wlinv, int g0) {
+  const double x1 = hct * wlinv[g0], x2 = hct * wlinv[g0 + 1];
+  const double xm = 0.5 * (x2 + x1), ax = fabs(x2 - x1);
+  const double f = fross(xm);
+  if (ftpi4r * ax * f != ftpi4r * ax * f) return 0.0;
+  return -(ftpi4r * ax * (f + xm * dfross(xm))) / T;
+}
+
+// opacity_planckmean / opacity_rossmean on the FP64 opacity in (ng, ncell) layout.
+__global__ void __launch_bounds__(256) opacity_means64_kernel(int nc, int ng, const double* __restrict__ wlinv,
+                                                              const double* __restrict__ temp,
+                                                              const double* __restrict__ sig,
+                                                              const double* __restrict__ cap,
+                                                              double* __restrict__ capgrey,
+                                                              double* __restrict__ capross) {
+  __shared__ double sp[256], sr[256];
+  const int i = blockIdx.x;
+  const double hct = hck * (1.0 / temp[i]);
+  const double s = sig ? sig[i] : 0.0;
+  double ap = 0.0, ar = 0.0;
+  for (int g = threadIdx.x; g < ng; g += blockDim.x) {
+    const double c = cap[(size_t)i * ng + g];
+    ap = ap + c * specintv_elem(hct, wlinv, g);
+    ar = ar + (1.0 / (s + c)) * spectintv_elem(hct, wlinv, g);
+  }
+  sp[threadIdx.x] = ap;
+  sr[threadIdx.x] = ar;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      sp[threadIdx.x] = sp[threadIdx.x] + sp[threadIdx.x + w];
+      sr[threadIdx.x] = sr[threadIdx.x] + sr[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    capgrey[i] = sp[0];
+    capross[i] = 1.0 / sr[0];
+  }
+}
+
+// Adjoint of opacity_means64_kernel: adds to gcap (ng, ncell), gsig and gT.
+__global__ void __launch_bounds__(256) means_bwd_kernel(int nc, int ng, const double* __restrict__ wlinv,
+                                                        const double* __restrict__ temp,
+                                                        const double* __restrict__ sig,
+                                                        const double* __restrict__ cap,
+                                                        const double* __restrict__ capross,
+                                                        const double* __restrict__ ggrey,
+                                                        const double* __restrict__ gross, double* __restrict__ gcap,
+                                                        double* __restrict__ gsig, double* __restrict__ gT) {
+  __shared__ double s1[256], s2[256];
+  const int i = blockIdx.x;
+  const double T = temp[i], hct = hck * (1.0 / T);
+  const double s = sig[i];
+  const double ug = ggrey ? ggrey[i] : 0.0;
+  const double cr = capross[i];
+  const double ur = gross ? gross[i] * cr * cr : 0.0;  // capross = 1/R: d capross = -capross^2 dR
+  double asig = 0.0, at = 0.0;
+  for (int g = threadIdx.x; g < ng; g += blockDim.x) {
+    const double c = cap[(size_t)i * ng + g];
+    const double w = specintv_elem(hct, wlinv, g);
+    const double wr = spectintv_elem(hct, wlinv, g);
+    const double inv = 1.0 / (s + c);
+    const double dr = wr * inv * inv;  // -dR/dc
+    gcap[(size_t)i * ng + g] += ug * w + ur * dr;
+    asig = asig + ur * dr;
+    at = at + ug * c * dspecintv_dT(hct, T, wlinv, g) - ur * inv * dspectintv_dT(hct, T, wlinv, g);
+  }
+  s1[threadIdx.x] = asig;
+  s2[threadIdx.x] = at;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      s1[threadIdx.x] += s1[threadIdx.x + w];
+      s2[threadIdx.x] += s2[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    gsig[i] += s1[0];
+    gT[i] += s2[0];
+  }
+}
+
+struct OpacBwd {
+  const double* gcap;  // (ng, ncell)
+  double* gT;          // (ncell), added to
+  double* ggrnd;       // [slot][cell], added to (d cap / d grndlev)
+  double* goc;         // [slot][cell], added to (bound-free)
+  double* ghlp;        // (ncell), added to (d cap / d hlparr)
+  double* gfr;         // (0:nelem, ncell), added to
+};
+
+// Adjoint of subgroup_opacity (ngs = 1): bb, bf and ff in one pass over the
+// lines of each group, with per-(ion, shell) sums gathered in shared memory.
+__global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArgs A, const OpacBwd B) {
+  extern __shared__ double sm[];
+  const int nslot = A.nelem * A.nst;
+  double* s_grnd = sm;                               // [slot][32]
+  double* s_oc = sm + (size_t)nslot * 32;            // [slot][32]
+  double* s_fr = s_oc + (size_t)nslot * 32;          // [nelem+1][32]
+  double* s_t = s_fr + (size_t)(A.nelem + 1) * 32;   // [warp][32]
+  double* s_h = s_t + OPAC_GT * 32;
+  const int ntot = (2 * nslot + A.nelem + 1) * 32;
+  for (int k = threadIdx.x; k < ntot; k += blockDim.x) sm[k] = 0.0;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ig = blockIdx.y * OPAC_GT + warp + 1;
+  const int i = blockIdx.x * OPAC_CT + lane;
+  const bool live = ig <= A.ng && i < A.nc && A.mass[i] > 0.0;
+  double gt = 0.0, gh = 0.0;
+  const double u = live ? B.gcap[(size_t)i * A.ng + (ig - 1)] : 0.0;
+  if (u != 0.0) {
+    const double h = A.hckt[i], T = A.temp[i];
+    if (!A.nobb) {
+      const int l0 = A.lstart[ig], l1 = A.lstart[ig + 1];
+      if (l1 > l0) {
+        const double wa = A.wlsub[ig - 1], wb = A.wlsub[ig];
+        const double wl = 0.5 * (wa + wb);
+        const double wlinv = 1.0 / wl;
+        const double eh = exp(-(h * wlinv));
+        const double expfac = 1.0 - eh;
+        const double phi = wl * wl / ((wb - wa) * pc_c);
+        double capbb = 0.0, schi = 0.0;
+        for (int l = l0; l < l1; ++l) {
+          const float4 rec = __ldg(reinterpret_cast<const float4*>(A.bb) + l);
+          const uint32_t izii = __float_as_uint(rec.w);
+          const int iz = (int)(int16_t)(izii & 0xffffu), ii = (int)(int16_t)(izii >> 16);
+          const int slot = (iz - 1) * A.nst + (ii - 1);
+          const double base = phi * (double)rec.y * exp(-((double)rec.z * h)) * expfac;  // d cap / d grndlev
+          atomicAdd(&s_grnd[slot * 32 + lane], u * base);
+          const double ocg = A.grndlev[(size_t)slot * A.nc + i];
+          if (ocg > 0.0) {
+            const double c = base * ocg;
+            capbb = capbb + c;
+            schi = schi + c * (double)rec.z;
+          }
+        }
+        // h = hc/kT: d exp(-chi h)/dT = chi h/T exp(..), d expfac/dT = -(h/T) wlinv eh
+        gt = gt + u * ((h / T) * schi - capbb * (h / T) * wlinv * eh / expfac);
+      }
+    }
+    if (!A.nobf) {
+      const double* xs = A.xstab + (size_t)(ig - 1) * A.maxact;
+      const int nact = *A.pnact;
+      for (int a = 0; a < nact; ++a) {
+        const double x = xs[a];
+        if (x != 0.0) atomicAdd(&s_oc[A.act_slot[a] * 32 + lane], u * x * pc_mbarn);
+      }
+    }
+    if (!A.noff) {
+      const double wl = A.wlsub[ig - 1];
+      const double wlinv = 1.0 / wl;
+      const double uu = h * wlinv;
+      const double ru = 10.0 * (log10(uu) + 4.0) + 1.0;
+      const int iu = ru < 1.0 ? 1 : (ru >= (double)(FF_NU - 1) ? FF_NU - 1 : (int)floor(ru));
+      const double du = ru - iu;
+      const double eu = exp(-uu);
+      const double hn = A.ffc1 * sqrt(h) * (1.0 - eu) * cube(wl);
+      const double help = hn * A.hlparr[i];
+      const double dlnhelp = -0.5 / T - eu * uu / (T * (1.0 - eu));
+      const double ln10 = 2.302585092994045684;
+      const double dru = -10.0 / (ln10 * T), drgg = -5.0 / (ln10 * T);  // table coordinates vs T
+      const double* nfr = A.natomfr + (size_t)(A.nelem + 1) * i;
+      double S = 0.0, dS = 0.0;
+      for (int iz = 1; iz <= A.nelem; ++iz) {
+        const double fr = nfr[iz];
+        int igg = A.ffigg[(size_t)(iz - 1) * A.nc + i];
+        const bool clamp1 = igg < 0;
+        igg = clamp1 ? -igg : igg;
+        const double dgg = A.ffdgg[(size_t)(iz - 1) * A.nc + i];
+        const double* G = A.gff;
+        const double g00 = G[(iu - 1) + FF_NU * (igg - 1)], g10 = G[iu + FF_NU * (igg - 1)];
+        const double g01 = G[(iu - 1) + FF_NU * igg], g11 = G[iu + FF_NU * igg];
+        const double graw = (1.0 - du) * (1.0 - dgg) * g00 + du * (1.0 - dgg) * g10 + (1.0 - du) * dgg * g01 +
+                            du * dgg * g11;
+        const bool flat = clamp1 && graw < 1.0;
+        const double g = flat ? 1.0 : graw;
+        const double dg = flat ? 0.0
+                               : ((1.0 - dgg) * (g10 - g00) + dgg * (g11 - g01)) * dru +
+                                     ((1.0 - du) * (g01 - g00) + du * (g11 - g10)) * drgg;
+        const double w = (double)(iz * iz);
+        atomicAdd(&s_fr[iz * 32 + lane], u * help * g * w);
+        if (fr == 0.0) continue;
+        S = S + g * w * fr;
+        dS = dS + dg * w * fr;
+      }
+      gh = gh + u * hn * S;
+      gt = gt + u * (help * S * dlnhelp + help * dS);
+    }
+  }
+  s_t[warp * 32 + lane] = gt;
+  s_h[warp * 32 + lane] = gh;
+  __syncthreads();
+  if (warp == 0 && i < A.nc) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < OPAC_GT; ++w) {
+      a += s_t[w * 32 + lane];
+      b += s_h[w * 32 + lane];
+    }
+    if (a != 0.0) atomicAdd(&B.gT[i], a);
+    if (b != 0.0) atomicAdd(&B.ghlp[i], b);
+  }
+  for (int k = threadIdx.x; k < ntot; k += blockDim.x) {
+    const double v = sm[k];
+    const int row = k >> 5, c = blockIdx.x * OPAC_CT + (k & 31);
+    if (v == 0.0 || c >= A.nc) continue;
+    if (row < nslot) atomicAdd(&B.ggrnd[(size_t)row * A.nc + c], v);
+    else if (row < 2 * nslot) atomicAdd(&B.goc[(size_t)(row - nslot) * A.nc + c], v);
+    else atomicAdd(&B.gfr[(size_t)c * (A.nelem + 1) + (row - 2 * nslot)], v);
+  }
+}
+
+// Adjoint of opac_cell_prep_kernel: grndlev = oc ginv, hlparr = (natom/vol)^2
+// nelec, gas_sig = cthomson nelec natom / vol.
+__global__ void opac_cell_bwd_kernel(int nc, int nelem, int nst, const int32_t* __restrict__ ion_ni,
+                                     const double* __restrict__ natom, const double* __restrict__ nelec,
+                                     const double* __restrict__ vol, const double* __restrict__ mass,
+                                     const double* __restrict__ ginv, int nothmson,
+                                     const double* __restrict__ ggrnd, const double* __restrict__ ghlp,
+                                     const double* __restrict__ gsig, double* __restrict__ goc,
+                                     double* __restrict__ gnelec, double* __restrict__ gnatom) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nc) return;
+  if (!(mass[i] > 0.0)) {
+    gnelec[i] = 0.0;
+    gnatom[i] = 0.0;
+    return;
+  }
+  for (int iz = 1; iz <= nelem; ++iz) {
+    const int lim = min(iz, ion_ni[iz - 1] - 1);
+    for (int ii = 1; ii <= lim && ii <= nst; ++ii) {
+      const size_t k = ((size_t)(iz - 1) * nst + (ii - 1)) * nc + i;
+      goc[k] += ggrnd[k] * ginv[k];
+    }
+  }
+  const double nd = natom[i] / vol[i];
+  double gne = ghlp[i] * nd * nd;
+  double gna = ghlp[i] * 2.0 * nd * nelec[i] / vol[i];
+  if (!nothmson) {
+    gne += gsig[i] * cthomson * natom[i] / vol[i];
+    gna += gsig[i] * cthomson * nelec[i] / vol[i];
+  }
+  gnelec[i] = gne;
+  gnatom[i] = gna;
+}
+
 }  // namespace
 
 // ============================================================ launchers
-int launch_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_flags* flags,
-                            double* gas_sig, float* gas_cap, float* gas_emiss, double* cap64) {
+// Everything the opacity kernels read, queued on the stream: sub-group edges,
+// the line binning, per-cell terms (and gas_sig) and the bound-free table.
+static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_flags* flags, double* gas_sig,
+                           OpacArgs& A) {
   const int nc = ctx->nx, ng = ctx->ng;
   const int ngs = flags->ngs < 1 ? 1 : flags->ngs;
   const int ngsub = ng * ngs;
@@ -557,7 +832,6 @@ int launch_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_
     bf_table_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(ngsub, nslot, d_nact, d_act, nst, d_wlsub,
                                                                   ctx->d_ph1, ctx->d_ph2, d_xs);
   }
-  OpacArgs A;
   A.nc = nc; A.ng = ng; A.ngs = ngs; A.ngsub = ngsub; A.nelem = nelem; A.nst = nst; A.maxact = nslot;
   A.pnact = d_nact;
   A.nobb = !do_bb; A.nobf = !do_bf; A.noff = flags->noff;
@@ -567,11 +841,80 @@ int launch_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_
   A.hckt = d_hckt; A.hlparr = d_hlp; A.mass = gas->mass; A.natomfr = gas->natomfr; A.temp = gas->temp;
   A.ffigg = d_ffigg; A.ffdgg = d_ffdgg; A.gff = ctx->d_gff;
   A.ffc1 = ff_c1a * sqrt(ff_c1b);
-  A.cap32 = gas_cap; A.emiss32 = gas_emiss; A.cap64 = cap64; A.flags = d_flags;
+  A.cap32 = nullptr; A.emiss32 = nullptr; A.cap64 = nullptr; A.capg64 = nullptr; A.flags = d_flags;
   if (!ctx->d_gff && !A.noff) return set_error(ctx, SLG_ERR_STATE, "free-free table not set");
-  dim3 grid((nc + OPAC_CT - 1) / OPAC_CT, (ng + OPAC_GT - 1) / OPAC_GT);
-  opacity_fwd_kernel<<<grid, OPAC_GT * 32, 0, st>>>(A);
+  return SLG_OK;
+}
+
+int launch_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_flags* flags,
+                            double* gas_sig, float* gas_cap, float* gas_emiss, double* cap64) {
+  OpacArgs A;
+  const int rc = opacity_prepare(ctx, gas, flags, gas_sig, A);
+  if (rc) return rc;
+  A.cap32 = gas_cap; A.emiss32 = gas_emiss; A.cap64 = cap64;
+  dim3 grid((A.nc + OPAC_CT - 1) / OPAC_CT, (A.ng + OPAC_GT - 1) / OPAC_GT);
+  opacity_fwd_kernel<<<grid, OPAC_GT * 32, 0, ctx->stream>>>(A);
   return cuda_check(ctx, cudaGetLastError(), "opacity_fwd launch");
+}
+
+// Physical opacity (ngs = 1) with the FP64 result in gas_cap's (ng, ncell)
+// layout; gas_cap/gas_emiss (float) are written as well.
+int launch_physical_opacity64(slg_ctx* ctx, const slg_gas* gas, double* gas_sig, double* capg64, float* gas_cap,
+                              float* gas_emiss) {
+  slg_opacity_flags fl{0, 0, 0, 0, 1, 0.0};
+  OpacArgs A;
+  const int rc = opacity_prepare(ctx, gas, &fl, gas_sig, A);
+  if (rc) return rc;
+  A.cap32 = gas_cap; A.emiss32 = gas_emiss; A.capg64 = capg64;
+  dim3 grid((A.nc + OPAC_CT - 1) / OPAC_CT, (A.ng + OPAC_GT - 1) / OPAC_GT);
+  opacity_fwd_kernel<<<grid, OPAC_GT * 32, 0, ctx->stream>>>(A);
+  return cuda_check(ctx, cudaGetLastError(), "opacity_fwd launch");
+}
+
+int launch_opacity_means64(slg_ctx* ctx, const double* temp, const double* sig, const double* cap,
+                           double* capgrey, double* capross) {
+  opacity_means64_kernel<<<ctx->nx, 256, 0, ctx->stream>>>(ctx->nx, ctx->ng, ctx->d_wlinv, temp, sig, cap,
+                                                          capgrey, capross);
+  return cuda_check(ctx, cudaGetLastError(), "opacity_means64 launch");
+}
+
+int launch_means_bwd(slg_ctx* ctx, const double* temp, const double* sig, const double* cap, const double* capross,
+                     const double* ggrey, const double* gross, double* gcap, double* gsig, double* gT) {
+  means_bwd_kernel<<<ctx->nx, 256, 0, ctx->stream>>>(ctx->nx, ctx->ng, ctx->d_wlinv, temp, sig, cap, capross, ggrey,
+                                                    gross, gcap, gsig, gT);
+  return cuda_check(ctx, cudaGetLastError(), "means adjoint launch");
+}
+
+// Adjoint of launch_physical_opacity64 for gcap (ng, ncell) and gsig: adds
+// dL/dT to gT and writes dL/d(oc, nelec, natom, natomfr) (goc [slot][cell],
+// gnelec, gnatom, gfr (0:nelem, ncell)).  work: nslot*ncell + ncell doubles.
+int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, const double* gsig, double* gT,
+                       double* goc, double* gnelec, double* gnatom, double* gfr, double* sig_work, double* work) {
+  slg_opacity_flags fl{0, 0, 0, 0, 1, 0.0};
+  OpacArgs A;
+  int rc = opacity_prepare(ctx, gas, &fl, sig_work, A);
+  if (rc) return rc;
+  const int nc = ctx->nx, nslot = A.nelem * A.nst;
+  double* ggrnd = work;
+  double* ghlp = work + (size_t)nslot * nc;
+  cudaStream_t st = ctx->stream;
+  cudaMemsetAsync(ggrnd, 0, sizeof(double) * ((size_t)nslot * nc + nc), st);
+  cudaMemsetAsync(goc, 0, sizeof(double) * (size_t)nslot * nc, st);
+  cudaMemsetAsync(gfr, 0, sizeof(double) * (size_t)nc * (A.nelem + 1), st);
+  OpacBwd B{gcap, gT, ggrnd, goc, ghlp, gfr};
+  const size_t shm = sizeof(double) * ((size_t)(2 * nslot + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
+  if (shm > 200 * 1024) return set_error(ctx, SLG_ERR_ARG, "opacity adjoint: too many ion slots (%d)", nslot);
+  static size_t shm_set = 0;  // raised only when needed
+  if (shm > 48 * 1024 && shm > shm_set) {
+    cudaFuncSetAttribute(opacity_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    shm_set = 200 * 1024;
+  }
+  dim3 grid((nc + OPAC_CT - 1) / OPAC_CT, (A.ng + OPAC_GT - 1) / OPAC_GT);
+  opacity_bwd_kernel<<<grid, OPAC_GT * 32, shm, st>>>(A, B);
+  opac_cell_bwd_kernel<<<(nc + 127) / 128, 128, 0, st>>>(nc, A.nelem, A.nst, ctx->d_ion_ni, gas->natom, gas->nelec,
+                                                         gas->vol, gas->mass, gas->ginv, 0, ggrnd, ghlp, gsig, goc,
+                                                         gnelec, gnatom);
+  return cuda_check(ctx, cudaGetLastError(), "opacity adjoint launch");
 }
 
 // Sanity bitmask of physical_opacity.f:282-291 (word 0) and line-binning

@@ -24,6 +24,7 @@ constexpr double pc_dext = 0.7104;
 constexpr double pc_ev = 1.60217653e-12;
 constexpr double pc_ang = 1e-8;
 constexpr double pc_mbarn = 1e-18;
+constexpr double pc_amu = 1.66053886e-24;
 
 constexpr double cinv = 1.0 / pc_c;
 constexpr double pi_4th = (pc_pi * pc_pi) * (pc_pi * pc_pi);

@@ -89,8 +89,10 @@ struct slg_ctx {
   double* d_eos_e = nullptr;
   double* d_eos_q = nullptr;
   double* d_eos_g1 = nullptr;
+  double* d_amass = nullptr;  // element masses [amu] of the differentiable opacity
+  int amass_n = 0;
   // derived per-call scratch
-  slg::DevBuf scratch[64];
+  slg::DevBuf scratch[96];
   slg::CellTables tables;
   slg::TransportAcc* d_acc = nullptr;
   slg::TransportAcc* h_acc = nullptr;  // pinned

@@ -340,6 +340,10 @@ int launch_transport_variant(int v, bool trace, int num_sms, long long npart, cu
   }
 }
 
+// Grids up to this many cells keep grd_tally in shared memory in the
+// mixed-precision kernel (32 KiB per block).
+constexpr int kSmemTallyCells = 4096;
+
 // Kernel arguments of one particle_advance over the context's grid and models.
 TrnArgs transport_args(slg_ctx* ctx, const slg_transport_in* in, slg_packet* prt, int32_t* isvacant,
                        long long npart, uint64_t seed, double* tally, double* jrad, double* eamp,
@@ -357,6 +361,7 @@ TrnArgs transport_args(slg_ctx* ctx, const slg_transport_in* in, slg_packet* prt
   A.epoch = ctx->capturing ? ctx->d_epoch : nullptr;
   A.nmodel = ctx->nmodel > 1 ? ctx->nmodel : 1;
   A.models = ctx->nmodel > 1 ? ctx->d_models : nullptr;
+  A.smem_cells = ctx->nx <= kSmemTallyCells ? ctx->nx : 0;
   return A;
 }
 

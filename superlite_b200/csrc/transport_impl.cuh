@@ -32,6 +32,7 @@ struct TrnArgs {
   int32_t* trace_nstep;
   const unsigned long long* epoch = nullptr;  // replay counter of a captured graph
   int nmodel = 1;                             // models (read by the mixed-precision kernel)
+  int smem_cells = 0;                         // tally cells kept in shared memory (mixed kernel; 0: global)
   const ModelDesc* models = nullptr;
 };
 

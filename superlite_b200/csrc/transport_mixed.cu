@@ -455,9 +455,16 @@ template <int MINB>
 __global__ void __launch_bounds__(MIX_BLOCK, MINB) particle_advance_mixed_kernel(const TrnArgs A) {
   __shared__ unsigned long long s_cnt[20];
   __shared__ double s_sum[3];
+  // grd_tally of the whole grid in shared memory when it fits (A.smem_cells
+  // cells): a DDMC walk changes shell on almost every event, and flushing
+  // each visit to the few hundred global tally words made the warps wait on
+  // contended L2 atomics
+  extern __shared__ double s_tally[];
   if (threadIdx.x < 20) s_cnt[threadIdx.x] = 0ull;
   if (threadIdx.x < 3) s_sum[threadIdx.x] = 0.0;
+  for (int k = threadIdx.x; k < A.smem_cells; k += blockDim.x) s_tally[k] = 0.0;
   __syncthreads();
+  double* const tally = A.smem_cells ? s_tally : A.tally;
   const int lane = threadIdx.x & 31;
   double evelo = 0.0, eout = 0.0, sflux = 0.0;
   unsigned long long nimc = 0, nddmc = 0, nswap = 0, npckt = 0, nflux = 0, nwarn = 0, nmax = 0;
@@ -560,7 +567,7 @@ __global__ void __launch_bounds__(MIX_BLOCK, MINB) particle_advance_mixed_kernel
     }
     atomicAdd(&s_cnt[9 + (p.idist > -3 ? p.idist : -3) + 3], 1ull);
     if (icold != t_ic) {
-      if (t_ic > 0) atomicAdd(&A.tally[t_ic - 1], t_acc - t_c);
+      if (t_ic > 0) atomicAdd(&tally[t_ic - 1], t_acc - t_c);
       t_ic = icold;
       t_acc = 0.0;
       t_c = 0.0;
@@ -602,7 +609,7 @@ __global__ void __launch_bounds__(MIX_BLOCK, MINB) particle_advance_mixed_kernel
       have = false;
     }
   }
-  if (t_ic > 0) atomicAdd(&A.tally[t_ic - 1], t_acc - t_c);
+  if (t_ic > 0) atomicAdd(&tally[t_ic - 1], t_acc - t_c);
   if (j_ic > 0) atomicAdd(&A.jrad[(size_t)(j_ic - 1) * A.ng + (j_ig - 1)], pc_c * (j_acc - j_c));
   atomicAdd(&s_sum[0], evelo);
   atomicAdd(&s_sum[1], eout);
@@ -628,16 +635,24 @@ __global__ void __launch_bounds__(MIX_BLOCK, MINB) particle_advance_mixed_kernel
     atomicAdd(&A.acc->nwarn, s_cnt[6]);
   }
   if (threadIdx.x < 11 && s_cnt[9 + threadIdx.x]) atomicAdd(&A.acc->ndist[threadIdx.x], s_cnt[9 + threadIdx.x]);
+  for (int k = threadIdx.x; k < A.smem_cells; k += blockDim.x)
+    if (s_tally[k] != 0.0) atomicAdd(&A.tally[k], s_tally[k]);
 }
 
 template <int MINB>
 int launch_mixed_one(int num_sms, long long npart, cudaStream_t st, const TrnArgs& A) {
-  static int occ = -1;  // resident blocks per SM, queried once (not during a capture)
-  if (occ < 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_mixed_kernel<MINB>, MIX_BLOCK, 0);
-  long long nblk = (long long)num_sms * (occ > 0 ? occ : MINB);
+  // resident blocks per SM, queried again only when the shared tally size changes
+  static int occ = -1;
+  static size_t occ_shm = 0;
+  const size_t shm = sizeof(double) * (size_t)A.smem_cells;
+  if (occ < 0 || shm != occ_shm) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_mixed_kernel<MINB>, MIX_BLOCK, shm);
+    occ_shm = shm;
+  }
+  long long nblk = (long long)num_sms * (occ > 0 ? occ : 1);
   const long long need = (npart + MIX_BLOCK - 1) / MIX_BLOCK;
   if (need < nblk) nblk = need > 0 ? need : 1;
-  particle_advance_mixed_kernel<MINB><<<(unsigned)nblk, MIX_BLOCK, 0, st>>>(A);
+  particle_advance_mixed_kernel<MINB><<<(unsigned)nblk, MIX_BLOCK, shm, st>>>(A);
   return cudaPeekAtLastError() == cudaSuccess ? SLG_OK : SLG_ERR_CUDA;
 }
 

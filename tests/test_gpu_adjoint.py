@@ -1,0 +1,102 @@
+"""Hand-written adjoint of the opacity build (slg_dev_opacity_grad_backward)
+against central finite differences of its own forward.
+
+L = sum of randomly weighted outputs (group opacities, Thomson opacity,
+Planck / Rosseland means, leakage opacities).  For random directions v in
+temperature, density and mass fractions, the directional derivative from the
+adjoint, grad(L) . v, must match (L(x + h v) - L(x - h v)) / 2h within 1e-6
+relative.  Mass-fraction directions keep absent elements at zero (the
+reference stops on negative fractions).
+"""
+import numpy as np
+import pytest
+import torch
+
+from superlite_b200 import HotPath
+from superlite_b200 import workloads as W
+from superlite_b200.differentiable import DifferentiableOpacity
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-6
+
+
+def _setup(nc=24, ng=120, nline=20000, seed=3, t_days=8.0):
+    case = W.opacity_case(ncell=nc, ng=ng, nline=nline, seed=seed, t_days=t_days)
+    hot = HotPath(0)
+    hot.set_groups(case.groups.wl)
+    hot.set_grid(case.grid.xarr, case.grid.vxarr, case.grid.vol, case.grid.divv)
+    g = case.gas
+    hot.set_atomic_data(g.ion_ni, g.oc.shape[1], case.lines, case.bf_ph1, case.bf_ph2, case.ff_gff)
+    amass = [W.ELEM_MASS.get(z, 2.0 * z) for z in range(1, W.NELEM + 1)]
+    D = DifferentiableOpacity(hot, W.ion_table(), q_temp=float(g.temp[0]), elem_mass=amass)
+    dev = D.device
+    T = torch.tensor(g.temp, dtype=torch.float64, device=dev)
+    R = torch.tensor(g.rho, dtype=torch.float64, device=dev)
+    X = torch.tensor(g.massfr, dtype=torch.float64, device=dev)
+    return hot, D, case, T, R, X
+
+
+def _loss_weights(outs, seed):
+    gen = torch.Generator(device=outs[0].device).manual_seed(seed)
+    ws = []
+    for o in outs:
+        w = torch.randn(o.shape, generator=gen, device=o.device, dtype=torch.float64)
+        if o.dim() == 2 and o.shape[1] == 11:  # opaclump: scale each row by its own size
+            w = w / (o.abs().mean(dim=0, keepdim=True) + 1e-300)
+        else:
+            w = w / (o.abs().mean() + 1e-300)
+        ws.append(w / o.numel())
+    ws[4][:, [2, 3, 4, 5, 8, 9]] = 0.0  # rows without a gradient (zero or integer)
+    return ws
+
+
+def _L(D, ws, T, R, X):
+    outs = D.opacity(T, R, X)
+    return sum((w * o).sum() for w, o in zip(ws, outs))
+
+
+@pytest.mark.parametrize("which", ["temp", "rho", "massfr"])
+def test_adjoint_matches_central_differences(which):
+    hot, D, case, T, R, X = _setup()
+    with torch.no_grad():
+        outs = D.opacity(T, R, X)
+    ws = _loss_weights(outs, seed=7)
+    Tg, Rg, Xg = T.clone().requires_grad_(), R.clone().requires_grad_(), X.clone().requires_grad_()
+    L = _L(D, ws, Tg, Rg, Xg)
+    L.backward()
+    grads = {"temp": Tg.grad, "rho": Rg.grad, "massfr": Xg.grad}
+    gen = torch.Generator(device=T.device).manual_seed(11)
+    base = {"temp": T, "rho": R, "massfr": X}[which]
+    h = 1e-6
+    for trial in range(3):
+        v = torch.randn(base.shape, generator=gen, device=T.device, dtype=torch.float64) * base
+        if which == "massfr":
+            v = v * (X > 0)
+        ad = float((grads[which] * v).sum())
+
+        def at(s):
+            args = {"temp": T, "rho": R, "massfr": X}
+            args[which] = base + s * h * v
+            with torch.no_grad():
+                return float(_L(D, ws, args["temp"], args["rho"], args["massfr"]))
+
+        fd = (at(1.0) - at(-1.0)) / (2.0 * h)
+        assert ad == pytest.approx(fd, rel=RTOL), (which, trial, ad, fd)
+    hot.close()
+
+
+def test_forward_equals_standard_path():
+    """The differentiable forward runs the same kernels as slg_saha_eos +
+    slg_physical_opacity: the same nelec, opacities and Thomson opacity."""
+    hot, D, case, T, R, X = _setup(nc=16, ng=80)
+    with torch.no_grad():
+        cap, sig, grey, ross, ol = D.opacity(T, R, X)
+    nelec = D.nelec.cpu().numpy()
+    mass, natom, natomfr = W.composition_state(case.gas.rho, case.gas.massfr, case.grid.vol)
+    nel, oc, ginv, it = hot.saha_eos(case.gas.temp, natom, case.grid.vol, natomfr, np.ones(16), acc=1e-14, noc=4)
+    np.testing.assert_allclose(nel, nelec, rtol=1e-12)
+    op = hot.physical_opacity(case.gas.temp, natom, nel, case.grid.vol, mass, natomfr, oc, ginv)
+    np.testing.assert_allclose(cap.cpu().numpy().astype(np.float32), op["cap"], rtol=2e-7)
+    np.testing.assert_allclose(sig.cpu().numpy(), op["sig"], rtol=1e-12)
+    hot.close()
