@@ -57,6 +57,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=0, help="particles in the CPU-baseline sample (0: auto)")
+    ap.add_argument("--workload", default="batched", choices=["batched", "timestep"],
+                    help="batched: many models in one persistent launch, graph-captured steps; "
+                         "timestep: one 256-shell model on physical opacities")
+    ap.add_argument("--nmodel", type=int, default=128)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 per-model comparison")
     return ap.parse_args()
 
 
@@ -325,7 +330,266 @@ def cpu_baseline(a, case, hot, ts, emit, nvol, params, budget_s=20.0):
             "transport_particle_steps_per_s": steps / dt}
 
 
+# ------------------------------------------------------------------ batched workload
+SEED_BATCH = 4
+
+
+def batched_config(a, world, b):
+    return {"workload": "batched: independent ejecta models, one persistent mixed-precision launch, "
+                        "graph-captured steps (configs[3])",
+            "models_per_gpu": int(len(b.nx)), "shells_total": int(b.nx.sum()), "shells_range": [50, 400],
+            "particles_per_gpu": int(b.npart.sum()), "particles_range": [1e5, 1e7],
+            "snapshot_days_range": [1.0, 30.0], "groups": int(b.groups.ng),
+            "opacity": "analytic grey kappa = 0.1 (rho/1e-13) (T/1e4)^-1.5 cm^2/g (configs[0] physics)",
+            "tauddmc": 5.0, "taulump": 10.0, "transport_precision": "mixed (FP32 distances, FP64 weights/tallies)",
+            "graph_steps": a.steps, "parallelism": f"models{world}",
+            "l2": "inputs larger than L2 (particle array 18.8 GB per GPU)"}
+
+
+def fp64_per_model(b, ts, params, local, seed):
+    """The plain FP64 form on the same models: it advances one model per
+    launch (each model in its own context and stream, launched back to back).
+    One step; returns (particle-steps/s, steps, seconds)."""
+    import torch
+    from superlite_b200 import HotPath
+    hots = []
+    co = np.concatenate([[0], np.cumsum(b.nx)])
+    eo = co + np.arange(len(b.nx) + 1)
+    po = np.concatenate([[0], np.cumsum(b.npart)])
+    for m in range(len(b.nx)):
+        h = HotPath(local)
+        h.set_groups(b.groups.wl)
+        h.set_grid(b.xarr[eo[m]:eo[m + 1] + 1], b.vxarr[eo[m]:eo[m + 1] + 1], b.vol[co[m]:co[m + 1]],
+                   b.divv[co[m]:co[m + 1]])
+        hots.append(h)
+    ts.prepare(seed)
+    ts.sync()
+    sl = lambda t, m: t[co[m]:co[m + 1]]
+    outs = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for m, h in enumerate(hots):
+        tables = dict(tempinv=sl(ts.tempinv, m), sig=sl(ts.sig, m), capgrey=sl(ts.capgrey, m),
+                      emitprob=sl(ts.emitprob, m), opaclump=sl(ts.opaclump, m), cap=sl(ts.cap, m))
+        outs.append(h.particle_advance_dev(tables, ts.prt[po[m]:po[m + 1]], ts.isv[po[m]:po[m + 1]],
+                                           sl(ts.tally, m), sl(ts.jrad, m), sl(ts.eamp, m), params,
+                                           seed=seed, precision=0))
+    for h in hots:
+        h.sync()
+    dt = time.perf_counter() - t0
+    steps = sum(o.nstepimc + o.nstepddmc for o in outs)
+    ts.flux()  # tally the escaped particles and free their slots in the batched context
+    ts.sync()
+    for h in hots:
+        h.close()
+    return steps / dt, int(steps), dt
+
+
+def run_batched(a):
+    import torch
+    from superlite_b200 import HotPath, workloads as W
+    from superlite_b200.timestep import BatchTimestep
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    b = W.analytic_batch(nmodel=a.nmodel, seed=SEED_BATCH + 1000 * rank)
+    params = W.TransportParams()
+    hot = HotPath(local)
+    ts = BatchTimestep(hot, b, params, precision=1)
+    stream = ts.stream
+    seed0 = 1000 * (rank + 1)
+    ts.prepare(seed0 - 1)
+    variant, tune_ms = ts.autotune(seed=seed0 - 1, nsample=1_000_000)
+    ts.finish(seed0 - 1)
+    ts.sync()
+    # warm-up steps (uncaptured); the last one also times its phases
+    ev_p = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    for k in range(a.warmup):
+        if k == a.warmup - 1:
+            ev_p[0].record(stream)
+            ts.prepare(seed0 + k)
+            ev_p[1].record(stream)
+            ts.finish(seed0 + k)
+            ev_p[2].record(stream)
+        else:
+            ts.step(seed0 + k)
+        ts.sync()
+    t_prep = ev_p[0].elapsed_time(ev_p[1]) if a.warmup else None
+    t_tr = ev_p[1].elapsed_time(ev_p[2]) if a.warmup else None
+    # the timed steps: one CUDA graph of a.steps whole timesteps, replayed once
+    ts.capture(a.steps, seed0 + a.warmup)
+    hot.transport_totals(reset=True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    ev[0].record(stream)
+    ts.replay(1)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = ev[0].elapsed_time(ev[1])
+    tot = hot.transport_totals()
+    steps_total = tot["nstepimc"] + tot["nstepddmc"]
+    ms_max, steps_all = ms, steps_total
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_max = float(t.item())
+        s = torch.tensor([steps_total], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(s)
+        steps_all = int(s.item())
+    value = steps_all / (ms_max / 1e3)
+    peak, peak_kind = measured_peaks()
+    tr_rate = (steps_total / a.steps) / (t_tr / 1e3) if t_tr else None
+    achieved = BYTES_PER_STEP * tr_rate / 1e9 if tr_rate else None
+    res = {
+        "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded generator, superlite_b200/workloads.py)",
+        "config": batched_config(a, world, b),
+        "phase_ms_last_warmup_step": {"sources+opacity+coefficients": t_prep, "particle_advance": t_tr},
+        "counters": {k: tot[k] for k in ("npckt", "nflux", "nstepimc", "nstepddmc", "nstepmax", "nmethodswap",
+                                         "ierr")},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "kernel": "particle_advance_mixed_kernel",
+                     "basis": f"{BYTES_PER_STEP:.0f} B per particle-step x steps of one step / particle_advance "
+                              f"time of the last warm-up step; peak {peak_kind}"},
+        "clocks": clocks, "autotune": {"variant": variant, "sample_ms": tune_ms},
+        "gpu_launches": None,
+    }
+    # kernels of one step: 6 (sources) + 1 (analytic opacity) + 1 (means) + 1 (leakage) + 1 (emitprob)
+    # + 1 (sourcetally) + 2 (cell tables, particle loop) + 1 (counter fold) + nmodel (flux tallies)
+    res["gpu_launches"] = (14 + int(len(b.nx))) * a.steps
+    if not a.no_fp64:
+        rate, st64, dt64 = fp64_per_model(b, ts, params, local, seed0 + 999)
+        res["fp64_plain_per_model"] = {"value": rate, "unit": "particle-steps/s", "steps": st64, "seconds": dt64,
+                                       "form": "FP64 particle loop, one launch per model, each model in its own "
+                                               "context and stream"}
+        res["mixed_batched_over_fp64_plain"] = value / rate
+    if not a.no_e2e:
+        res["e2e"] = batched_e2e(a, b, params, local, seed0)
+    if rank == 0 and world == 1 and not a.no_cpu:
+        res["cpu_baseline"] = batched_cpu_baseline(a, b, params)
+    hot.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(res))
+
+
+def batched_e2e(a, b, params, local, seed0):
+    """One step of the batch through the host-pointer C ABI (the calls a
+    Fortran driver makes, every module array copied in and out)."""
+    from superlite_b200 import HotPath
+    from superlite_b200.api import PACKET_DTYPE
+    hot = HotPath(local)
+    hot.set_groups(b.groups.wl)
+    hot.set_models(b.nx, b.npart, b.xarr, b.vxarr, b.vol, b.divv)
+    n = int(b.npart.sum())
+    prt = np.zeros(n, dtype=PACKET_DTYPE)
+    isv = np.ones(n, dtype=np.int32)
+    emit, _ = hot.sourceenergy(b.temp, L_BOL)
+    nvol, _ = hot.models_sourcenumbers(emit, b.npart)
+    tinv = 1.0 / b.temp
+    times, steps = [], 0
+    for k in range(2):
+        t0 = time.perf_counter()
+        hot.interior_source(b.temp, emit, nvol, prt, isv, seed=seed0 + 31 + k)
+        sig, cap = hot.analytic_opacity(b.temp, b.rho, kind=1)
+        grey, ross = hot.opacity_means(b.temp, sig, cap)
+        ol = hot.leakage_opacity(tinv, sig, cap, tauddmc=params.tauddmc, taulump=params.taulump)
+        ep = hot.emission_probability(tinv, cap, grey)
+        tables = dict(tempinv=tinv, sig=sig, capgrey=grey, emitprob=ep, opaclump=ol, cap=cap)
+        r = hot.particle_advance(tables, prt, isv, params, seed=seed0 + 41 + k, precision=1)
+        hot.fluxtally(prt, isv, b.groups.wl)
+        t1 = time.perf_counter()
+        if k > 0:
+            times.append(t1 - t0)
+            steps += r["nstepimc"] + r["nstepddmc"]
+    hot.close()
+    nc, ng = int(b.nx.sum()), b.groups.ng
+    P = n * 68
+    h2d = 3 * P + nc * 8 * 12 + 3 * nc * ng * 4 + nc * hot.nep * 8
+    d2h = 3 * P + nc * 8 * 20 + 2 * nc * ng * 4 + nc * ng * 8 + 3 * len(b.nx) * ng * 8
+    return {"value": steps / sum(times), "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "steps": 1,
+            "path": "host-pointer C ABI per phase (slg_interior_source .. slg_fluxtally), all models"}
+
+
+def batched_cpu_baseline(a, b, params, budget_s=20.0):
+    """The oracle (C++ restatement of the Fortran, FP64, mzran, OpenMP over
+    particles) on a bounded sample: a few models, a particle sample each."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    from superlite_b200 import workloads as W
+    cores = os.cpu_count() or 1
+    co = np.concatenate([[0], np.cumsum(b.nx)])
+    eo = co + np.arange(len(b.nx) + 1)
+    steps = 0
+    dt = 0.0
+    used = []
+    for m in range(len(b.nx)):
+        g = W.Grid(int(b.nx[m]), 0.0, b.xarr[eo[m]:eo[m + 1] + 1], b.vxarr[eo[m]:eo[m + 1] + 1],
+                   b.vol[co[m]:co[m + 1]], b.divv[co[m]:co[m + 1]])
+        T, rho = b.temp[co[m]:co[m + 1]], b.rho[co[m]:co[m + 1]]
+        sig, cap = po.analytic_opacity(b.groups.wlinv, T, rho, kind=1)
+        tinv = 1.0 / T
+        grey = po.planckmean(b.groups.wlinv, T, cap)
+        ol = po.leakage_opacity11(g, b.groups.wlinv, tinv, sig, cap, tauddmc=params.tauddmc, taulump=params.taulump)
+        ep = po.emission_probability(b.groups.wlinv, tinv, cap, grey, b.groups.nep, b.groups.nepg)
+        tt = po.TransportTables(g, b.groups, tinv, sig, cap, grey, ep, ol, params)
+        sample = int(min(b.npart[m], a.cpu_sample or 4000))
+        prt, isv, _, _, _ = po.make_source_particles(g, b.groups, T, L_BOL, sample)
+        st = po.rnd_init(cores, m)
+        t0 = time.perf_counter()
+        r = po.particle_advance(tt, prt, isv, rngmode=0, nthreads=cores, rnd_states=st)
+        dt += time.perf_counter() - t0
+        steps += r["nstepimc"] + r["nstepddmc"]
+        used.append((m, sample))
+        if dt > budget_s:
+            break
+    return {"value": steps / dt, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "sample": f"{len(used)} of {len(b.nx)} models, {used[0][1]} particles each (mzran, OpenMP static,1, "
+                      f"FP64 oracle), transport only"}
+
+
 # ------------------------------------------------------------------ reference arm
+def run_reference_batched(a):
+    """The reference's CPU path (the oracle restatement, FP64, one model at a
+    time as the reference runs) on the batched workload: per step a bounded
+    sample of models and particles on the host cores."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from superlite_b200 import workloads as W
+    b = W.analytic_batch(nmodel=a.nmodel, seed=SEED_BATCH)
+    params = W.TransportParams()
+    rates, tsteps = [], []
+    for k in range(a.warmup + a.steps):
+        t0 = time.perf_counter()
+        r = batched_cpu_baseline(a, b, params, budget_s=6.0)
+        if k >= a.warmup:
+            rates.append(r["value"])
+            tsteps.append(time.perf_counter() - t0)
+    value = statistics.mean(rates)
+    res = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": 1e3 * statistics.mean(tsteps), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded generator, superlite_b200/workloads.py)", "config": batched_config(a, world, b),
+           "impl": "reference",
+           "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": r["cores"], "kind": "port",
+                            "sample": "per step: " + r["sample"]},
+           "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(res))
+
+
 def run_reference(a):
     """The reference's CPU path as restated by the oracle (the Fortran itself has
     no compiler here), on the host cores, same workload, bounded sample per step."""
@@ -381,7 +645,12 @@ def run_reference(a):
 def main():
     a = parse()
     if a.impl == "reference":
-        run_reference(a)
+        if a.workload == "batched":
+            run_reference_batched(a)
+        else:
+            run_reference(a)
+    elif a.workload == "batched":
+        run_batched(a)
     else:
         run_ours(a)
 

@@ -282,6 +282,10 @@ int slg_dev_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity
                              double* gas_sig, float* gas_cap, float* gas_emiss, double* cap64);
 int slg_dev_opacity_means(slg_ctx* ctx, const double* temp, const double* sig,
                           const float* gas_cap, double* capgrey, double* capross);
+int slg_dev_analytic_opacity(slg_ctx* ctx, const double* temp, const double* rho, int32_t kind,
+                             double capcoef, double captpwr, double caprpwr, double sigcoef,
+                             double sigtpwr, double sigrpwr, double ldisp1, double ldisp2,
+                             double* gas_sig, float* gas_cap);
 int slg_dev_saha_eos(slg_ctx* ctx, const double* temp, const double* natom, const double* vol,
                      const double* natomfr, double acc, double* nelec, int32_t noc, double* oc,
                      double* ginv, int32_t* iconv);

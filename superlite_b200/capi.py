@@ -63,6 +63,7 @@ SIGNATURES = {
     "slg_set_atomic_data": (C.c_int, [vp, C.c_int32, C.c_int32, vp, C.c_int64, vp, vp, vp, vp]),
     "slg_physical_opacity": (C.c_int, [vp, C.POINTER(SlgGas), C.POINTER(SlgOpacityFlags), vp, vp, vp, vp, vp]),
     "slg_analytic_opacity": (C.c_int, [vp, vp, vp, C.c_int32] + [C.c_double] * 8 + [vp, vp]),
+    "slg_dev_analytic_opacity": (C.c_int, [vp, vp, vp, C.c_int32] + [C.c_double] * 8 + [vp, vp]),
     "slg_opacity_means": (C.c_int, [vp, vp, vp, vp, vp, vp]),
     "slg_leakage_opacity11": (C.c_int, [vp, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
     "slg_emission_probability": (C.c_int, [vp, vp, vp, vp, vp]),

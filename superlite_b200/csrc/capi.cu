@@ -38,7 +38,7 @@ void* scratch(slg_ctx* ctx, int slot, size_t bytes) {
     cudaFree(b.p);
     b.p = nullptr;
     b.bytes = 0;
-    if (slot >= 12 && slot <= 20) ctx->tables.nx = ctx->tables.ng = 0;
+    if ((slot >= 12 && slot <= 20) || slot == 72) ctx->tables.nx = ctx->tables.ng = 0;
   }
   const size_t alloc = bytes + bytes / 8;  // headroom for small growth
   if (cudaMalloc(&b.p, alloc) != cudaSuccess) {
@@ -560,6 +560,17 @@ int slg_analytic_opacity(slg_ctx* ctx, const double* temp, const double* rho, in
   down(ctx, gas_sig, ds, nc, &rc);
   down(ctx, gas_cap, dc, nc * ng, &rc);
   return finish(ctx, rc);
+}
+
+int slg_dev_analytic_opacity(slg_ctx* ctx, const double* temp, const double* rho, int32_t kind, double capcoef,
+                             double captpwr, double caprpwr, double sigcoef, double sigtpwr, double sigrpwr,
+                             double ldisp1, double ldisp2, double* gas_sig, float* gas_cap) {
+  if (!ctx || !temp || !rho || !gas_sig || !gas_cap || kind < 1 || kind > 3)
+    return set_error(ctx, SLG_ERR_ARG, "bad argument");
+  if (!need_grid(ctx)) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
+  cudaSetDevice(ctx->device);
+  const double c[8] = {capcoef, captpwr, caprpwr, sigcoef, sigtpwr, sigrpwr, ldisp1, ldisp2};
+  return launch_analytic_opacity(ctx, temp, rho, kind, c, gas_sig, gas_cap);
 }
 
 int slg_opacity_means(slg_ctx* ctx, const double* temp, const double* sig, const float* gas_cap, double* capgrey,

@@ -29,8 +29,14 @@ struct CellTables {
   // per-cell scalars: nlump, emitlump, caplump, doplump, capgreyinv, speclump
   int32_t* nlump = nullptr;
   double* scal = nullptr;     // 8 doubles per cell (see SCAL_*)
+  // guide tables of the four running sums above (dop, left, right, scat):
+  // per cell and table kGuideM+1 entries, entry k = number of sums <= k/kGuideM,
+  // so a draw r in [k, k+1)/kGuideM is searched only between entries k and k+1
+  // (null: plain search over the whole table)
+  int16_t* guide = nullptr;
   int nx = 0, ng = 0;
 };
+constexpr int kGuideM = 256;  // a power of two, so r * kGuideM and k / kGuideM are exact
 enum { SCAL_EMITLUMP = 0, SCAL_CAPLUMP, SCAL_DOPLUMP, SCAL_CAPGREYINV, SCAL_SPECLUMP, SCAL_FAR,
        SCAL_DX3, SCAL_DVDR, SCAL_N };
 

@@ -41,12 +41,12 @@ struct Ptcl {
   int ix, ig, itype, stat, idist;  // ic == ix (1-D, no void cells)
 };
 
-// first position q in [0,n) with a[q] > r, else n-1 (the last position a
-// linear scan visits).  a is non-decreasing, so the count of entries <= r
-// is a prefix; an 8-ary search issues the 7 probes of a round together,
-// which needs 4 dependent rounds of loads for n = 2000 instead of 11.
-__device__ inline int first_gt(const double* __restrict__ a, int n, double r) {
-  int lo = 0, hi = n;  // answer in [lo, hi]
+// first_gt: first position q in [0,n) with a[q] > r, else n-1 (the last
+// position a linear scan visits).  a is non-decreasing, so the count of
+// entries <= r is a prefix; an 8-ary search issues the 7 probes of a round
+// together, which needs 4 dependent rounds of loads for n = 2000 instead of
+// 11.  first_gt_range: the same when the answer is known to lie in [lo, hi].
+__device__ inline int first_gt_range(const double* __restrict__ a, int lo, int hi, int n, double r) {
   while (hi - lo > 8) {
     const int step = (hi - lo) >> 3;
     double v[7];
@@ -68,6 +68,20 @@ __device__ inline int first_gt(const double* __restrict__ a, int n, double r) {
   for (int j = 0; j < 8; ++j) c += (lo + j < hi) && v[j] <= r;
   const int q = lo + c;
   return q < n ? q : n - 1;
+}
+__device__ inline int first_gt(const double* __restrict__ a, int n, double r) {
+  return first_gt_range(a, 0, n, n, r);
+}
+
+// first_gt over running-sum table `table` (0 dop, 1 left, 2 right, 3 scat) of
+// cell `cell` (0-based over all models), narrowed by the cell's guide table:
+// the same answer, after one guide load and a search of about n/kGuideM entries.
+__device__ inline int cdf_search(const CellTables& T, int table, int cell, const double* __restrict__ a, int n,
+                                 double r) {
+  if (!T.guide) return first_gt(a, n, r);
+  const int16_t* g = T.guide + ((size_t)cell * 4 + table) * (kGuideM + 1);
+  const int k = (int)(r * (double)kGuideM);  // exact: kGuideM is a power of two and r < 1
+  return first_gt_range(a, g[k], g[k + 1], n, r);
 }
 
 __device__ inline double CAPd(const TrnArgs& A, int ig, int ic) {
@@ -461,7 +475,7 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       iiig = ig;
     } else {
       r1 = rng.draw();
-      const int q = first_gt(A.T.cdf_dop + off, glump, r1);
+      const int q = cdf_search(A.T, 0, ic - 1, A.T.cdf_dop + off, glump, r1);
       iiig = divv >= 0.0 ? glumps[q] : glumps[glump - 1 - q];
     }
     if (divv >= 0.0) {
@@ -505,7 +519,7 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       mu = r1 > r2 ? r1 : r2;
       if (glump != 0) {
         r1 = rng.draw();
-        ig = glumps[first_gt(A.T.cdf_right + off, glump, r1)];
+        ig = glumps[cdf_search(A.T, 2, ic - 1, A.T.cdf_right + off, glump, r1)];
       }
       r1 = rng.draw();
       wl = 1.0 / (r1 * A.wlinv[ig] + (1.0 - r1) * A.wlinv[ig - 1]);
@@ -525,7 +539,7 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       iiig = ig;
     } else {
       r1 = rng.draw();
-      iiig = glumps[first_gt((right ? A.T.cdf_right : A.T.cdf_left) + off, glump, r1)];
+      iiig = glumps[cdf_search(A.T, right ? 2 : 1, ic - 1, (right ? A.T.cdf_right : A.T.cdf_left) + off, glump, r1)];
     }
     const double dxl = right ? A.xarr[ix + 1] - Xb : Xa - A.xarr[ix - 2];
     if ((A.sig[l - 1] + CAPd(A, iiig, l)) * dxl < A.tauddmc) {
@@ -556,7 +570,7 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       iiig = emitgroup_dev(A, r1, ic);
     } else {
       r1 = rng.draw();
-      const int q = first_gt(A.T.cdf_scat + off, ng - glump, r1);
+      const int q = cdf_search(A.T, 3, ic - 1, A.T.cdf_scat + off, ng - glump, r1);
       iiig = glumps[ng - 1 - q];
     }
     ig = iiig;

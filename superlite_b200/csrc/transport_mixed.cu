@@ -339,7 +339,7 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
     if (glump == 0) {
       iiig = ig;
     } else {
-      const int q = first_gt(A.T.cdf_dop + off, glump, (double)rng.draw());
+      const int q = cdf_search(A.T, 0, gc, A.T.cdf_dop + off, glump, (double)rng.draw());
       iiig = divv >= 0.f ? glumps[q] : glumps[glump - 1 - q];
     }
     if (divv >= 0.f) {
@@ -376,7 +376,7 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
       p.stat = 1;
       const float a = rng.draw(), b = rng.draw();
       mu = a > b ? a : b;
-      if (glump != 0) ig = glumps[first_gt(A.T.cdf_right + off, glump, (double)rng.draw())];
+      if (glump != 0) ig = glumps[cdf_search(A.T, 2, gc, A.T.cdf_right + off, glump, (double)rng.draw())];
       const float r = rng.draw();
       wl = 1.0f / (r * (float)A.wlinv[ig] + (1.0f - r) * (float)A.wlinv[ig - 1]);
       p.x = X[v.nx];
@@ -392,7 +392,8 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
     }
     const int l = right ? ix + 1 : ix - 1;
     iiig = glump == 0 ? ig
-                      : glumps[first_gt((right ? A.T.cdf_right : A.T.cdf_left) + off, glump, (double)rng.draw())];
+                      : glumps[cdf_search(A.T, right ? 2 : 1, gc, (right ? A.T.cdf_right : A.T.cdf_left) + off, glump,
+                                          (double)rng.draw())];
     const float dxl = (float)(right ? X[ix + 1] - Xb : Xa - X[ix - 2]);
     if (((float)A.sig[v.co + l - 1] + capf(A, iiig, v.co + l)) * dxl < tau_d) {
       p.itype = 1;
@@ -419,7 +420,7 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
     if (glump == 0) {
       iiig = emitgroup_dev(A, (double)rng.draw(), gc + 1);
     } else {
-      const int q = first_gt(A.T.cdf_scat + off, ng - glump, (double)rng.draw());
+      const int q = cdf_search(A.T, 3, gc, A.T.cdf_scat + off, ng - glump, (double)rng.draw());
       iiig = glumps[ng - 1 - q];
     }
     ig = iiig;

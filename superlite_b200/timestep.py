@@ -143,3 +143,104 @@ class DeviceTimestep:
     def counters(self):
         from .api import transport_out_dict
         return transport_out_dict(self._tout)
+
+
+class BatchTimestep:
+    """One timestep of many independent models in one context (slg_set_models),
+    device resident: analytic opacity (configs[0] physics), Planck/Rosseland
+    means, leakage opacities, emission probabilities, source particles, the
+    source tally, one persistent particle loop over every model's particles
+    (precision 1) and per-model flux tallies.  ``capture(nsteps, seed)``
+    records nsteps such steps in one CUDA graph; ``replay()`` runs it."""
+
+    def __init__(self, hot: HotPath, batch, params, precision: int = 1, L_bol: float = 1e42):
+        self.hot = hot
+        self.params = params
+        self.precision = precision
+        b = batch
+        hot.set_groups(b.groups.wl)
+        hot.set_models(b.nx, b.npart, b.xarr, b.vxarr, b.vol, b.divv)
+        dev = torch.device("cuda", hot.device)
+        nc, ng = int(b.nx.sum()), b.groups.ng
+        self.nc, self.ng, self.nmodel = nc, ng, len(b.nx)
+        self.npart = int(b.npart.sum())
+        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)
+        e64 = lambda *s: torch.empty(s, dtype=torch.float64, device=dev)
+        self.temp, self.rho = f64(b.temp), f64(b.rho)
+        self.tempinv = 1.0 / self.temp
+        self.sig, self.capgrey, self.capross = e64(nc), e64(nc), e64(nc)
+        self.cap = torch.empty((nc, ng), dtype=torch.float32, device=dev)
+        self.opaclump = e64(nc, 11)
+        self.emitprob = e64(nc, hot.nep)
+        self.tally, self.jrad, self.eamp = e64(nc), e64(nc, ng), e64(nc)
+        self.mswap = torch.empty(nc, dtype=torch.int32, device=dev)
+        self.src_energy = e64(ng, nc)
+        self.src_number = torch.empty((ng, nc), dtype=torch.int32, device=dev)
+        self.flx_wl = f64(b.groups.wl)
+        self.lum, self.lumdev = e64(self.nmodel, ng), e64(self.nmodel, ng)
+        self.lumnum = torch.empty((self.nmodel, ng), dtype=torch.int32, device=dev)
+        self.prt = torch.empty((self.npart, 8), dtype=torch.float64, device=dev)
+        self.isv = torch.ones(self.npart, dtype=torch.int32, device=dev)
+        self.emit, _ = hot.sourceenergy(b.temp, L_bol)
+        self.nvol, self.nnew = hot.models_sourcenumbers(self.emit, b.npart)
+        self._tin = HotPath.transport_in(self.tempinv, self.sig, self.capgrey, self.emitprob, self.opaclump,
+                                         self.cap, params, precision)
+        self._tout = capi.SlgTransportOut(ptr(self.tally), ptr(self.jrad), ptr(self.eamp), ptr(self.mswap),
+                                          0.0, 0.0, 0.0)
+        self.stream = torch.cuda.ExternalStream(hot.stream(), device=dev)
+
+    def _chk(self, rc):
+        self.hot._check(rc)
+
+    def step(self, seed: int):
+        self.prepare(seed)
+        self.finish(seed)
+
+    def prepare(self, seed: int):
+        """Sources, opacities and coefficients of a step (everything before the particle loop)."""
+        L, h, p = self.hot.lib, self.hot.h, self.params
+        self.hot.interior_source(self.temp, self.emit, self.nvol, self.prt, self.isv, seed=2 * seed)
+        self._chk(L.slg_dev_analytic_opacity(h, ptr(self.temp), ptr(self.rho), 1, 1e18, -1.5, 2.0, 0.0, 0.0, 0.0,
+                                             0.0, 0.0, ptr(self.sig), ptr(self.cap)))
+        self._chk(L.slg_dev_opacity_means(h, ptr(self.temp), ptr(self.sig), ptr(self.cap), ptr(self.capgrey),
+                                          ptr(self.capross)))
+        self._chk(L.slg_dev_leakage_opacity11(h, ptr(self.tempinv), ptr(self.sig), ptr(self.cap), None, p.tauddmc,
+                                              p.taulump, ptr(self.opaclump)))
+        self._chk(L.slg_dev_emission_probability(h, ptr(self.tempinv), ptr(self.cap), ptr(self.capgrey),
+                                                 ptr(self.emitprob)))
+        self._chk(L.slg_dev_sourcetally(h, self.npart, ptr(self.prt), ptr(self.isv), ptr(self.src_energy),
+                                        ptr(self.src_number)))
+
+    def finish(self, seed: int):
+        """The particle loop over every model and the per-model flux tallies."""
+        L, h = self.hot.lib, self.hot.h
+        self._tout.tot_evelo = self._tout.tot_eout = self._tout.tot_sflux = 0.0
+        self._chk(L.slg_dev_particle_advance(h, C.byref(self._tin), ptr(self.prt), ptr(self.isv), self.npart,
+                                             2 * seed + 1, C.byref(self._tout)))
+        self.flux()
+
+    def flux(self):
+        """fluxtally per model (also frees the escaped particles' slots)."""
+        self._chk(self.hot.lib.slg_dev_fluxtally(self.hot.h, self.npart, ptr(self.prt), ptr(self.isv), self.ng,
+                                                 ptr(self.flx_wl), ptr(self.lum), ptr(self.lumdev),
+                                                 ptr(self.lumnum)))
+
+    def autotune(self, seed=0, nsample=1_000_000):
+        best = C.c_int32(0)
+        ms = (C.c_float * 4)()
+        self._chk(self.hot.lib.slg_autotune_transport(self.hot.h, C.byref(self._tin), ptr(self.prt), ptr(self.isv),
+                                                      self.npart, seed, int(min(nsample, self.npart)),
+                                                      C.byref(best), ms))
+        return int(best.value), [float(m) for m in ms]
+
+    def capture(self, nsteps: int, seed: int):
+        self.hot.graph_begin()
+        for k in range(nsteps):
+            self.step(seed + k)
+        self.hot.graph_end()
+
+    def replay(self, n: int = 1):
+        self.hot.graph_launch(n)
+
+    def sync(self):
+        self.hot.sync()

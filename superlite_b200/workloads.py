@@ -450,6 +450,47 @@ def model_batch(nmodel: int = 128, seed: int = 4, ng: int = 2000, nline: int = 5
                       concat_gas([c.gas for c in models]))
 
 
+@dataclasses.dataclass
+class AnalyticBatch:
+    """Independent ejecta models with configs[0] physics (analytic grey
+    opacity, so no composition enters), laid out for slg_set_models."""
+    nx: np.ndarray          # shells per model (int32)
+    npart: np.ndarray       # particle slots per model (int64)
+    t_days: np.ndarray
+    groups: Groups
+    xarr: np.ndarray        # each model's nx+1 edges, model after model
+    vxarr: np.ndarray
+    vol: np.ndarray         # per cell, model order
+    divv: np.ndarray
+    temp: np.ndarray
+    rho: np.ndarray
+
+
+def analytic_batch(nmodel: int = 128, seed: int = 4, ng: int = 100, nx_range=(50, 400),
+                   npart_range=(1e5, 1e7), t_range_days=(1.0, 30.0), nx=None, npart=None) -> AnalyticBatch:
+    """The batched workload: nmodel models with shells ~ U{nx_range},
+    particle budgets log-uniform in npart_range and snapshot times
+    log-uniform in t_range_days; per model (seed [seed, m]) T ~ U(6000, 14000)
+    K and the 1 Msun broken power-law density of configs[0]; 100 log groups."""
+    rng = np.random.default_rng(seed)
+    nxs = (rng.integers(nx_range[0], nx_range[1] + 1, nmodel) if nx is None
+           else np.asarray(nx)).astype(np.int32)
+    nps = (np.exp(rng.uniform(math.log(npart_range[0]), math.log(npart_range[1]), nmodel)).astype(np.int64)
+           if npart is None else np.asarray(npart, dtype=np.int64))
+    ts = np.exp(rng.uniform(math.log(t_range_days[0]), math.log(t_range_days[1]), len(nxs)))
+    grids, temps, rhos = [], [], []
+    for m in range(len(nxs)):
+        mr = np.random.default_rng([seed, m])
+        g = homologous_grid(int(nxs[m]), float(ts[m]) * PC_DAY)
+        rho, _ = broken_powerlaw_rho(g)
+        grids.append(g)
+        temps.append(mr.uniform(6000.0, 14000.0, int(nxs[m])))
+        rhos.append(rho)
+    cat = lambda k: np.concatenate([getattr(g, k) for g in grids])
+    return AnalyticBatch(nxs, nps, ts, group_grid(ng), cat("xarr"), cat("vxarr"), cat("vol"), cat("divv"),
+                         np.concatenate(temps), np.concatenate(rhos))
+
+
 def analytic_grey(grid: Grid, temp: np.ndarray, rho: np.ndarray, ng: int):
     """Config-1 opacity source: in_opacanaltype='grey', capcoef=1e18,
     captpwr=-1.5, caprpwr=2 (analytic_opacity.f90:38-43); sigma = 0."""
