@@ -46,7 +46,8 @@ BYTES_PER_STEP = 128.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 1 for the batched workload, whose step runs about a minute; 3 otherwise)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--npart", type=float, default=5e7)
@@ -343,13 +344,14 @@ def batched_config(a, world, b):
             "opacity": "analytic grey kappa = 0.1 (rho/1e-13) (T/1e4)^-1.5 cm^2/g (configs[0] physics)",
             "tauddmc": 5.0, "taulump": 10.0, "transport_precision": "mixed (FP32 distances, FP64 weights/tallies)",
             "graph_steps": a.steps, "parallelism": f"models{world}",
-            "l2": "inputs larger than L2 (particle array 18.8 GB per GPU)"}
+            "l2": f"inputs larger than L2 (particle array {b.npart.sum() * 64 / 1e9:.1f} GB per GPU)"}
 
 
 def fp64_per_model(b, ts, params, local, seed):
-    """The plain FP64 form on the same models: it advances one model per
-    launch (each model in its own context and stream, launched back to back).
-    One step; returns (particle-steps/s, steps, seconds)."""
+    """The plain FP64 form on the same models: one model per call, as the
+    single-model C ABI is called by a driver that runs the models one after
+    another (each model in its own context; every call completes before the
+    next).  One step; returns (particle-steps/s, steps, seconds)."""
     import torch
     from superlite_b200 import HotPath
     hots = []
@@ -359,7 +361,7 @@ def fp64_per_model(b, ts, params, local, seed):
     for m in range(len(b.nx)):
         h = HotPath(local)
         h.set_groups(b.groups.wl)
-        h.set_grid(b.xarr[eo[m]:eo[m + 1] + 1], b.vxarr[eo[m]:eo[m + 1] + 1], b.vol[co[m]:co[m + 1]],
+        h.set_grid(b.xarr[eo[m]:eo[m + 1]], b.vxarr[eo[m]:eo[m + 1]], b.vol[co[m]:co[m + 1]],
                    b.divv[co[m]:co[m + 1]])
         hots.append(h)
     ts.prepare(seed)
@@ -374,7 +376,6 @@ def fp64_per_model(b, ts, params, local, seed):
         outs.append(h.particle_advance_dev(tables, ts.prt[po[m]:po[m + 1]], ts.isv[po[m]:po[m + 1]],
                                            sl(ts.tally, m), sl(ts.jrad, m), sl(ts.eamp, m), params,
                                            seed=seed, precision=0))
-    for h in hots:
         h.sync()
     dt = time.perf_counter() - t0
     steps = sum(o.nstepimc + o.nstepddmc for o in outs)
@@ -401,13 +402,16 @@ def run_batched(a):
     ts = BatchTimestep(hot, b, params, precision=1)
     stream = ts.stream
     seed0 = 1000 * (rank + 1)
+    # warm-up 1: sources and opacities, the autotuner on a sample of this
+    # step's particles, then the particle loop with the chosen variant
     ts.prepare(seed0 - 1)
     variant, tune_ms = ts.autotune(seed=seed0 - 1, nsample=1_000_000)
     ts.finish(seed0 - 1)
     ts.sync()
-    # warm-up steps (uncaptured); the last one also times its phases
+    # warm-ups 2..W (uncaptured); the last one also times its phases
     ev_p = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-    for k in range(a.warmup):
+    t_prep = t_tr = None
+    for k in range(1, a.warmup):
         if k == a.warmup - 1:
             ev_p[0].record(stream)
             ts.prepare(seed0 + k)
@@ -417,8 +421,8 @@ def run_batched(a):
         else:
             ts.step(seed0 + k)
         ts.sync()
-    t_prep = ev_p[0].elapsed_time(ev_p[1]) if a.warmup else None
-    t_tr = ev_p[1].elapsed_time(ev_p[2]) if a.warmup else None
+        if k == a.warmup - 1:
+            t_prep, t_tr = ev_p[0].elapsed_time(ev_p[1]), ev_p[1].elapsed_time(ev_p[2])
     # the timed steps: one CUDA graph of a.steps whole timesteps, replayed once
     ts.capture(a.steps, seed0 + a.warmup)
     hot.transport_totals(reset=True)
@@ -444,6 +448,9 @@ def run_batched(a):
         torch.distributed.all_reduce(s)
         steps_all = int(s.item())
     value = steps_all / (ms_max / 1e3)
+    if rank == 0:
+        print(f"[bench] batched: {value:.4g} particle-steps/s, {ms_max:.0f} ms for {a.steps} step(s)", file=sys.stderr,
+              flush=True)
     peak, peak_kind = measured_peaks()
     tr_rate = (steps_total / a.steps) / (t_tr / 1e3) if t_tr else None
     achieved = BYTES_PER_STEP * tr_rate / 1e9 if tr_rate else None
@@ -464,13 +471,14 @@ def run_batched(a):
         "gpu_launches": None,
     }
     # kernels of one step: 6 (sources) + 1 (analytic opacity) + 1 (means) + 1 (leakage) + 1 (emitprob)
-    # + 1 (sourcetally) + 2 (cell tables, particle loop) + 1 (counter fold) + nmodel (flux tallies)
-    res["gpu_launches"] = (14 + int(len(b.nx))) * a.steps
+    # + 1 (sourcetally) + 2 (cell tables, particle loop) + 1 (counter fold) + nmodel (flux tallies);
+    # + 1 epoch counter per graph replay
+    res["gpu_launches"] = (14 + int(len(b.nx))) * a.steps + 1
     if not a.no_fp64:
         rate, st64, dt64 = fp64_per_model(b, ts, params, local, seed0 + 999)
         res["fp64_plain_per_model"] = {"value": rate, "unit": "particle-steps/s", "steps": st64, "seconds": dt64,
-                                       "form": "FP64 particle loop, one launch per model, each model in its own "
-                                               "context and stream"}
+                                       "form": "FP64 particle loop, one call per model (own context), "
+                                               "each completed before the next"}
         res["mixed_batched_over_fp64_plain"] = value / rate
     if not a.no_e2e:
         res["e2e"] = batched_e2e(a, b, params, local, seed0)
@@ -499,7 +507,7 @@ def batched_e2e(a, b, params, local, seed0):
     nvol, _ = hot.models_sourcenumbers(emit, b.npart)
     tinv = 1.0 / b.temp
     times, steps = [], 0
-    for k in range(2):
+    for k in range(1):  # one step (a step of this batch runs for about a minute)
         t0 = time.perf_counter()
         hot.interior_source(b.temp, emit, nvol, prt, isv, seed=seed0 + 31 + k)
         sig, cap = hot.analytic_opacity(b.temp, b.rho, kind=1)
@@ -510,9 +518,8 @@ def batched_e2e(a, b, params, local, seed0):
         r = hot.particle_advance(tables, prt, isv, params, seed=seed0 + 41 + k, precision=1)
         hot.fluxtally(prt, isv, b.groups.wl)
         t1 = time.perf_counter()
-        if k > 0:
-            times.append(t1 - t0)
-            steps += r["nstepimc"] + r["nstepddmc"]
+        times.append(t1 - t0)
+        steps += r["nstepimc"] + r["nstepddmc"]
     hot.close()
     nc, ng = int(b.nx.sum()), b.groups.ng
     P = n * 68
@@ -520,7 +527,8 @@ def batched_e2e(a, b, params, local, seed0):
     d2h = 3 * P + nc * 8 * 20 + 2 * nc * ng * 4 + nc * ng * 8 + 3 * len(b.nx) * ng * 8
     return {"value": steps / sum(times), "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "steps": 1,
-            "path": "host-pointer C ABI per phase (slg_interior_source .. slg_fluxtally), all models"}
+            "path": "host-pointer C ABI per phase (slg_interior_source .. slg_fluxtally), all models; "
+                    "first step of a fresh context (device buffers allocated inside the timed step)"}
 
 
 def batched_cpu_baseline(a, b, params, budget_s=20.0):
@@ -536,7 +544,7 @@ def batched_cpu_baseline(a, b, params, budget_s=20.0):
     dt = 0.0
     used = []
     for m in range(len(b.nx)):
-        g = W.Grid(int(b.nx[m]), 0.0, b.xarr[eo[m]:eo[m + 1] + 1], b.vxarr[eo[m]:eo[m + 1] + 1],
+        g = W.Grid(int(b.nx[m]), 0.0, b.xarr[eo[m]:eo[m + 1]], b.vxarr[eo[m]:eo[m + 1]],
                    b.vol[co[m]:co[m + 1]], b.divv[co[m]:co[m + 1]])
         T, rho = b.temp[co[m]:co[m + 1]], b.rho[co[m]:co[m + 1]]
         sig, cap = po.analytic_opacity(b.groups.wlinv, T, rho, kind=1)
@@ -644,6 +652,8 @@ def run_reference(a):
 
 def main():
     a = parse()
+    if a.steps is None:
+        a.steps = 1 if a.workload == "batched" else 3
     if a.impl == "reference":
         if a.workload == "batched":
             run_reference_batched(a)

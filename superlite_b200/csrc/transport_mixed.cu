@@ -34,6 +34,15 @@ constexpr float cinvf = (float)cinv;
 constexpr float pc_cf = (float)pc_c;
 constexpr float dextf = (float)pc_dext;
 
+// One Philox4x32-10 block, kept out of line: draw() is called from about
+// twenty places of the event code, and one shared copy of the rounds keeps
+// the loop small enough for the instruction cache (measured: with the copies
+// inlined, "no instruction" was the largest warp stall).
+__device__ __noinline__ u32x4 philox_block(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                           uint32_t k1) {
+  return philox4x32_10(u32x4{c0, c1, c2, c3}, k0, k1);
+}
+
 // four 23-bit uniforms per Philox call: (m + 1/2) 2^-23, in (0,1)
 struct PhiloxStream32 {
   uint32_t k0, k1, pid_lo, pid_hi, stream;
@@ -48,7 +57,7 @@ struct PhiloxStream32 {
   __device__ inline float draw() {
     const uint32_t j = k & 3u;
     if (j == 0u) {
-      const u32x4 o = philox4x32_10(u32x4{k >> 2, pid_lo, pid_hi, stream}, k0, k1);
+      const u32x4 o = philox_block(k >> 2, pid_lo, pid_hi, stream, k0, k1);
       w[0] = o.a; w[1] = o.b; w[2] = o.c; w[3] = o.d;
     }
     ++k;
@@ -111,11 +120,16 @@ __device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& 
   const double x = p.x, mud = (double)mu;
   double dbd;
   int ixnext;
+  // The radicands are >= 0 in exact arithmetic (x <= Xb; the inner branch is
+  // taken only when the chord meets the inner shell).  This unit contracts to
+  // FMA, and Xb*Xb - round(x*x) with x == Xb is the (signed) rounding error of
+  // the square: a particle on its outer edge with |mu| < ~1e-8 would get a
+  // NaN distance, so the radicands are clamped at 0.
   if (ix == 1 || mud >= -sqrt(1.0 - sq(Xa / x))) {
-    dbd = fabs(sqrt(sq(Xb) - (1.0 - sq(mud)) * sq(x)) - mud * x);
+    dbd = fabs(sqrt(fmax(sq(Xb) - (1.0 - sq(mud)) * sq(x), 0.0)) - mud * x);
     ixnext = ix + 1;
   } else {
-    dbd = fabs(sqrt(sq(Xa) - (1.0 - sq(mud)) * sq(x)) + mud * x);
+    dbd = fabs(sqrt(fmax(sq(Xa) - (1.0 - sq(mud)) * sq(x), 0.0)) + mud * x);
     ixnext = ix - 1;
   }
   if (dbd != dbd) { ierr = 1; return; }
@@ -144,8 +158,13 @@ __device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& 
   // event kind with the reference's precedence (transport11.f90:256-489)
   const bool is_thm = d == dthm, is_col = !is_thm && d == dcol;
   const bool is_b = !is_thm && !is_col && d == db;
-  const double dd = is_b ? dbd : (double)d;
-  const double xnew = sqrt(sq(x) + sq(dd) + 2.0 * dd * x * mud);
+  // An FP32 event distance may round past the FP64 boundary distance (d <=
+  // (float)dbd but d > dbd); the event then happens on the shell edge, and
+  // the FP64 position stays inside [Xa, Xb] so that the next boundary
+  // distance is defined (a position past Xb with |mu| small gives a NaN).
+  const double dd = is_b ? dbd : fmin((double)d, dbd);
+  double xnew = sqrt(fmax(sq(x) + sq(dd) + 2.0 * dd * x * mud, 0.0));  // (x + dd mu)^2 + dd^2 (1 - mu^2)
+  if (!is_b) xnew = fmin(fmax(xnew, Xa), Xb);
   p.x = xnew;
   vx = (float)((VX[ix - 1] * (Xb - xnew) + VX[ix] * (xnew - Xa)) / (Xb - Xa));
   mu = xnew == 0.0 ? 1.0f : fminf(fmaxf((float)((x * mud + dd) / xnew), -1.0f), 1.0f);
@@ -467,12 +486,14 @@ __global__ void __launch_bounds__(MIX_BLOCK, MINB) particle_advance_mixed_kernel
   __syncthreads();
   double* const tally = A.smem_cells ? s_tally : A.tally;
   const int lane = threadIdx.x & 31;
-  double evelo = 0.0, eout = 0.0, sflux = 0.0;
-  unsigned long long nimc = 0, nddmc = 0, nswap = 0, npckt = 0, nflux = 0, nwarn = 0, nmax = 0;
+  // counters are kept per particle in 32 bits (DDMC steps, method swaps; the
+  // IMC steps are istep - nd_p) and added to the block's shared counters when
+  // the particle ends, so few registers carry them through the loop
+  double evelo = 0.0;
+  unsigned nd_p = 0, nsw_p = 0;
   long long ip = -1;
   bool have = false, queue_done = false;
   PtclM p;
-  double y = 0, z = 0, om = 0;
   PhiloxStream32 rng;
   // replays of a captured graph draw from counter word 3 = 2 | replay << 2
   const uint32_t sw = 2u | (A.epoch ? (uint32_t)(*A.epoch << 2) : 0u);
@@ -498,10 +519,9 @@ __global__ void __launch_bounds__(MIX_BLOCK, MINB) particle_advance_mixed_kernel
         } else if (!A.isvacant[cand]) {
           ip = cand;
           const double2* q = reinterpret_cast<const double2*>(A.prt + ip);
-          const double2 a = q[0], b = q[1], c = q[2], d = q[3];
-          double x = a.x, mu = b.y, e = c.y, e0 = d.x, wl = d.y;
-          y = a.y; z = b.x; om = c.x;
-          npckt++;
+          const double2 b = q[1], c = q[2], d = q[3];
+          double x = A.prt[ip].x, mu = b.y, e = c.y, e0 = d.x, wl = d.y;
+          atomicAdd(&s_cnt[0], 1ull);
           // the slot's model (models own consecutive slot ranges)
           int m = 0;
           long long poff = 0;
@@ -538,6 +558,8 @@ __global__ void __launch_bounds__(MIX_BLOCK, MINB) particle_advance_mixed_kernel
             p.x = x; p.e = e; p.e0 = e0; p.mu = (float)mu; p.wl = (float)wl; p.vx = (float)vx;
             p.ix = ix; p.ig = ig; p.stat = 0; p.idist = 0;
             istep = 0;
+            nd_p = 0;
+            nsw_p = 0;
             rng.init(A.seed + (unsigned long long)m * kModelSeedStride, (uint64_t)(ip - poff), sw);
             have = true;
           }
@@ -552,21 +574,25 @@ __global__ void __launch_bounds__(MIX_BLOCK, MINB) particle_advance_mixed_kernel
     double eraddens;
     int ierr;
     if (p.itype == 1 || A.puretran) {
-      nimc++;
       transport11_mix(A, v, p, rng, eraddens, evelo, ierr);
       if (p.itype != 1) {
-        nswap++;
+        nsw_p++;
         if (A.dogrdtally) atomicAdd(&A.methodswap[icold - 1], 1);
       }
     } else {
-      nddmc++;
+      nd_p++;
       diffusion11_mix(A, v, p, rng, eraddens, evelo, ierr);
       if (p.itype == 1) {
-        nswap++;
+        nsw_p++;
         if (A.dogrdtally) atomicAdd(&A.methodswap[icold - 1], 1);
       }
     }
-    atomicAdd(&s_cnt[9 + (p.idist > -3 ? p.idist : -3) + 3], 1ull);
+    {
+      // ndist histogram: one shared-memory add per distinct bin in the warp
+      const int di = 9 + (p.idist > -3 ? p.idist : -3) + 3;
+      const unsigned grp = __match_any_sync(__activemask(), di);
+      if (lane == __ffs(grp) - 1) atomicAdd(&s_cnt[di], (unsigned long long)__popc(grp));
+    }
     if (icold != t_ic) {
       if (t_ic > 0) atomicAdd(&tally[t_ic - 1], t_acc - t_c);
       t_ic = icold;
@@ -587,25 +613,29 @@ __global__ void __launch_bounds__(MIX_BLOCK, MINB) particle_advance_mixed_kernel
         if (ierr == 0) ierr = -99;
       }
     }
-    if (ierr == -99) nwarn++;
+    if (ierr == -99) atomicAdd(&s_cnt[6], 1ull);
     if (ierr == 0 && A.max_steps > 0 && istep >= A.max_steps && p.stat == 0) ierr = 1001;
     if (ierr > 0) {
       if (A.errorfatal) atomicMin(&A.acc->ierr_key, ((unsigned long long)(ip + 1) << 32) | (unsigned)ierr);
       p.stat = 2;
     }
     if (p.stat != 0) {
-      if ((unsigned long long)istep > nmax) nmax = istep;
+      atomicMax(&s_cnt[5], (unsigned long long)istep);
+      atomicAdd(&s_cnt[2], (unsigned long long)(istep - nd_p));
+      atomicAdd(&s_cnt[3], (unsigned long long)nd_p);
+      if (nsw_p) atomicAdd(&s_cnt[4], (unsigned long long)nsw_p);
       if (p.stat == 2) {
         A.isvacant[ip] = 1;
       } else {
-        nflux++;
-        sflux = sflux - p.e;
-        eout = eout + p.e;
-        double2* q = reinterpret_cast<double2*>(A.prt + ip);
-        q[0] = make_double2(DBL_MAX, y);
-        q[1] = make_double2(z, (double)p.mu);
-        q[2] = make_double2(om, p.e);
-        q[3] = make_double2(p.e0, (double)p.wl);
+        atomicAdd(&s_cnt[1], 1ull);
+        atomicAdd(&s_sum[1], p.e);   // tot_eout
+        atomicAdd(&s_sum[2], -p.e);  // tot_sflux
+        // y, z and om are never changed in the slot
+        slg_packet* q = A.prt + ip;
+        q->x = DBL_MAX;
+        q->mu = (double)p.mu;
+        q->e = p.e;
+        reinterpret_cast<double2*>(q)[3] = make_double2(p.e0, (double)p.wl);
       }
       have = false;
     }
@@ -613,15 +643,6 @@ __global__ void __launch_bounds__(MIX_BLOCK, MINB) particle_advance_mixed_kernel
   if (t_ic > 0) atomicAdd(&tally[t_ic - 1], t_acc - t_c);
   if (j_ic > 0) atomicAdd(&A.jrad[(size_t)(j_ic - 1) * A.ng + (j_ig - 1)], pc_c * (j_acc - j_c));
   atomicAdd(&s_sum[0], evelo);
-  atomicAdd(&s_sum[1], eout);
-  atomicAdd(&s_sum[2], sflux);
-  atomicAdd(&s_cnt[0], npckt);
-  atomicAdd(&s_cnt[1], nflux);
-  atomicAdd(&s_cnt[2], nimc);
-  atomicAdd(&s_cnt[3], nddmc);
-  atomicAdd(&s_cnt[4], nswap);
-  atomicMax(&s_cnt[5], nmax);
-  atomicAdd(&s_cnt[6], nwarn);
   __syncthreads();
   if (threadIdx.x == 0) {
     atomicAdd(&A.acc->evelo, s_sum[0]);
