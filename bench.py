@@ -63,6 +63,9 @@ def parse():
                          "timestep: one 256-shell model on physical opacities")
     ap.add_argument("--nmodel", type=int, default=128)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 per-model comparison")
+    ap.add_argument("--no-opacity", action="store_true", help="skip the opacity forward/adjoint measurement")
+    ap.add_argument("--npart-scale", type=float, default=1.0,
+                    help="scale the models' particle budgets (small cases for profilers; default 1)")
     return ap.parse_args()
 
 
@@ -397,6 +400,9 @@ def run_batched(a):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     b = W.analytic_batch(nmodel=a.nmodel, seed=SEED_BATCH + 1000 * rank)
+    if a.npart_scale != 1.0:
+        b = W.analytic_batch(nmodel=a.nmodel, seed=SEED_BATCH + 1000 * rank,
+                             npart=np.maximum(1000, (b.npart * a.npart_scale).astype(np.int64)))
     params = W.TransportParams()
     hot = HotPath(local)
     ts = BatchTimestep(hot, b, params, precision=1)
@@ -482,6 +488,9 @@ def run_batched(a):
         res["mixed_batched_over_fp64_plain"] = value / rate
     if not a.no_e2e:
         res["e2e"] = batched_e2e(a, b, params, local, seed0)
+    if not a.no_opacity:
+        res["opacity"] = opacity_measure(local)
+        res["opacity_cell_group_evals_per_s"] = res["opacity"]["forward"]["cell_group_evals_per_s"]
     if rank == 0 and world == 1 and not a.no_cpu:
         res["cpu_baseline"] = batched_cpu_baseline(a, b, params)
     hot.close()
@@ -566,6 +575,74 @@ def batched_cpu_baseline(a, b, params, budget_s=20.0):
     return {"value": steps / dt, "unit": "particle-steps/s", "cores": cores, "kind": "port",
             "sample": f"{len(used)} of {len(b.nx)} models, {used[0][1]} particles each (mzran, OpenMP static,1, "
                       f"FP64 oracle), transport only"}
+
+
+# ------------------------------------------------------------------ opacity forward / adjoint
+def opacity_measure(local, reps=5):
+    """Opacity build of configs[1] (256 shells x 2000 groups x 5e5 lines,
+    Saha populations, FP64) forward and reverse through the device C ABI
+    (slg_dev_opacity_grad_forward / _backward): cell-group evaluations per
+    second of each, timed with CUDA events on the library's stream."""
+    import torch
+    from superlite_b200 import HotPath, workloads as W
+    from superlite_b200.capi import ptr
+    case = W.opacity_case(ncell=256, ng=2000, nline=500_000, seed=SEED_CASE, t_days=T_DAYS)
+    hot = HotPath(local)
+    hot.set_groups(case.groups.wl)
+    hot.set_grid(case.grid.xarr, case.grid.vxarr, case.grid.vol, case.grid.divv)
+    g = case.gas
+    hot.set_atomic_data(g.ion_ni, g.oc.shape[1], case.lines, case.bf_ph1, case.bf_ph2, case.ff_gff)
+    hot.set_ions(W.ion_table(), float(g.temp[0]))
+    m = np.ascontiguousarray([W.ELEM_MASS.get(z, 2.0 * z) for z in range(1, W.NELEM + 1)], dtype=np.float64)
+    hot._check(hot.lib.slg_set_element_masses(hot.h, len(m), ptr(m)))
+    dev = torch.device("cuda", local)
+    nc, ng = hot.nx, hot.ng
+    f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)
+    T, R, X = f64(g.temp), f64(g.rho), f64(g.massfr)
+    e = lambda *sh: torch.empty(sh, dtype=torch.float64, device=dev)
+    nelec = torch.ones(nc, dtype=torch.float64, device=dev)
+    cap, sig, grey, ross, ol = e(nc, ng), e(nc), e(nc), e(nc), e(nc, 11)
+    gen = torch.Generator(device=dev).manual_seed(5)
+    gcap = torch.randn((nc, ng), generator=gen, device=dev, dtype=torch.float64)
+    gsig, ggrey, gross = (torch.randn(nc, generator=gen, device=dev, dtype=torch.float64) for _ in range(3))
+    gol = torch.randn((nc, 11), generator=gen, device=dev, dtype=torch.float64)
+    gT, gR, gX = e(nc), e(nc), torch.empty_like(X)
+    torch.cuda.synchronize()
+    L, h = hot.lib, hot.h
+    acc, taud, taul = 1e-14, 5.0, 10.0
+
+    def fwd():
+        nelec.fill_(1.0)
+        hot._check(L.slg_dev_opacity_grad_forward(h, ptr(T), ptr(R), ptr(X), acc, taud, taul, ptr(nelec), ptr(cap),
+                                                  ptr(sig), ptr(grey), ptr(ross), ptr(ol)))
+
+    def bwd():
+        hot._check(L.slg_dev_opacity_grad_backward(h, ptr(T), ptr(R), ptr(X), acc, taud, taul, ptr(nelec), ptr(cap),
+                                                   ptr(sig), ptr(grey), ptr(ross), ptr(ol), ptr(gcap), ptr(gsig),
+                                                   ptr(ggrey), ptr(gross), ptr(gol), ptr(gT), ptr(gR), ptr(gX)))
+    stream = torch.cuda.ExternalStream(hot.stream(), device=dev)
+    out = {}
+    for name, f in (("forward", fwd), ("backward", bwd)):
+        for _ in range(3):
+            f()
+        hot.sync()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        for _ in range(reps):
+            f()
+        ev[1].record(stream)
+        hot.sync()
+        ms = ev[0].elapsed_time(ev[1]) / reps
+        out[name] = {"ms": ms, "cell_group_evals_per_s": nc * ng / (ms / 1e3)}
+    hot.close()
+    lines_bytes = 16 * len(case.lines)
+    out["workload"] = "configs[1]: 256 shells x 2000 groups x 5e5 lines, Saha populations, FP64 (forward: EOS + " \
+                      "bb/bf/ff + means + leakage; backward: adjoint of all of it)"
+    out["bound"] = "FP64 issue (one exp per line-shell term), not HBM: the algorithmic bytes " \
+                   f"({(lines_bytes + 8 * nc * ng * 3) / 1e6:.0f} MB: lines, cap64, dL/dcap) take " \
+                   f"{(lines_bytes + 8 * nc * ng * 3) / (measured_peaks()[0] * 1e9) * 1e3:.4f} ms at the measured " \
+                   "HBM copy bandwidth"
+    return out
 
 
 # ------------------------------------------------------------------ reference arm

@@ -64,6 +64,14 @@ def test_mixed_matches_fp64_statistically(hot, oracle, t_days, kind):
     assert abs(_welch(steps[0], steps[1])) < 4.0, (steps[0], steps[1])
     assert abs(_welch(dep[0], dep[1])) < 4.0, (dep[0], dep[1])
     assert abs(_welch(esc[0], esc[1])) < 4.0, (esc[0], esc[1])
+    # deposition per shell, in 8 contiguous shell bins (each with enough events)
+    nx = c["grid"].nx
+    edges = np.linspace(0, nx, 9).astype(int)
+    for a, b in zip(edges[:-1], edges[1:]):
+        d0 = [r["tally"][a:b].sum() for r, _, _ in runs[0]]
+        d1 = [r["tally"][a:b].sum() for r, _, _ in runs[1]]
+        if max(d0 + d1) > 0:
+            assert abs(_welch(d0, d1)) < 4.0, (a, b, d0, d1)
     # group luminosities, summed over the K runs, binned, with lumdev noise
     lum64 = sum(l for _, l, _ in runs[0]); dev64 = sum(d for _, _, d in runs[0])
     lum32 = sum(l for _, l, _ in runs[1]); dev32 = sum(d for _, _, d in runs[1])
