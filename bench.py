@@ -354,9 +354,10 @@ def fp64_per_model(b, ts, params, local, seed):
     """The plain FP64 form on the same models: one model per call, as the
     single-model C ABI is called by a driver that runs the models one after
     another (each model in its own context; every call completes before the
-    next).  One step; returns (particle-steps/s, steps, seconds)."""
+    next).  One step; returns (particle-steps/s, steps, seconds, variant)."""
     import torch
     from superlite_b200 import HotPath
+    from superlite_b200.capi import ptr
     hots = []
     co = np.concatenate([[0], np.cumsum(b.nx)])
     eo = co + np.arange(len(b.nx) + 1)
@@ -370,6 +371,20 @@ def fp64_per_model(b, ts, params, local, seed):
     ts.prepare(seed)
     ts.sync()
     sl = lambda t, m: t[co[m]:co[m + 1]]
+    # the FP64 kernel's variant: autotuned once (largest model, 1e6-particle
+    # sample) and used by every model's context
+    import ctypes as C
+    big = int(np.argmax(b.npart))
+    tin = HotPath.transport_in(sl(ts.tempinv, big), sl(ts.sig, big), sl(ts.capgrey, big), sl(ts.emitprob, big),
+                               sl(ts.opaclump, big), sl(ts.cap, big), params, 0)
+    best, ms = C.c_int32(0), (C.c_float * 4)()
+    hb = hots[big]
+    hb._check(hb.lib.slg_autotune_transport(hb.h, C.byref(tin), ptr(ts.prt[po[big]:po[big + 1]]),
+                                            ptr(ts.isv[po[big]:po[big + 1]]), int(b.npart[big]), seed,
+                                            1_000_000, C.byref(best), ms))
+    for h in hots:
+        h._check(h.lib.slg_set_transport_variant(h.h, int(best.value)))
+    hb.sync()
     outs = []
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -386,7 +401,7 @@ def fp64_per_model(b, ts, params, local, seed):
     ts.sync()
     for h in hots:
         h.close()
-    return steps / dt, int(steps), dt
+    return steps / dt, int(steps), dt, int(best.value)
 
 
 def run_batched(a):
@@ -481,8 +496,9 @@ def run_batched(a):
     # + 1 epoch counter per graph replay
     res["gpu_launches"] = (14 + int(len(b.nx))) * a.steps + 1
     if not a.no_fp64:
-        rate, st64, dt64 = fp64_per_model(b, ts, params, local, seed0 + 999)
+        rate, st64, dt64, var64 = fp64_per_model(b, ts, params, local, seed0 + 999)
         res["fp64_plain_per_model"] = {"value": rate, "unit": "particle-steps/s", "steps": st64, "seconds": dt64,
+                                       "variant": var64,
                                        "form": "FP64 particle loop, one call per model (own context), "
                                                "each completed before the next"}
         res["mixed_batched_over_fp64_plain"] = value / rate

@@ -298,7 +298,8 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
   const double tinv = A.tempinv[gc];
   const float divv = (float)A.divv[v.co + ix - 1];
   const float tau_l = (float)A.taulump, tau_d = (float)A.tauddmc;
-  const int glump = (capc * dist >= tau_l) ? A.T.nlump[gc] : 0;
+  const int nl = __ldg(&A.T.nlump[gc]);  // loaded with capc, not after it
+  const int glump = (capc * dist >= tau_l) ? nl : 0;
   if ((sigc + capc) * dist < tau_d) { ierr = 100; return; }
   float emitlump, caplump, doplump, o1, o2;
   if (glump > 0) {
@@ -681,12 +682,12 @@ int launch_mixed_one(int num_sms, long long npart, cudaStream_t st, const TrnArg
 }  // namespace
 
 // Variants: resident 128-thread blocks per SM requested from the compiler
-// (register budget 128 / 102 / 85 / 64 per thread).
+// (register budget 128 / 102 / 85 / 73 per thread).
 int launch_transport_mixed(int variant, int num_sms, long long npart, cudaStream_t st, const TrnArgs& A) {
   switch (variant) {
     case 1: return launch_mixed_one<5>(num_sms, npart, st, A);
     case 2: return launch_mixed_one<6>(num_sms, npart, st, A);
-    case 3: return launch_mixed_one<8>(num_sms, npart, st, A);
+    case 3: return launch_mixed_one<7>(num_sms, npart, st, A);
     default: return launch_mixed_one<4>(num_sms, npart, st, A);
   }
 }
