@@ -36,7 +36,21 @@ struct CellTables {
   int16_t* guide = nullptr;
   int nx = 0, ng = 0;
 };
-constexpr int kGuideM = 256;  // a power of two, so r * kGuideM and k / kGuideM are exact
+constexpr int kGuideM = 256;
+
+// Per-cell record of the mixed-precision particle loop: everything an event
+// reads about its shell except per-group values, in one 128-byte line
+// (instead of about ten lines of separate arrays).  Values are the same
+// roundings the event code made from the separate arrays.
+struct alignas(128) MixCell {
+  double xa, xb, vxa, vxb;  // shell edges and edge velocities
+  double x0;                // the model's inner edge
+  double capgreyinv, tinv;  // 1/capgrey, 1/T
+  int nlump, pad;
+  float dist, sig, emitlump, caplump, doplump, o1, o2, divv;  // o1, o2: opaclump(1:2) of the lumped groups
+  float far, dvdr, sigl, sigr, dxl, dxr, fa, fb;  // neighbours (0 at the model's ends); fa, fb = x^2 / dx3
+};
+static_assert(sizeof(MixCell) == 128, "MixCell is one 128-byte line");  // a power of two, so r * kGuideM and k / kGuideM are exact
 enum { SCAL_EMITLUMP = 0, SCAL_CAPLUMP, SCAL_DOPLUMP, SCAL_CAPGREYINV, SCAL_SPECLUMP, SCAL_FAR,
        SCAL_DX3, SCAL_DVDR, SCAL_N };
 

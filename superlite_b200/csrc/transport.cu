@@ -345,6 +345,67 @@ int launch_transport_variant(int v, bool trace, int num_sms, long long npart, cu
 constexpr int kSmemTallyCells = 4096;
 
 // Kernel arguments of one particle_advance over the context's grid and models.
+// MixCell records of every cell (over all models), after build_cell_tables.
+__global__ void mix_cell_kernel(int nc, const int4* __restrict__ cellmap, const double* __restrict__ xarr,
+                                const double* __restrict__ vxarr, const double* __restrict__ divv,
+                                const double* __restrict__ sig, const double* __restrict__ tempinv,
+                                const double* __restrict__ opaclump, const double* __restrict__ scal,
+                                const int32_t* __restrict__ nlump, MixCell* __restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  int i = c + 1, nx = nc, co = 0, m = 0;
+  if (cellmap) {
+    const int4 cm = cellmap[c];
+    i = cm.x;
+    nx = cm.y;
+    co = cm.z;
+    m = cm.w;
+  }
+  const double* X = xarr + co + m;
+  const double* VX = vxarr + co + m;
+  const double* sc = scal + (size_t)SCAL_N * c;
+  MixCell r;
+  r.xa = X[i - 1];
+  r.xb = X[i];
+  r.vxa = VX[i - 1];
+  r.vxb = VX[i];
+  r.x0 = X[0];
+  r.capgreyinv = sc[SCAL_CAPGREYINV];
+  r.tinv = tempinv[c];
+  r.nlump = nlump[c];
+  r.pad = 0;
+  r.dist = (float)(r.xb - r.xa);
+  r.sig = (float)sig[c];
+  r.emitlump = (float)sc[SCAL_EMITLUMP];
+  r.caplump = (float)sc[SCAL_CAPLUMP];
+  r.doplump = (float)sc[SCAL_DOPLUMP];
+  r.o1 = (float)opaclump[(size_t)11 * c];
+  r.o2 = (float)opaclump[(size_t)11 * c + 1];
+  r.divv = (float)divv[c];
+  r.far = (float)sc[SCAL_FAR];
+  r.dvdr = (float)sc[SCAL_DVDR];
+  r.sigl = i > 1 ? (float)sig[c - 1] : 0.f;
+  r.sigr = i < nx ? (float)sig[c + 1] : 0.f;
+  r.dxl = i > 1 ? (float)(r.xa - X[i - 2]) : 0.f;
+  r.dxr = i < nx ? (float)(X[i + 1] - r.xb) : 0.f;
+  r.fa = (float)(sq(r.xa) / sc[SCAL_DX3]);
+  r.fb = (float)(sq(r.xb) / sc[SCAL_DX3]);
+  out[c] = r;
+}
+
+// Builds the MixCell records for a mixed-precision launch (scratch slot 76).
+int build_mix_cells(slg_ctx* ctx, const slg_transport_in* in, TrnArgs& A) {
+  const int nc = ctx->nx;
+  auto* rec = (MixCell*)scratch(ctx, 76, sizeof(MixCell) * (size_t)nc);
+  if (!rec) return SLG_ERR_OOM;
+  mix_cell_kernel<<<(nc + 127) / 128, 128, 0, ctx->stream>>>(nc, ctx->nmodel > 1 ? ctx->d_cellmap : nullptr,
+                                                            ctx->d_xarr, ctx->d_vxarr, ctx->d_divv, in->sig,
+                                                            in->tempinv, in->opaclump, ctx->tables.scal,
+                                                            ctx->tables.nlump, rec);
+  A.mcell = rec;
+  return cuda_check(ctx, cudaGetLastError(), "mix_cell_kernel");
+}
+
 TrnArgs transport_args(slg_ctx* ctx, const slg_transport_in* in, slg_packet* prt, int32_t* isvacant,
                        long long npart, uint64_t seed, double* tally, double* jrad, double* eamp,
                        int32_t* methodswap) {
@@ -398,6 +459,7 @@ int launch_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packet
   if (in->precision == 1) {
     A.trace_hash = nullptr;  // the mixed form has no per-event trace
     A.trace_nstep = nullptr;
+    if ((rc = build_mix_cells(ctx, in, A))) return rc;
     rc = launch_transport_mixed(ctx->mix_variant, ctx->num_sms, npart, st, A);
   } else {
     rc = launch_transport_variant(ctx->trn_variant, d_trace_hash != nullptr, ctx->num_sms, npart, st, A);
@@ -521,8 +583,9 @@ int autotune_transport(slg_ctx* ctx, const slg_transport_in* in, const slg_packe
   double* eamp = (double*)scratch(ctx, 44, sizeof(double) * nx);
   int32_t* msw = (int32_t*)scratch(ctx, 45, sizeof(int32_t) * nx);
   if (!p || !v || !tally || !jrad || !eamp || !msw) return SLG_ERR_OOM;
-  const TrnArgs A = transport_args(ctx, in, p, v, n, seed, tally, jrad, eamp, msw);
+  TrnArgs A = transport_args(ctx, in, p, v, n, seed, tally, jrad, eamp, msw);
   const bool mixed = in->precision == 1;
+  if (mixed && (rc = build_mix_cells(ctx, in, A))) return rc;
   const int nvar = mixed ? kMixedVariants : kTransportVariants;
   cudaEvent_t e0, e1;
   if ((rc = cuda_check(ctx, cudaEventCreate(&e0), "event"))) return rc;

@@ -34,6 +34,7 @@ struct TrnArgs {
   int nmodel = 1;                             // models (read by the mixed-precision kernel)
   int smem_cells = 0;                         // tally cells kept in shared memory (mixed kernel; 0: global)
   const ModelDesc* models = nullptr;
+  const MixCell* mcell = nullptr;  // per-cell records (mixed-precision kernel)
 };
 
 struct Ptcl {

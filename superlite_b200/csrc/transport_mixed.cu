@@ -108,15 +108,13 @@ __device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& 
   float& vx = p.vx;
   const int ic = ix;
   const int gc = v.co + ic - 1;  // 0-based index of the cell over all models
-  const double* X = A.xarr + v.xo;
-  const double* VX = A.vxarr + v.xo;
+  const MixCell& R = A.mcell[gc];  // this shell's record (one line), read where needed
   ierr = 0;
   eraddens = 0.0;
   float elabfact = 1.0f - mu * vx * cinvf;
   const float elabfactold = elabfact;
-  const double* sc = A.T.scal + (size_t)SCAL_N * gc;
-  const float far = (float)sc[SCAL_FAR];
-  const double Xa = X[ix - 1], Xb = X[ix];
+  const float far = R.far;
+  const double Xa = R.xa, Xb = R.xb;
   const double x = p.x, mud = (double)mu;
   double dbd;
   int ixnext;
@@ -125,7 +123,9 @@ __device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& 
   // FMA, and Xb*Xb - round(x*x) with x == Xb is the (signed) rounding error of
   // the square: a particle on its outer edge with |mu| < ~1e-8 would get a
   // NaN distance, so the radicands are clamped at 0.
-  if (ix == 1 || mud >= -sqrt(1.0 - sq(Xa / x))) {
+  // outward unless the chord meets the inner shell: mu >= -sqrt(1 - (Xa/x)^2)
+  // (transport11.f90:95-103) without its FP64 division and square root
+  if (ix == 1 || mud >= 0.0 || sq(mud) * sq(x) <= sq(x) - sq(Xa)) {
     dbd = fabs(sqrt(fmax(sq(Xb) - (1.0 - sq(mud)) * sq(x), 0.0)) - mud * x);
     ixnext = ix + 1;
   } else {
@@ -134,16 +134,16 @@ __device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& 
   }
   if (dbd != dbd) { ierr = 1; return; }
   const float db = (float)dbd;
-  const float sigc = (float)A.sig[gc];
+  const float sigc = R.sig;
   float dthm, dcol, ddop;
-  if (sigc > 0.f) dthm = -__logf(rng.draw()) / (elabfact * sigc);
+  if (sigc > 0.f) dthm = __fdividef(-__logf(rng.draw()), elabfact * sigc);
   else dthm = far;
   const float capc = capf(A, ig, gc + 1);
   if (capc <= 0.f) dcol = far;
-  else dcol = -__logf(rng.draw()) / (elabfact * capc);
-  const float dvdr = (float)sc[SCAL_DVDR];
-  if (dvdr > 0.f && ig < A.ng) ddop = 3.0f * pc_cf / (float)A.divv[v.co + ix - 1] * (elabfact - wl * (float)A.wlinv[ig]);
-  else if (dvdr < 0.f && ig > 1) ddop = 3.0f * pc_cf / (float)A.divv[v.co + ix - 1] * (elabfact - wl * (float)A.wlinv[ig - 1]);
+  else dcol = __fdividef(-__logf(rng.draw()), elabfact * capc);
+  const float dvdr = R.dvdr;
+  if (dvdr > 0.f && ig < A.ng) ddop = 3.0f * pc_cf / R.divv * (elabfact - wl * (float)A.wlinv[ig]);
+  else if (dvdr < 0.f && ig > 1) ddop = 3.0f * pc_cf / R.divv * (elabfact - wl * (float)A.wlinv[ig - 1]);
   else ddop = far;
   if (ddop < 0.f) ddop = far;
   float d = dcol;
@@ -166,13 +166,14 @@ __device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& 
   double xnew = sqrt(fmax(sq(x) + sq(dd) + 2.0 * dd * x * mud, 0.0));  // (x + dd mu)^2 + dd^2 (1 - mu^2)
   if (!is_b) xnew = fmin(fmax(xnew, Xa), Xb);
   p.x = xnew;
-  vx = (float)((VX[ix - 1] * (Xb - xnew) + VX[ix] * (xnew - Xa)) / (Xb - Xa));
-  mu = xnew == 0.0 ? 1.0f : fminf(fmaxf((float)((x * mud + dd) / xnew), -1.0f), 1.0f);
+  // FP32 quotients of FP64-formed terms (no FP64 division on the event path)
+  vx = __fdividef((float)(R.vxa * (Xb - xnew) + R.vxb * (xnew - Xa)), R.dist);
+  mu = xnew == 0.0 ? 1.0f : fminf(fmaxf(__fdividef((float)(x * mud + dd), (float)xnew), -1.0f), 1.0f);
   eraddens = p.e * (double)(elabfact * elabfact) * dd * cinv;
   elabfact = 1.0f - mu * vx * cinvf;
-  if (xnew < X[0]) {
-    p.x = X[0];
-    vx = (float)VX[0];
+  if (xnew < R.x0) {
+    p.x = R.x0;
+    vx = (float)A.vxarr[v.xo];
     ix = 1;
     mu = 1.0f - rng.draw();
     return;
@@ -201,7 +202,7 @@ __device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& 
     p.e0 = p.e0 * help;
     if (A.ng != 1) {
       ig = emitgroup_dev(A, (double)rng.draw(), gc + 1);
-      if (((sigc + capf(A, ig, gc + 1)) * (float)(Xb - Xa) >= (float)A.tauddmc) && !A.puretran) p.itype = 2;
+      if (((sigc + capf(A, ig, gc + 1)) * R.dist >= (float)A.tauddmc) && !A.puretran) p.itype = 2;
     }
     if (p.itype == 2) {
       const double g = (double)(vx * mu * cinvf);
@@ -216,12 +217,12 @@ __device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& 
   } else if (is_b) {
     const bool out = ixnext > ix;
     const int l = out ? ix + 1 : ix - 1;
-    const float capl = capf(A, ig, v.co + l), sigl = (float)A.sig[v.co + l - 1];
-    const float dxl = (float)(X[l] - X[l - 1]);
+    const float capl = capf(A, ig, v.co + l), sigl = out ? R.sigr : R.sigl;
+    const float dxl = out ? R.dxr : R.dxl;
     const double edge = out ? Xb : Xa;
     if ((sigl + capl) * dxl < (float)A.tauddmc || A.puretran) {
       p.x = edge;
-      vx = (float)VX[out ? ix : ix - 1];
+      vx = (float)(out ? R.vxb : R.vxa);
       ix = l;
     } else {
       mu = aberrate(mu, -vx * cinvf);
@@ -241,7 +242,7 @@ __device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& 
         mu = out ? -m : m;
         mu = aberrate(mu, vx * cinvf);
         p.x = edge;
-        vx = (float)VX[out ? ix : ix - 1];
+        vx = (float)(out ? R.vxb : R.vxa);
       }
     }
   } else {  // Doppler shift
@@ -262,7 +263,7 @@ __device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& 
         wl = 1.0f / (r1 * (float)A.wlinv[0] + (1.0f - r1) * (float)A.wlinv[1]) * elabfact;
       }
     }
-    if (((sigc + capf(A, ig, gc + 1)) * (float)(Xb - Xa) >= (float)A.tauddmc) && !A.puretran) {
+    if (((sigc + capf(A, ig, gc + 1)) * R.dist >= (float)A.tauddmc) && !A.puretran) {
       p.itype = 2;
       totevelo = totevelo + p.e * (double)(vx * mu * cinvf);
       p.e = p.e * (double)elabfact;
@@ -284,33 +285,28 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
   float& vx = p.vx;
   const int ic = ix;
   const int gc = v.co + ic - 1;  // 0-based index of the cell over all models
-  const double* X = A.xarr + v.xo;
-  const double* VX = A.vxarr + v.xo;
+  const MixCell& R = A.mcell[gc];  // this shell's record (one line), read where needed
   ierr = 0;
   eraddens = 0.0;
-  const double Xa = X[ix - 1], Xb = X[ix];
-  const float dist = (float)(Xb - Xa);
+  const double Xa = R.xa, Xb = R.xb;
+  const float dist = R.dist;
   const size_t off = (size_t)gc * ng;
-  const double* sc = A.T.scal + (size_t)SCAL_N * gc;
-  const double dx3 = sc[SCAL_DX3];
-  const float sigc = (float)A.sig[gc];
+  const float sigc = R.sig;
   const float capc = capf(A, ig, gc + 1);
-  const double tinv = A.tempinv[gc];
-  const float divv = (float)A.divv[v.co + ix - 1];
+  const float divv = R.divv;
   const float tau_l = (float)A.taulump, tau_d = (float)A.tauddmc;
-  const int nl = __ldg(&A.T.nlump[gc]);  // loaded with capc, not after it
-  const int glump = (capc * dist >= tau_l) ? nl : 0;
+  const int glump = (capc * dist >= tau_l) ? R.nlump : 0;
   if ((sigc + capc) * dist < tau_d) { ierr = 100; return; }
   float emitlump, caplump, doplump, o1, o2;
   if (glump > 0) {
-    emitlump = (float)sc[SCAL_EMITLUMP];
-    caplump = (float)sc[SCAL_CAPLUMP];
-    doplump = (float)sc[SCAL_DOPLUMP];
-    const double* OL = A.opaclump + (size_t)11 * gc;
-    o1 = (float)OL[0];
-    o2 = (float)OL[1];
+    emitlump = R.emitlump;
+    caplump = R.caplump;
+    doplump = R.doplump;
+    o1 = R.o1;
+    o2 = R.o2;
   } else {
-    emitlump = (float)(specint0(tinv, A.wlinv, ig) * sc[SCAL_CAPGREYINV] * (double)capc);
+    const double tinv = R.tinv;
+    emitlump = (float)(specint0(tinv, A.wlinv, ig) * R.capgreyinv * (double)capc);
     caplump = capc;
     const double spec_ig = A.T.specarr[off + ig - 1];
     const double divvd = A.divv[v.co + ix - 1];
@@ -318,12 +314,12 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
     else if (ig != 1 && divv < 0.f) doplump = (float)(-dopspeccalc(tinv, A.wlinv, ig - 1) * divvd / (spec_ig * 3.0 * pc_c));
     else doplump = 0.f;
     // x^2 / (x_b^3 - x_a^3) per face, formed in FP64
-    const float fa = (float)(sq(Xa) / dx3), fb = (float)(sq(Xb) / dx3);
+    const float fa = R.fa, fb = R.fb;
     if (ix == 1) {
       o1 = 0.f;
     } else {
-      const float capl = capf(A, ig, v.co + ix - 1), sigl = (float)A.sig[v.co + ix - 2];
-      const float dxl = (float)(Xa - X[ix - 2]);
+      const float capl = capf(A, ig, v.co + ix - 1), sigl = R.sigl;
+      const float dxl = R.dxl;
       if ((capl + sigl) * dxl < tau_d) {
         const float ppl = 4.0f / (3.0f * (capc + sigc) * dist + 6.0f * dextf);
         o1 = 1.5f * ppl * fa;
@@ -335,8 +331,8 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
     float capl = 0.f, sigl = 0.f, dxl = 0.f;
     if (ix != v.nx) {
       capl = capf(A, ig, v.co + ix + 1);
-      sigl = (float)A.sig[v.co + ix];
-      dxl = (float)(X[ix + 1] - Xb);
+      sigl = R.sigr;
+      dxl = R.dxr;
       lhelp = (capl + sigl) * dxl < tau_d;
     }
     if (lhelp) {
@@ -350,7 +346,7 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
   const float s_dop = doplump, s_left = doplump + o1, s_leak = doplump + (o1 + o2);
   const float r_scat = glump == ng ? 0.0f : (1.0f - emitlump) * caplump;
   const float total = s_leak + r_scat;
-  const float ddmct = fabsf(__logf(rng.draw()) / total * cinvf);
+  const float ddmct = fabsf(__fdividef(__logf(rng.draw()), total) * cinvf);
   eraddens = p.e * (double)ddmct;
   const float u = rng.draw() * total;  // < total: r < 1 rounds below
   const int16_t* glumps = A.T.glumps + off;
@@ -379,7 +375,7 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
       x = x < Xb ? x : Xb;
       x = x > Xa ? x : Xa;
       p.x = x;
-      vx = (float)((VX[ix - 1] * (Xb - x) + VX[ix] * (x - Xa)) / (Xb - Xa));
+      vx = (float)((R.vxa * (Xb - x) + R.vxb * (x - Xa)) / (Xb - Xa));
       mu = aberrate(mu, vx * cinvf);
       const float f = 1.0f - vx * mu * cinvf;
       wl = wl * f;
@@ -399,8 +395,8 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
       if (glump != 0) ig = glumps[cdf_search(A.T, 2, gc, A.T.cdf_right + off, glump, (double)rng.draw())];
       const float r = rng.draw();
       wl = 1.0f / (r * (float)A.wlinv[ig] + (1.0f - r) * (float)A.wlinv[ig - 1]);
-      p.x = X[v.nx];
-      vx = (float)VX[v.nx];
+      p.x = Xb;  // ix == nx
+      vx = (float)R.vxb;
       mu = aberrate(mu, vx * cinvf);
       mu = mu < 1.0f ? mu : 1.0f;
       const double help = 1.0 / (double)(1.0f - mu * vx * cinvf);
@@ -414,13 +410,13 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
     iiig = glump == 0 ? ig
                       : glumps[cdf_search(A.T, right ? 2 : 1, gc, (right ? A.T.cdf_right : A.T.cdf_left) + off, glump,
                                           (double)rng.draw())];
-    const float dxl = (float)(right ? X[ix + 1] - Xb : Xa - X[ix - 2]);
-    if (((float)A.sig[v.co + l - 1] + capf(A, iiig, v.co + l)) * dxl < tau_d) {
+    const float dxl = right ? R.dxr : R.dxl;
+    if (((right ? R.sigr : R.sigl) + capf(A, iiig, v.co + l)) * dxl < tau_d) {
       p.itype = 1;
       const float r = rng.draw();
       wl = 1.0f / (r * (float)A.wlinv[iiig] + (1.0f - r) * (float)A.wlinv[iiig - 1]);
       p.x = right ? Xb : Xa;
-      vx = (float)VX[right ? ix : ix - 1];
+      vx = (float)(right ? R.vxb : R.vxa);
       const float a = rng.draw(), b = rng.draw();
       const float m = a > b ? a : b;
       mu = right ? m : -m;
@@ -454,7 +450,7 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
       x = x < Xb ? x : Xb;
       x = x > Xa ? x : Xa;
       p.x = x;
-      vx = (float)((VX[ix - 1] * (Xb - x) + VX[ix] * (x - Xa)) / (Xb - Xa));
+      vx = (float)((R.vxa * (Xb - x) + R.vxb * (x - Xa)) / (Xb - Xa));
       mu = aberrate(mu, vx * cinvf);
       const float f = 1.0f - vx * mu * cinvf;
       const double help = 1.0 / (double)f;
@@ -464,8 +460,8 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
       wl = wl * f;
     }
   }
-  if (p.x < X[0]) { p.stat = 2; return; }
-  const float dv = (float)A.divv[v.co + ix - 1];
+  if (p.x < R.x0) { p.stat = 2; return; }
+  const float dv = ix == ic ? divv : (float)A.divv[v.co + ix - 1];  // the shell after a leak
   const double decay = (double)__expf(-dv * ddmct * (1.0f / 3.0f));
   totevelo = totevelo + p.e * (1.0 - decay);
   p.e = p.e * decay;
