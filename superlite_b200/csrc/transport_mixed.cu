@@ -142,8 +142,8 @@ __device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& 
   if (capc <= 0.f) dcol = far;
   else dcol = __fdividef(-__logf(rng.draw()), elabfact * capc);
   const float dvdr = R.dvdr;
-  if (dvdr > 0.f && ig < A.ng) ddop = 3.0f * pc_cf / R.divv * (elabfact - wl * (float)A.wlinv[ig]);
-  else if (dvdr < 0.f && ig > 1) ddop = 3.0f * pc_cf / R.divv * (elabfact - wl * (float)A.wlinv[ig - 1]);
+  if (dvdr > 0.f && ig < A.ng) ddop = __fdividef(3.0f * pc_cf, R.divv) * (elabfact - wl * (float)A.wlinv[ig]);
+  else if (dvdr < 0.f && ig > 1) ddop = __fdividef(3.0f * pc_cf, R.divv) * (elabfact - wl * (float)A.wlinv[ig - 1]);
   else ddop = far;
   if (ddop < 0.f) ddop = far;
   float d = dcol;
@@ -188,15 +188,15 @@ __device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& 
   }
   if (is_thm) {
     const float f = 1.0f - mu * vx * cinvf;
-    wl = wl * f / elabfact;
-    help = (double)(elabfact / f);
+    wl = __fdividef(wl * f, elabfact);
+    help = (double)__fdividef(elabfact, f);
     totevelo = totevelo + p.e * (1.0 - help);
     p.e = p.e * help;
     p.e0 = p.e0 * help;
   } else if (is_col) {
     rng.draw();  // the reference's unused draw (transport11.f90:313)
     const float f = 1.0f - mu * vx * cinvf;
-    help = (double)(elabfact / f);
+    help = (double)__fdividef(elabfact, f);
     totevelo = totevelo + p.e * (1.0 - help);
     p.e = p.e * help;
     p.e0 = p.e0 * help;
@@ -227,14 +227,14 @@ __device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& 
     } else {
       mu = aberrate(mu, -vx * cinvf);
       float hp = (capl + sigl) * dxl;
-      hp = 4.0f / (3.0f * hp + 6.0f * dextf);
+      hp = __fdividef(4.0f, 3.0f * hp + 6.0f * dextf);
       const float r1 = rng.draw();
       if (r1 < hp * (1.0f + 1.5f * fabsf(mu))) {
         p.itype = 2;
         totevelo = totevelo + p.e * (1.0 - (double)elabfact);
         p.e = p.e * (double)elabfact;
         p.e0 = p.e0 * (double)elabfact;
-        wl = wl / elabfact;
+        wl = __fdividef(wl, elabfact);
         ix = l;
       } else {
         const float a = rng.draw(), b = rng.draw();
