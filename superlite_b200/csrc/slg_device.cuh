@@ -150,6 +150,13 @@ __device__ inline u32x4 philox4x32_10(u32x4 ctr, uint32_t k0, uint32_t k1) {
   }
   return ctr;
 }
+// The same rounds kept out of line for the event loops, which draw from
+// many places: one copy of the rounds instead of one per call site keeps the
+// loop within the instruction cache.  Same results as philox4x32_10.
+static __device__ __noinline__ u32x4 philox4x32_10_call(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                                        uint32_t k0, uint32_t k1) {
+  return philox4x32_10(u32x4{c0, c1, c2, c3}, k0, k1);
+}
 __device__ inline double u52_to_unit(uint32_t w0, uint32_t w1) {
   const uint64_t m = ((uint64_t)w0 << 20) | (w1 >> 12);
   return ((double)m + 0.5) * 0x1p-52;
@@ -169,7 +176,7 @@ struct PhiloxStream {
   __device__ inline double draw() {
     double r;
     if ((k & 1u) == 0u) {
-      const u32x4 o = philox4x32_10(u32x4{k >> 1, pid_lo, pid_hi, stream}, k0, k1);
+      const u32x4 o = philox4x32_10_call(k >> 1, pid_lo, pid_hi, stream, k0, k1);
       w2 = o.c; w3 = o.d;
       r = u52_to_unit(o.a, o.b);
     } else {

@@ -34,13 +34,13 @@ __device__ inline void load_packet(const slg_packet* p, double& x, double& y, do
   const double2 a = q[0], b = q[1], c = q[2], d = q[3];
   x = a.x; y = a.y; z = b.x; mu = b.y; om = c.x; e = c.y; e0 = d.x; wl = d.y;
 }
-__device__ inline void store_packet(slg_packet* p, double x, double y, double z, double mu, double om,
-                                    double e, double e0, double wl) {
-  double2* q = reinterpret_cast<double2*>(p);
-  q[0] = make_double2(x, y);
-  q[1] = make_double2(z, mu);
-  q[2] = make_double2(om, e);
-  q[3] = make_double2(e0, wl);
+// an escaped particle's slot: x = huge, and its lab-frame mu, e, e0, wl
+// (y, z and om are never changed in the slot)
+__device__ inline void store_flux_packet(slg_packet* p, double mu, double e, double e0, double wl) {
+  p->x = DBL_MAX;
+  p->mu = mu;
+  p->e = e;
+  reinterpret_cast<double2*>(p)[3] = make_double2(e0, wl);
 }
 
 // MINB = minimum resident blocks per SM requested from the register
@@ -55,13 +55,15 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
   if (threadIdx.x < 3) s_sum[threadIdx.x] = 0.0;
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  double evelo = 0.0, eout = 0.0, sflux = 0.0;
-  unsigned long long nimc = 0, nddmc = 0, nswap = 0, npckt = 0, nflux = 0, nwarn = 0, nmax = 0;
+  // counters are kept per particle in 32 bits (DDMC steps, method swaps; the
+  // IMC steps are istep - nd_p) and added to the block's shared counters when
+  // the particle ends, so few registers carry them through the loop
+  double evelo = 0.0;
+  unsigned nd_p = 0, nsw_p = 0;
   // current particle
   long long ip = -1;
   bool have = false;
   Ptcl p;
-  double y = 0, z = 0, om = 0;
   PhiloxStream rng;
   // replays of a captured graph draw from counter word 3 = stream | replay << 2
   const uint32_t sw = A.epoch ? (uint32_t)(*A.epoch << 2) : 0u;
@@ -95,9 +97,9 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
             have = false;  // vacant slot: nothing to do, take another next iteration
           } else {
             // ---- particle set-up, particle_advance.f90:141-202
-            double x, mu, e, e0, wl;
+            double x, y, z, mu, om, e, e0, wl;
             load_packet(A.prt + ip, x, y, z, mu, om, e, e0, wl);
-            npckt++;
+            atomicAdd(&s_cnt[0], 1ull);
             p.x = x; p.mu = mu; p.e = e; p.e0 = e0; p.wl = wl; p.dist = 0.0;
             p.ix = binsrch(x, A.xarr, A.nx + 1, false);
             p.ig = binsrch(wl, A.wl, A.ng + 1, false);
@@ -122,6 +124,8 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
             p.stat = 0;
             p.idist = 0;
             istep = 0;
+            nd_p = 0;
+            nsw_p = 0;
             rng.init(A.seed, (uint64_t)ip, sw);
             if (TRACE) h = 1469598103934665603ull;
             have = !bad;
@@ -137,24 +141,25 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
     double eraddens, jrad, eamp = 0.0;
     int ierr;
     if (p.itype == 1 || A.puretran) {
-      nimc++;
       transport11_dev(A, p, rng, eraddens, eamp, jrad, evelo, ierr);
       if (p.itype != 1) {
-        nswap++;
+        nsw_p++;
         if (A.dogrdtally) atomicAdd(&A.methodswap[icold - 1], 1);
       }
       if (!A.noampfact && eamp != 0.0) atomicAdd(&A.eamp[icold - 1], eamp);
     } else {
-      nddmc++;
+      nd_p++;
       diffusion11_dev(A, p, rng, eraddens, jrad, evelo, ierr);
       if (p.itype == 1) {
-        nswap++;
+        nsw_p++;
         if (A.dogrdtally) atomicAdd(&A.methodswap[icold - 1], 1);
       }
     }
     {
-      const int id = p.idist > -3 ? p.idist : -3;
-      atomicAdd(&s_cnt[9 + id + 3], 1ull);
+      // ndist histogram: one shared-memory add per distinct bin in the warp
+      const int di = 9 + (p.idist > -3 ? p.idist : -3) + 3;
+      const unsigned grp = __match_any_sync(__activemask(), di);
+      if (lane == __ffs(grp) - 1) atomicAdd(&s_cnt[di], (unsigned long long)__popc(grp));
     }
     if (icold != t_ic) {
       if (t_ic > 0 && t_acc != 0.0) atomicAdd(&A.tally[t_ic - 1], t_acc);
@@ -181,7 +186,7 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
         if (ierr == 0) ierr = -99;
       }
     }
-    if (ierr == -99) nwarn++;
+    if (ierr == -99) atomicAdd(&s_cnt[6], 1ull);
     if (ierr == 0 && A.max_steps > 0 && istep >= A.max_steps && p.stat == 0) ierr = 1001;
     if (ierr > 0) {
       if (A.errorfatal) {
@@ -192,7 +197,10 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
     }
     if (p.stat != 0) {
       // ---- particle end, particle_advance.f90:271-292
-      if ((unsigned long long)istep > nmax) nmax = istep;
+      atomicMax(&s_cnt[5], (unsigned long long)istep);
+      atomicAdd(&s_cnt[2], (unsigned long long)(istep - nd_p));
+      atomicAdd(&s_cnt[3], (unsigned long long)nd_p);
+      if (nsw_p) atomicAdd(&s_cnt[4], (unsigned long long)nsw_p);
       if (TRACE) {
         A.trace_hash[ip] = h;
         A.trace_nstep[ip] = istep;
@@ -200,10 +208,10 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
       if (p.stat == 2) {
         A.isvacant[ip] = 1;
       } else {
-        nflux++;
-        sflux = sflux - p.e;
-        eout = eout + p.e;
-        store_packet(A.prt + ip, DBL_MAX, y, z, p.mu, om, p.e, p.e0, p.wl);
+        atomicAdd(&s_cnt[1], 1ull);
+        atomicAdd(&s_sum[1], p.e);   // tot_eout
+        atomicAdd(&s_sum[2], -p.e);  // tot_sflux
+        store_flux_packet(A.prt + ip, p.mu, p.e, p.e0, p.wl);
       }
       have = false;
     }
@@ -212,15 +220,6 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
   if (t_ic > 0 && t_acc != 0.0) atomicAdd(&A.tally[t_ic - 1], t_acc);
   if (j_ic > 0 && j_acc != 0.0) atomicAdd(&A.jrad[(size_t)(j_ic - 1) * A.ng + (j_ig - 1)], j_acc);
   atomicAdd(&s_sum[0], evelo);
-  atomicAdd(&s_sum[1], eout);
-  atomicAdd(&s_sum[2], sflux);
-  atomicAdd(&s_cnt[0], npckt);
-  atomicAdd(&s_cnt[1], nflux);
-  atomicAdd(&s_cnt[2], nimc);
-  atomicAdd(&s_cnt[3], nddmc);
-  atomicAdd(&s_cnt[4], nswap);
-  atomicMax(&s_cnt[5], nmax);
-  atomicAdd(&s_cnt[6], nwarn);
   __syncthreads();
   if (threadIdx.x == 0) {
     atomicAdd(&A.acc->evelo, s_sum[0]);

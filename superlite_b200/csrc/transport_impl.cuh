@@ -395,7 +395,6 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
   const size_t off = (size_t)(ic - 1) * ng;
   const double* sc = A.T.scal + (size_t)SCAL_N * (ic - 1);
   const double dx3 = sc[SCAL_DX3];
-  const double speclump = sc[SCAL_SPECLUMP];
   const double capgreyinv = sc[SCAL_CAPGREYINV];
   const double sigc = A.sig[ic - 1];
   const double capc = CAPd(A, ig, ic);
