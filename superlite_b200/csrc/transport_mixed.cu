@@ -7,8 +7,8 @@
 //         (Kahan-compensated register sums flushed with FP64 atomics);
 //   FP32: free-flight distances, Doppler distance, direction cosine mu, fluid
 //         velocity, wavelength, DDMC event time and leak probabilities, with
-//         fast single-precision log/exp, and 24-bit random numbers (four per
-//         Philox4x32-10 call, stream 2 of the particle).
+//         fast single-precision log/exp, and 23-bit random numbers (one
+//         Philox4x32-10 block of four per event, stream 2 of the particle).
 // Cell factors whose magnitude leaves the FP32 range are formed in FP64 and
 // rounded once: shell volume factors (x_b^3 - x_a^3 reaches 1e43 cm^3 at a
 // few days, above FLT_MAX), Planck group fractions deep in the Wien tail,
@@ -43,25 +43,39 @@ __device__ __noinline__ u32x4 philox_block(uint32_t c0, uint32_t c1, uint32_t c2
   return philox4x32_10(u32x4{c0, c1, c2, c3}, k0, k1);
 }
 
-// four 23-bit uniforms per Philox call: (m + 1/2) 2^-23, in (0,1)
+// Per-particle stream of 23-bit uniforms, (m + 1/2) 2^-23 in (0,1).  Event n
+// of the particle draws from Philox blocks with counter word 0 = 4 n + b
+// (b = 0, 1, ... for its 1st-4th, 5th-8th ... draw), words 1-2 = the particle,
+// word 3 = the stream.  Block 0 of every event is made at the top of the
+// event loop, where the warp's lanes are converged: one Philox call per
+// iteration for the whole warp, instead of a call wherever some lane's buffer
+// ran out (with lanes out of step, that was every draw site, with a quarter
+// of the lanes active).
 struct PhiloxStream32 {
   uint32_t k0, k1, pid_lo, pid_hi, stream;
-  uint32_t k;
+  uint32_t ev, j;  // event number, draws taken in this event
   uint32_t w[4];
   __device__ inline void init(uint64_t seed, uint64_t pid, uint32_t s) {
     k0 = (uint32_t)seed; k1 = (uint32_t)(seed >> 32);
     pid_lo = (uint32_t)pid; pid_hi = (uint32_t)(pid >> 32);
     stream = s;
-    k = 0;
+    ev = 0;
+    j = 0;
+  }
+  __device__ inline void begin_event(uint32_t n) {
+    ev = n;
+    j = 0;
+    const u32x4 o = philox_block(n << 2, pid_lo, pid_hi, stream, k0, k1);
+    w[0] = o.a; w[1] = o.b; w[2] = o.c; w[3] = o.d;
   }
   __device__ inline float draw() {
-    const uint32_t j = k & 3u;
-    if (j == 0u) {
-      const u32x4 o = philox_block(k >> 2, pid_lo, pid_hi, stream, k0, k1);
+    const uint32_t i = j & 3u;
+    if (i == 0u && j != 0u) {  // a 5th, 9th ... draw in one event (rare)
+      const u32x4 o = philox_block((ev << 2) | (j >> 2), pid_lo, pid_hi, stream, k0, k1);
       w[0] = o.a; w[1] = o.b; w[2] = o.c; w[3] = o.d;
     }
-    ++k;
-    const uint32_t u = j == 0u ? w[0] : (j == 1u ? w[1] : (j == 2u ? w[2] : w[3]));
+    ++j;
+    const uint32_t u = i == 0u ? w[0] : (i == 1u ? w[1] : (i == 2u ? w[2] : w[3]));
     return ((float)(u >> 9) + 0.5f) * 0x1p-23f;
   }
 };
@@ -566,6 +580,7 @@ __global__ void __launch_bounds__(MIX_BLOCK, MINB) particle_advance_mixed_kernel
     if (__all_sync(0xffffffffu, !have && queue_done)) break;
     if (!have) continue;
     istep++;
+    rng.begin_event((uint32_t)istep);
     const MView v{vnx, vco, vxo};
     const int icold = v.co + p.ix, igold = p.ig;  // cell over all models, 1-based
     double eraddens;

@@ -46,12 +46,12 @@ def test_mixed_matches_fp64_statistically(hot, oracle, t_days, kind):
     """K independent seeds per form.  Steps per particle and the deposited energy
     have heavy-tailed per-particle distributions (a few per cent spread between
     seeds at 2e4 particles), so they are compared with the K-run batch variance
-    (Welch t, |t| < 4 at 2K-2 = 10 degrees of freedom); luminosities use the
+    (Welch t, |t| < 4 at 2K-2 = 18 degrees of freedom); luminosities use the
     fluxtally variance estimate lumdev."""
     c = cases.transport_case(oracle, t_days=t_days, npart=20000, kind=kind)
     hot.set_groups(c["groups"].wl)
     hot.set_grid(c["grid"].xarr, c["grid"].vxarr, c["grid"].vol, c["grid"].divv)
-    K = 6
+    K = 10
     runs = {0: [], 1: []}
     for prec in (0, 1):
         for k in range(K):
@@ -64,9 +64,11 @@ def test_mixed_matches_fp64_statistically(hot, oracle, t_days, kind):
     assert abs(_welch(steps[0], steps[1])) < 4.0, (steps[0], steps[1])
     assert abs(_welch(dep[0], dep[1])) < 4.0, (dep[0], dep[1])
     assert abs(_welch(esc[0], esc[1])) < 4.0, (esc[0], esc[1])
-    # deposition per shell, in 8 contiguous shell bins (each with enough events)
+    # deposition per shell, in 4 contiguous shell bins (each with enough events
+    # that the K-run means are near normal: the per-particle deposition is
+    # heavy-tailed in the optically thick cases)
     nx = c["grid"].nx
-    edges = np.linspace(0, nx, 9).astype(int)
+    edges = np.linspace(0, nx, 5).astype(int)
     for a, b in zip(edges[:-1], edges[1:]):
         d0 = [r["tally"][a:b].sum() for r, _, _ in runs[0]]
         d1 = [r["tally"][a:b].sum() for r, _, _ in runs[1]]
