@@ -360,7 +360,7 @@ __device__ inline TabArgs tab_view(TabArgs A, int c, int* ic) {
     A.cap += cg;
     A.T.specarr += cg; A.T.glumps += cg; A.T.cdf_dop += cg; A.T.cdf_left += cg; A.T.cdf_right += cg;
     A.T.cdf_scat += cg; A.T.emitcum += cg;
-    if (A.T.guide) A.T.guide += (size_t)co * 4 * (kGuideM + 1);
+    if (A.T.guide) A.T.guide += (size_t)co * 4 * (A.T.guide_m + 1);
     A.T.nlump += co;
     A.T.scal += (size_t)SCAL_N * co;
   }
@@ -559,19 +559,20 @@ __global__ void __launch_bounds__(GB) cell_tables_kernel(const TabArgs A0) {
   // ---- phase C: guide tables of the four running sums (see CellTables::guide)
   if (A.T.guide && nlump > 0) {
     __syncthreads();
-    int16_t* gd = A.T.guide + (size_t)(ic - 1) * 4 * (kGuideM + 1);
+    const int gm = A.T.guide_m;
+    int16_t* gd = A.T.guide + (size_t)(ic - 1) * 4 * (gm + 1);
     for (int t = 0; t < 4; ++t) {
       const double* a = t == 0 ? cdop : (t == 1 ? cleft : (t == 2 ? cright : cscat));
       const int n = t == 3 ? ng - nlump : nlump;
-      for (int k = threadIdx.x; k <= kGuideM; k += blockDim.x) {
-        const double v = (double)k * (1.0 / kGuideM);
+      for (int k = threadIdx.x; k <= gm; k += blockDim.x) {
+        const double v = (double)k / (double)gm;  // exact: gm is a power of two
         int lo = 0, hi = (t == 1 && ix == 1) ? 0 : n;  // no left leak from the first shell
         while (lo < hi) {
           const int mid = (lo + hi) >> 1;
           if (a[mid] <= v) lo = mid + 1;
           else hi = mid;
         }
-        gd[t * (kGuideM + 1) + k] = (int16_t)lo;
+        gd[t * (gm + 1) + k] = (int16_t)lo;
       }
     }
   }
@@ -633,7 +634,8 @@ int build_cell_tables(slg_ctx* ctx, const slg_transport_in* in) {
     T.nlump = (int32_t*)scratch(ctx, 19, sizeof(int32_t) * nx);
     T.scal = (double*)scratch(ctx, 20, sizeof(double) * SCAL_N * nx);
     // guide entries are int16 positions
-    T.guide = ng < 32768 ? (int16_t*)scratch(ctx, 72, sizeof(int16_t) * 4 * (kGuideM + 1) * (size_t)nx) : nullptr;
+    T.guide_m = guide_size(ng);
+    T.guide = ng < 32768 ? (int16_t*)scratch(ctx, 72, sizeof(int16_t) * 4 * (T.guide_m + 1) * (size_t)nx) : nullptr;
     if (!T.specarr || !T.glumps || !T.cdf_dop || !T.cdf_left || !T.cdf_right || !T.cdf_scat ||
         !T.emitcum || !T.nlump || !T.scal || (ng < 32768 && !T.guide)) {
       T.nx = T.ng = 0;

@@ -30,13 +30,25 @@ struct CellTables {
   int32_t* nlump = nullptr;
   double* scal = nullptr;     // 8 doubles per cell (see SCAL_*)
   // guide tables of the four running sums above (dop, left, right, scat):
-  // per cell and table kGuideM+1 entries, entry k = number of sums <= k/kGuideM,
-  // so a draw r in [k, k+1)/kGuideM is searched only between entries k and k+1
-  // (null: plain search over the whole table)
+  // per cell and table guide_m+1 entries, entry k = number of sums <= k/guide_m,
+  // so a draw r in [k, k+1)/guide_m is searched only between entries k and k+1
+  // (null: plain search over the whole table).  guide_m is a power of two
+  // (so r * guide_m and k / guide_m are exact) near ng/4: a range of a few
+  // entries, searched in one round of loads, without a guide larger than the
+  // tables it indexes.
   int16_t* guide = nullptr;
+  int guide_m = 0;
+  // FP32 copies of cdf_dop/left/right/scat for the mixed-precision loop (half
+  // the bytes per gather; null when only the FP64 loop runs)
+  float *cdf32_dop = nullptr, *cdf32_left = nullptr, *cdf32_right = nullptr, *cdf32_scat = nullptr;
   int nx = 0, ng = 0;
 };
-constexpr int kGuideM = 256;
+constexpr int kGuideMax = 256;
+inline int guide_size(int ng) {
+  int m = 16;
+  while (m < kGuideMax && 4 * m < ng) m *= 2;
+  return m;
+}
 
 // Per-cell record of the mixed-precision particle loop: everything an event
 // reads about its shell except per-group values, in one 128-byte line
@@ -50,7 +62,7 @@ struct alignas(128) MixCell {
   float dist, sig, emitlump, caplump, doplump, o1, o2, divv;  // o1, o2: opaclump(1:2) of the lumped groups
   float far, dvdr, sigl, sigr, dxl, dxr, fa, fb;  // neighbours (0 at the model's ends); fa, fb = x^2 / dx3
 };
-static_assert(sizeof(MixCell) == 128, "MixCell is one 128-byte line");  // a power of two, so r * kGuideM and k / kGuideM are exact
+static_assert(sizeof(MixCell) == 128, "MixCell is one 128-byte line");
 enum { SCAL_EMITLUMP = 0, SCAL_CAPLUMP, SCAL_DOPLUMP, SCAL_CAPGREYINV, SCAL_SPECLUMP, SCAL_FAR,
        SCAL_DX3, SCAL_DVDR, SCAL_N };
 

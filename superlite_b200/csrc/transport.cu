@@ -392,11 +392,39 @@ __global__ void mix_cell_kernel(int nc, const int4* __restrict__ cellmap, const 
   out[c] = r;
 }
 
-// Builds the MixCell records for a mixed-precision launch (scratch slot 76).
+// FP32 copies of the four running-sum tables (n entries each).
+__global__ void cdf32_kernel(size_t n, const double* __restrict__ a0, const double* __restrict__ a1,
+                             const double* __restrict__ a2, const double* __restrict__ a3, float* __restrict__ b0,
+                             float* __restrict__ b1, float* __restrict__ b2, float* __restrict__ b3) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    b0[i] = (float)a0[i];
+    b1[i] = (float)a1[i];
+    b2[i] = (float)a2[i];
+    b3[i] = (float)a3[i];
+  }
+}
+
+// Builds the MixCell records and the FP32 running sums for a mixed-precision
+// launch (scratch slots 76-80).
 int build_mix_cells(slg_ctx* ctx, const slg_transport_in* in, TrnArgs& A) {
   const int nc = ctx->nx;
   auto* rec = (MixCell*)scratch(ctx, 76, sizeof(MixCell) * (size_t)nc);
   if (!rec) return SLG_ERR_OOM;
+  const size_t n = (size_t)nc * ctx->ng;
+  float* c32[4];
+  for (int t = 0; t < 4; ++t) {
+    c32[t] = (float*)scratch(ctx, 77 + t, sizeof(float) * n);
+    if (!c32[t]) return SLG_ERR_OOM;
+  }
+  const CellTables& T = ctx->tables;
+  long long nb = (long long)((n + 255) / 256);
+  if (nb > 4LL * ctx->num_sms) nb = 4LL * ctx->num_sms;
+  cdf32_kernel<<<(unsigned)(nb > 0 ? nb : 1), 256, 0, ctx->stream>>>(n, T.cdf_dop, T.cdf_left, T.cdf_right, T.cdf_scat,
+                                                                    c32[0], c32[1], c32[2], c32[3]);
+  A.T.cdf32_dop = c32[0];
+  A.T.cdf32_left = c32[1];
+  A.T.cdf32_right = c32[2];
+  A.T.cdf32_scat = c32[3];
   mix_cell_kernel<<<(nc + 127) / 128, 128, 0, ctx->stream>>>(nc, ctx->nmodel > 1 ? ctx->d_cellmap : nullptr,
                                                             ctx->d_xarr, ctx->d_vxarr, ctx->d_divv, in->sig,
                                                             in->tempinv, in->opaclump, ctx->tables.scal,

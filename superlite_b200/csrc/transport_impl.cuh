@@ -76,13 +76,48 @@ __device__ inline int first_gt(const double* __restrict__ a, int n, double r) {
 
 // first_gt over running-sum table `table` (0 dop, 1 left, 2 right, 3 scat) of
 // cell `cell` (0-based over all models), narrowed by the cell's guide table:
-// the same answer, after one guide load and a search of about n/kGuideM entries.
+// the same answer, after one guide load and a search of about n/guide_m entries.
 __device__ inline int cdf_search(const CellTables& T, int table, int cell, const double* __restrict__ a, int n,
                                  double r) {
   if (!T.guide) return first_gt(a, n, r);
-  const int16_t* g = T.guide + ((size_t)cell * 4 + table) * (kGuideM + 1);
-  const int k = (int)(r * (double)kGuideM);  // exact: kGuideM is a power of two and r < 1
+  const int16_t* g = T.guide + ((size_t)cell * 4 + table) * (T.guide_m + 1);
+  const int k = (int)(r * (double)T.guide_m);  // exact: guide_m is a power of two and r < 1
   return first_gt_range(a, g[k], g[k + 1], n, r);
+}
+
+// FP32 forms of first_gt_range / cdf_search (mixed-precision loop): the
+// same guide narrows the search over the FP32 running sums.  Where rounding
+// to FP32 moves a sum across r the answer may differ from the FP64 search by
+// one position (the result stays within the guide's range).
+__device__ inline int first_gt_range32(const float* __restrict__ a, int lo, int hi, int n, float r) {
+  while (hi - lo > 8) {
+    const int step = (hi - lo) >> 3;
+    float v[7];
+#pragma unroll
+    for (int j = 0; j < 7; ++j) v[j] = __ldg(a + lo + (j + 1) * step);
+    int c = 0;
+#pragma unroll
+    for (int j = 0; j < 7; ++j) c += v[j] <= r;
+    const int nlo = c == 0 ? lo : lo + c * step + 1;
+    const int nhi = c == 7 ? hi : lo + (c + 1) * step;
+    lo = nlo;
+    hi = nhi;
+  }
+  float v[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) v[j] = lo + j < hi ? __ldg(a + lo + j) : 0.0f;
+  int c = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) c += (lo + j < hi) && v[j] <= r;
+  const int q = lo + c;
+  return q < n ? q : n - 1;
+}
+__device__ inline int cdf_search32(const CellTables& T, int table, int cell, const float* __restrict__ a, int n,
+                                   float r) {
+  if (!T.guide) return first_gt_range32(a, 0, n, n, r);
+  const int16_t* g = T.guide + ((size_t)cell * 4 + table) * (T.guide_m + 1);
+  const int k = (int)(r * (float)T.guide_m);  // exact: guide_m is a power of two and r < 1
+  return first_gt_range32(a, g[k], g[k + 1], n, r);
 }
 
 __device__ inline double CAPd(const TrnArgs& A, int ig, int ic) {

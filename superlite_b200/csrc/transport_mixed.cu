@@ -369,7 +369,7 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
     if (glump == 0) {
       iiig = ig;
     } else {
-      const int q = cdf_search(A.T, 0, gc, A.T.cdf_dop + off, glump, (double)rng.draw());
+      const int q = cdf_search32(A.T, 0, gc, A.T.cdf32_dop + off, glump, rng.draw());
       iiig = divv >= 0.f ? glumps[q] : glumps[glump - 1 - q];
     }
     if (divv >= 0.f) {
@@ -406,7 +406,7 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
       p.stat = 1;
       const float a = rng.draw(), b = rng.draw();
       mu = a > b ? a : b;
-      if (glump != 0) ig = glumps[cdf_search(A.T, 2, gc, A.T.cdf_right + off, glump, (double)rng.draw())];
+      if (glump != 0) ig = glumps[cdf_search32(A.T, 2, gc, A.T.cdf32_right + off, glump, rng.draw())];
       const float r = rng.draw();
       wl = 1.0f / (r * (float)A.wlinv[ig] + (1.0f - r) * (float)A.wlinv[ig - 1]);
       p.x = Xb;  // ix == nx
@@ -422,8 +422,8 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
     }
     const int l = right ? ix + 1 : ix - 1;
     iiig = glump == 0 ? ig
-                      : glumps[cdf_search(A.T, right ? 2 : 1, gc, (right ? A.T.cdf_right : A.T.cdf_left) + off, glump,
-                                          (double)rng.draw())];
+                      : glumps[cdf_search32(A.T, right ? 2 : 1, gc,
+                                            (right ? A.T.cdf32_right : A.T.cdf32_left) + off, glump, rng.draw())];
     const float dxl = right ? R.dxr : R.dxl;
     if (((right ? R.sigr : R.sigl) + capf(A, iiig, v.co + l)) * dxl < tau_d) {
       p.itype = 1;
@@ -450,7 +450,7 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
     if (glump == 0) {
       iiig = emitgroup_dev(A, (double)rng.draw(), gc + 1);
     } else {
-      const int q = cdf_search(A.T, 3, gc, A.T.cdf_scat + off, ng - glump, (double)rng.draw());
+      const int q = cdf_search32(A.T, 3, gc, A.T.cdf32_scat + off, ng - glump, rng.draw());
       iiig = glumps[ng - 1 - q];
     }
     ig = iiig;
