@@ -1,22 +1,28 @@
 """Benchmark of SuperLite's per-timestep hot path on B200.
 
-Workload (default): one full IMC/DDMC timestep on the physical opacities of
-256 shells x 2000 groups x 5e5 lines, 5e7 source particles, FP64 transport
-(particle_advance.f90 with transport11/diffusion11):
+Default workload (--workload batched): one timestep of 128 independent
+ejecta models (shells U{50..400}, particle budgets log-uniform in [1e5, 1e7],
+snapshot times log-uniform in 1-30 d, 100 groups, analytic grey opacity)
+in one context: sources, opacity, means, leakage, emission probabilities and
+the source tally, then ONE persistent mixed-precision particle loop over all
+models and per-model flux tallies, the timed steps captured in a CUDA graph.
+Beside it: the plain FP64 particle loop called once per model, the same step
+through the host-pointer C ABI (e2e), the opacity forward/adjoint of
+configs[1], and the oracle on the host cores.
 
-    source particles (GPU)  -> physical_opacity + Planck/Rosseland means
-    -> leakage_opacity11 + emission_probability -> sourcetally
-    -> particle_advance -> fluxtally
+--workload timestep: one full IMC/DDMC timestep on the physical opacities of
+256 shells x 2000 groups x 5e5 lines, 5e7 source particles
+(--precision fp64|mixed).
 
 metric: particle-steps/s = (IMC + DDMC events, particle_advance.f90:209,219)
-        / wall time of the whole timestep.  The opacity build is reported
-        beside it as cell-group evaluations per second.
+        / device time of the step(s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-N > 1 (torchrun): every rank runs its own independent particles on the same
-grid (weak scaling) and the grid/flux tallies are summed with one NCCL
-all-reduce, as the reference's reduce_gridtally / reduce_fluxtally do.
+N > 1 (torchrun): batched -- every rank runs its own batch of models (no
+exchange); timestep -- every rank runs its own particles on the same grid and
+the grid/flux tallies are summed with one NCCL all-reduce, as the reference's
+reduce_gridtally / reduce_fluxtally do.
 """
 from __future__ import annotations
 
@@ -39,7 +45,7 @@ METRIC = "particle-steps/s"
 T_DAYS = 10.0
 SEED_CASE = 2
 L_BOL = 1e42
-# SURVEY-defined algorithmic bytes of one particle-step (event-based SoA traffic)
+# algorithmic bytes of one particle-step: event-based SoA traffic, 2 x (5 x 8 + 4 x 4 + 8) B
 BYTES_PER_STEP = 128.0
 
 
