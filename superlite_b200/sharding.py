@@ -41,3 +41,28 @@ def reduce_counters(counters: dict, device, group=None) -> dict:
     out = {k: int(x) for k, x in zip(keys, v.tolist())}
     out["nstepmax"] = int(m.item())
     return out
+
+
+def shard_cells(ncell: int, rank: int, world: int):
+    """[lo, hi) shells whose opacity `rank` builds (the opacity of a shell
+    depends on that shell alone: physical_opacity.f:94-247)."""
+    return shard_range(ncell, rank, world)
+
+
+def gather_cells(local, ncell: int, group=None):
+    """All-gather per-shell rows: `local` holds this rank's shells
+    shard_cells(ncell, rank, world) along dim 0 (e.g. gas_cap (n, ng) FP32,
+    gas_sig / capgrey / capross (n,) FP64); returns the (ncell, ...) tensor on
+    every rank, in shell order (the exchange of mpimod_mpi.f:668-711 after a
+    cell-sharded opacity build).  Ranks' slices differ by at most one shell,
+    so each is padded to the largest before one all_gather."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    sizes = [shard_cells(ncell, r, world) for r in range(world)]
+    nmax = max(hi - lo for lo, hi in sizes)
+    pad = torch.zeros((nmax,) + tuple(local.shape[1:]), dtype=local.dtype, device=local.device)
+    pad[:local.shape[0]] = local
+    parts = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(parts, pad, group=group)
+    return torch.cat([p[:hi - lo] for p, (lo, hi) in zip(parts, sizes)], dim=0)

@@ -83,3 +83,54 @@ def test_shard_ranges_cover_all():
         assert rs[0][0] == 0 and rs[-1][1] == n
         assert all(rs[k][1] == rs[k + 1][0] for k in range(w - 1))
         assert max(b - a for a, b in rs) - min(b - a for a, b in rs) <= 1
+
+
+def _opacity_worker(rank, world, port, q):
+    import dataclasses
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for p in (root, os.path.join(root, "oracle"), os.path.join(root, "tests")):
+        sys.path.insert(0, p)
+    import torch
+    import torch.distributed as dist
+    import pyoracle as po
+    from superlite_b200 import sharding, workloads as W
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        case = W.opacity_case(ncell=37, ng=60, nline=3000, seed=13)
+        lo, hi = sharding.shard_cells(case.grid.nx, rank, world)
+        g, gr = case.gas, case.grid
+        sub_grid = dataclasses.replace(gr, nx=hi - lo, xarr=gr.xarr[lo:hi + 1], vxarr=gr.vxarr[lo:hi + 1],
+                                       vol=gr.vol[lo:hi], divv=gr.divv[lo:hi])
+        sub_gas = dataclasses.replace(g, temp=g.temp[lo:hi], mass=g.mass[lo:hi], rho=g.rho[lo:hi],
+                                      natom=g.natom[lo:hi], nelec=g.nelec[lo:hi], natomfr=g.natomfr[lo:hi],
+                                      massfr=g.massfr[lo:hi], oc=g.oc[:, :, lo:hi], ginv=g.ginv[:, :, lo:hi])
+        r = po.physical_opacity(dataclasses.replace(case, grid=sub_grid, gas=sub_gas))
+        got = [sharding.gather_cells(torch.tensor(r[k]), case.grid.nx) for k in ("cap", "sig", "cap64")]
+        if rank == 0:
+            q.put([t.numpy() for t in got])
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_cell_sharded_opacity_equals_single_process(oracle):
+    """Opacity sharded by shells (each rank builds its shells, then one
+    all-gather) equals the single-process build bit for bit: the opacity of a
+    shell depends on that shell alone."""
+    from superlite_b200 import workloads as W
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_opacity_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    ref = oracle.physical_opacity(W.opacity_case(ncell=37, ng=60, nline=3000, seed=13))
+    assert np.array_equal(got[0], ref["cap"])
+    assert np.array_equal(got[1], ref["sig"])
+    assert np.array_equal(got[2], ref["cap64"])
