@@ -501,7 +501,14 @@ def run_batched(a):
         "counters": {k: tot[k] for k in ("npckt", "nflux", "nstepimc", "nstepddmc", "nstepmax", "nmethodswap",
                                          "ierr")},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "frac": achieved / peak if achieved else None,
+                     # DRAM bytes of one launch: ncu dram__bytes_read.sum + dram__bytes_write.sum of this
+                     # kernel on the same batch with particle budgets x 0.1 (4.157e9 B for 2.944e7
+                     # particles: the packets read and written once, plus table and tally traffic),
+                     # scaled by the particles of this launch
+                     "traffic": 4.157e9 * float(b.npart.sum()) / 2.944e7,
+                     "traffic_basis": "ncu capture of particle_advance_mixed_kernel at 0.1x particle budgets "
+                                      "(4.16 GB), scaled by particles",
                      "kernel": "particle_advance_mixed_kernel",
                      "basis": f"{BYTES_PER_STEP:.0f} B per particle-step x steps of one step / particle_advance "
                               f"time of the last warm-up step; peak {peak_kind}"},
@@ -512,15 +519,29 @@ def run_batched(a):
     # + 1 (sourcetally) + 2 (cell tables, particle loop) + 1 (counter fold) + nmodel (flux tallies);
     # + 1 epoch counter per graph replay
     res["gpu_launches"] = (14 + int(len(b.nx))) * a.steps + 1
+    def whole_job(steps, seconds):
+        # every rank runs its own models: steps add up, the job takes the slowest rank's time
+        if world == 1:
+            return steps / seconds, steps, seconds
+        import torch.distributed as dist
+        t = torch.tensor([float(steps)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        m = torch.tensor([float(seconds)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        return float(t.item()) / float(m.item()), int(t.item()), float(m.item())
+
     if not a.no_fp64:
         rate, st64, dt64, var64 = fp64_per_model(b, ts, params, local, seed0 + 999)
+        rate, st64, dt64 = whole_job(st64, dt64)
         res["fp64_plain_per_model"] = {"value": rate, "unit": "particle-steps/s", "steps": st64, "seconds": dt64,
                                        "variant": var64,
                                        "form": "FP64 particle loop, one call per model (own context), "
                                                "each completed before the next"}
         res["mixed_batched_over_fp64_plain"] = value / rate
     if not a.no_e2e:
-        res["e2e"] = batched_e2e(a, b, params, local, seed0)
+        e = batched_e2e(a, b, params, local, seed0)
+        e["value"], e["particle_steps"], e["seconds"] = whole_job(e["particle_steps"], e["seconds"])
+        res["e2e"] = e
     if not a.no_opacity:
         res["opacity"] = opacity_measure(local)
         res["opacity_cell_group_evals_per_s"] = res["opacity"]["forward"]["cell_group_evals_per_s"]
@@ -567,7 +588,7 @@ def batched_e2e(a, b, params, local, seed0):
     h2d = 3 * P + nc * 8 * 12 + 3 * nc * ng * 4 + nc * hot.nep * 8
     d2h = 3 * P + nc * 8 * 20 + 2 * nc * ng * 4 + nc * ng * 8 + 3 * len(b.nx) * ng * 8
     return {"value": steps / sum(times), "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "steps": 1,
+            "d2h_bytes_per_step": int(d2h), "steps": 1, "particle_steps": int(steps), "seconds": sum(times),
             "path": "host-pointer C ABI per phase (slg_interior_source .. slg_fluxtally), all models; "
                     "particle arrays in pinned host memory; first step of a fresh context (device buffers "
                     "allocated inside the timed step)"}
