@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=0, help="particles in the CPU-baseline sample (0: auto)")
-    ap.add_argument("--workload", default="batched", choices=["batched", "timestep"],
+    ap.add_argument("--workload", default="batched", choices=["batched", "timestep", "opacity"],
                     help="batched: many models in one persistent launch, graph-captured steps; "
                          "timestep: one 256-shell model on physical opacities")
     ap.add_argument("--nmodel", type=int, default=128)
@@ -632,15 +632,20 @@ def batched_cpu_baseline(a, b, params, budget_s=20.0):
 
 
 # ------------------------------------------------------------------ opacity forward / adjoint
-def opacity_measure(local, reps=5):
-    """Opacity build of configs[1] (256 shells x 2000 groups x 5e5 lines,
-    Saha populations, FP64) forward and reverse through the device C ABI
+OPACITY_SIZES = {1: (256, 2000, 500_000), 4: (4096, 10000, 2_000_000)}
+
+
+def opacity_measure(local, reps=5, which=1):
+    """Opacity build of configs[1] (which=1: 256 shells x 2000 groups x 5e5
+    lines) or configs[4] (which=4: 4096 x 10000 x 2e6), Saha populations,
+    FP64, forward and reverse through the device C ABI
     (slg_dev_opacity_grad_forward / _backward): cell-group evaluations per
     second of each, timed with CUDA events on the library's stream."""
     import torch
     from superlite_b200 import HotPath, workloads as W
     from superlite_b200.capi import ptr
-    case = W.opacity_case(ncell=256, ng=2000, nline=500_000, seed=SEED_CASE, t_days=T_DAYS)
+    ncell, ngroup, nline = OPACITY_SIZES[which]
+    case = W.opacity_case(ncell=ncell, ng=ngroup, nline=nline, seed=SEED_CASE, t_days=T_DAYS)
     hot = HotPath(local)
     hot.set_groups(case.groups.wl)
     hot.set_grid(case.grid.xarr, case.grid.vxarr, case.grid.vol, case.grid.divv)
@@ -690,8 +695,9 @@ def opacity_measure(local, reps=5):
         out[name] = {"ms": ms, "cell_group_evals_per_s": nc * ng / (ms / 1e3)}
     hot.close()
     lines_bytes = 16 * len(case.lines)
-    out["workload"] = "configs[1]: 256 shells x 2000 groups x 5e5 lines, Saha populations, FP64 (forward: EOS + " \
-                      "bb/bf/ff + means + leakage; backward: adjoint of all of it)"
+    out["workload"] = f"configs[{which}]: {ncell} shells x {ngroup} groups x {nline:.0e} lines, Saha populations, " \
+                      "FP64 (forward: EOS + bb/bf/ff + means + leakage; backward: adjoint of all of it)"
+    out["line_shell_terms_per_s"] = {k: nline * ncell / (out[k]["ms"] / 1e3) for k in ("forward", "backward")}
     out["bound"] = "FP64 issue (one exp per line-shell term), not HBM: the algorithmic bytes " \
                    f"({(lines_bytes + 8 * nc * ng * 3) / 1e6:.0f} MB: lines, cap64, dL/dcap) take " \
                    f"{(lines_bytes + 8 * nc * ng * 3) / (measured_peaks()[0] * 1e9) * 1e3:.4f} ms at the measured " \
@@ -781,6 +787,22 @@ def run_reference(a):
     print(json.dumps(res))
 
 
+def run_opacity(a):
+    """--workload opacity: the differentiable opacity build at configs[4]
+    scale (4096 shells x 10000 groups x 2e6 lines), forward and adjoint."""
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    r = opacity_measure(local, reps=a.steps, which=4)
+    res = {"metric": "opacity cell-group evals/s", "value": r["backward"]["cell_group_evals_per_s"],
+           "unit": "cell-group evals/s", "n_gpus": 1, "steps": a.steps, "warmup": 3,
+           "ms_per_step": r["forward"]["ms"] + r["backward"]["ms"], "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, superlite_b200/workloads.py)",
+           "config": {"workload": r["workload"]}, "opacity": r, "gpu_launches": None}
+    if rank == 0:
+        print(json.dumps(res))
+
+
 def main():
     a = parse()
     if a.steps is None:
@@ -792,6 +814,8 @@ def main():
             run_reference(a)
     elif a.workload == "batched":
         run_batched(a)
+    elif a.workload == "opacity":
+        run_opacity(a)
     else:
         run_ours(a)
 
