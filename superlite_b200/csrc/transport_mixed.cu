@@ -45,8 +45,8 @@ __device__ __noinline__ u32x4 philox_block(uint32_t c0, uint32_t c1, uint32_t c2
 
 // Per-particle stream of 23-bit uniforms, (m + 1/2) 2^-23 in (0,1).  Event n
 // of the particle draws from Philox blocks with counter word 0 = 4 n + b
-// (b = 0, 1, ... for its 1st-4th, 5th-8th ... draw), words 1-2 = the particle,
-// word 3 = the stream.  Block 0 of every event is made at the top of the
+// (b = 0, 1, 2, 3 for its 1st-4th, 5th-8th ... draw: room for 16 draws; an
+// event here draws at most 7), words 1-2 = the particle, word 3 = the stream.  Block 0 of every event is made at the top of the
 // event loop, where the warp's lanes are converged: one Philox call per
 // iteration for the whole warp, instead of a call wherever some lane's buffer
 // ran out (with lanes out of step, that was every draw site, with a quarter
