@@ -116,3 +116,38 @@ def test_models_source_stays_in_model_slots():
     with pytest.raises(SlgError):
         hot.interior_source(b.gas.temp, emit, nvol, prt, isv, seed=1)
     hot.close()
+
+
+def test_models_edge_cases():
+    """Ragged batches: two- and three-shell models beside a 40-shell one, and a
+    call whose slots are all vacant (nothing to transport, zero counters)."""
+    params = W.TransportParams()
+    b = W.analytic_batch(nmodel=3, seed=11, nx=[2, 40, 3], npart=[1000, 3000, 500], t_range_days=(6.0, 12.0))
+    hot = HotPath(0)
+    hot.set_groups(b.groups.wl)
+    hot.set_models(b.nx, b.npart, b.xarr, b.vxarr, b.vol, b.divv)
+    sig, cap = hot.analytic_opacity(b.temp, b.rho, kind=1)
+    grey, _ = hot.opacity_means(b.temp, sig, cap)
+    tinv = 1.0 / b.temp
+    ol = hot.leakage_opacity(tinv, sig, cap)
+    ep = hot.emission_probability(tinv, cap, grey)
+    tab = dict(tempinv=tinv, sig=sig, capgrey=grey, emitprob=ep, opaclump=ol, cap=cap)
+    n = int(b.npart.sum())
+    prt = np.zeros(n, dtype=PACKET_DTYPE)
+    isv = np.ones(n, dtype=np.int32)
+    # all slots vacant: the loop has nothing to do
+    r0 = hot.particle_advance(tab, prt, isv, params, seed=1, precision=1)
+    assert r0["ierr"] == 0 and r0["npckt"] == 0 and r0["nstepimc"] + r0["nstepddmc"] == 0
+    # sources in every model, then one step over all three
+    emit, _ = hot.sourceenergy(b.temp, L_BOL)
+    nvol, nnew = hot.models_sourcenumbers(emit, b.npart)
+    assert nnew <= n
+    hot.interior_source(b.temp, emit, nvol, prt, isv, seed=2)
+    assert int((isv == 0).sum()) == nnew
+    r = hot.particle_advance(tab, prt, isv, params, seed=3, precision=1)
+    assert r["ierr"] == 0 and r["npckt"] == nnew
+    lum, dev, num = hot.fluxtally(prt, isv, b.groups.wl)
+    lum = np.asarray(lum).reshape(3, -1)
+    assert np.all(lum.sum(axis=1) > 0.0)
+    assert np.all(isv == 1)               # every particle escaped or was absorbed and freed
+    hot.close()
