@@ -272,8 +272,12 @@ def pinned_particles(n):
     pins its particle arrays would see."""
     import torch
     from superlite_b200.api import PACKET_DTYPE
-    raw = torch.zeros(n * PACKET_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
-    vac = torch.ones(n, dtype=torch.int32, pin_memory=True)
+    try:
+        raw = torch.zeros(n * PACKET_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
+        vac = torch.ones(n, dtype=torch.int32, pin_memory=True)
+    except RuntimeError:  # the host cannot page-lock this much (several ranks per node): pageable arrays
+        raw = torch.zeros(n * PACKET_DTYPE.itemsize, dtype=torch.uint8)
+        vac = torch.ones(n, dtype=torch.int32)
     return (raw, vac), raw.numpy().view(PACKET_DTYPE), vac.numpy()
 
 
