@@ -593,6 +593,7 @@ def batched_e2e(a, b, params, local, seed0):
     d2h = 3 * P + nc * 8 * 20 + 2 * nc * ng * 4 + nc * ng * 8 + 3 * len(b.nx) * ng * 8
     return {"value": steps / sum(times), "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h), "steps": 1, "particle_steps": int(steps), "seconds": sum(times),
+            "pinned": bool(keep[0].is_pinned()),
             "path": "host-pointer C ABI per phase (slg_interior_source .. slg_fluxtally), all models; "
                     "particle arrays in pinned host memory; first step of a fresh context (device buffers "
                     "allocated inside the timed step)"}
