@@ -253,6 +253,20 @@ class HotPath:
                                                       seed, C.byref(out)))
         return out
 
+    def autotune_transport(self, tables: dict, prt, isvacant, params, precision=0, seed=0, nsample=1_000_000):
+        """slg_autotune_transport on device tensors (torch CUDA): times every
+        variant of the particle loop of `precision` on a copy of the first
+        nsample particles and keeps the fastest for this context.  Returns
+        (variant, [ms per variant])."""
+        tin = self.transport_in(tables["tempinv"], tables["sig"], tables["capgrey"], tables["emitprob"],
+                                tables["opaclump"], tables["cap"], params, precision)
+        best = C.c_int32(0)
+        ms = (C.c_float * 4)()
+        npart = int(prt.shape[0])
+        self._check(self.lib.slg_autotune_transport(self.h, C.byref(tin), ptr(prt), ptr(isvacant), npart, int(seed),
+                                                    int(min(nsample, npart)), C.byref(best), ms))
+        return int(best.value), [float(m) for m in ms]
+
     def fluxtally(self, prt, isvacant, flx_wl):
         rows = getattr(self, "nmodel", 1)  # one row of groups per model
         if _is_torch(prt):

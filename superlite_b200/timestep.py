@@ -21,10 +21,6 @@ from . import capi
 from .api import HotPath, PACKET_DTYPE
 from .capi import ptr
 
-# libslg kernels queued by one DeviceTimestep step: opacity (bin lines, cell prep, bf table,
-# opacity, means, ...), leakage, emission probabilities, source tally, cell tables, particle
-# loop, counter fold, flux tally
-KERNELS_PER_STEP = 15
 
 
 class DeviceTimestep:

@@ -89,3 +89,23 @@ def test_graph_capture_rejects_changed_upload():
     _step(hot, ts, emit, nvol, 1)
     assert ts.sync()["ierr"] == 0
     hot.close()
+
+
+def test_autotuner_leaves_particles_and_picks_a_variant():
+    """slg_autotune_transport (HotPath.autotune_transport) times every variant on
+    a copy: the caller's particles and vacancy flags are unchanged."""
+    from superlite_b200.timestep import BatchTimestep
+    b = W.analytic_batch(nmodel=2, seed=4, nx=[20, 30], npart=[2000, 3000], t_range_days=(5.0, 10.0))
+    hot = HotPath(0)
+    params = W.TransportParams()
+    ts = BatchTimestep(hot, b, params, precision=1)
+    ts.prepare(3)
+    ts.sync()
+    before_p, before_v = ts.prt.clone(), ts.isv.clone()
+    tables = dict(tempinv=ts.tempinv, sig=ts.sig, capgrey=ts.capgrey, emitprob=ts.emitprob, opaclump=ts.opaclump,
+                  cap=ts.cap)
+    v, ms = hot.autotune_transport(tables, ts.prt, ts.isv, params, precision=1, seed=3, nsample=4000)
+    hot.sync()
+    assert 0 <= v < 4 and all(m > 0.0 for m in ms)
+    assert torch.equal(ts.prt, before_p) and torch.equal(ts.isv, before_v)
+    hot.close()
