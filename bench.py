@@ -8,7 +8,8 @@ the source tally, then ONE persistent mixed-precision particle loop over all
 models and per-model flux tallies, the timed steps captured in a CUDA graph.
 Beside it: the plain FP64 particle loop called once per model, the same step
 through the host-pointer C ABI (e2e), the opacity forward/adjoint of
-configs[1], and the oracle on the host cores.
+the opacity case (256 shells x 2000 groups x 5e5 lines), and the oracle on the
+host cores.
 
 --workload timestep: one full IMC/DDMC timestep on the physical opacities of
 256 shells x 2000 groups x 5e5 lines, 5e7 source particles
@@ -88,7 +89,7 @@ def make_case(a):
 
 
 def config_dict(a, world):
-    return {"workload": "IMC-DDMC timestep on physical LTE opacities (configs[2])",
+    return {"workload": "IMC-DDMC timestep on physical LTE opacities (256 shells x 2000 groups x 5e5 lines)",
             "shells": a.ncell, "groups": a.ng, "lines": int(a.nline), "particles_per_gpu": int(a.npart),
             "snapshot_days": T_DAYS, "tauddmc": 5.0, "taulump": 10.0, "transport_precision": a.precision,
             "parallelism": f"particles{world}", "l2": "inputs larger than L2 (particle array 3.2 GB per GPU)"}
@@ -361,11 +362,11 @@ SEED_BATCH = 4
 
 def batched_config(a, world, b):
     return {"workload": "batched: independent ejecta models, one persistent mixed-precision launch, "
-                        "graph-captured steps (configs[3])",
+                        "graph-captured steps (128 models)",
             "models_per_gpu": int(len(b.nx)), "shells_total": int(b.nx.sum()), "shells_range": [50, 400],
             "particles_per_gpu": int(b.npart.sum()), "particles_range": [1e5, 1e7],
             "snapshot_days_range": [1.0, 30.0], "groups": int(b.groups.ng),
-            "opacity": "analytic grey kappa = 0.1 (rho/1e-13) (T/1e4)^-1.5 cm^2/g (configs[0] physics)",
+            "opacity": "analytic grey kappa = 0.1 (rho/1e-13) (T/1e4)^-1.5 cm^2/g (1 Msun broken power-law ejecta, T ~ U(6000, 14000) K)",
             "tauddmc": 5.0, "taulump": 10.0, "transport_precision": "mixed (FP32 distances, FP64 weights/tallies)",
             "graph_steps": a.steps, "parallelism": f"models{world}",
             "l2": f"inputs larger than L2 (particle array {b.npart.sum() * 64 / 1e9:.1f} GB per GPU)"}
@@ -641,8 +642,8 @@ OPACITY_SIZES = {1: (256, 2000, 500_000), 4: (4096, 10000, 2_000_000)}
 
 
 def opacity_measure(local, reps=5, which=1):
-    """Opacity build of configs[1] (which=1: 256 shells x 2000 groups x 5e5
-    lines) or configs[4] (which=4: 4096 x 10000 x 2e6), Saha populations,
+    """Opacity build of the opacity case (which=1: 256 shells x 2000 groups x
+    5e5 lines) or the opacity case at scale (which=4: 4096 x 10000 x 2e6), Saha populations,
     FP64, forward and reverse through the device C ABI
     (slg_dev_opacity_grad_forward / _backward): cell-group evaluations per
     second of each, timed with CUDA events on the library's stream."""
@@ -700,7 +701,7 @@ def opacity_measure(local, reps=5, which=1):
         out[name] = {"ms": ms, "cell_group_evals_per_s": nc * ng / (ms / 1e3)}
     hot.close()
     lines_bytes = 16 * len(case.lines)
-    out["workload"] = f"configs[{which}]: {ncell} shells x {ngroup} groups x {nline:.0e} lines, Saha populations, " \
+    out["workload"] = f"opacity: {ncell} shells x {ngroup} groups x {nline:.0e} lines, Saha populations, " \
                       "FP64 (forward: EOS + bb/bf/ff + means + leakage; backward: adjoint of all of it)"
     out["line_shell_terms_per_s"] = {k: nline * ncell / (out[k]["ms"] / 1e3) for k in ("forward", "backward")}
     out["bound"] = "FP64 issue (one exp per line-shell term), not HBM: the algorithmic bytes " \
@@ -793,7 +794,7 @@ def run_reference(a):
 
 
 def run_opacity(a):
-    """--workload opacity: the differentiable opacity build at configs[4]
+    """--workload opacity: the differentiable opacity build at the large
     scale (4096 shells x 10000 groups x 2e6 lines), forward and adjoint."""
     import torch
     rank, world, local = dist_env()

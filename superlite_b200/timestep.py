@@ -145,7 +145,7 @@ class DeviceTimestep:
 
 class BatchTimestep:
     """One timestep of many independent models in one context (slg_set_models),
-    device resident: analytic opacity (configs[0] physics), Planck/Rosseland
+    device resident: analytic grey opacity, Planck/Rosseland
     means, leakage opacities, emission probabilities, source particles, the
     source tally, one persistent particle loop over every model's particles
     (precision 1) and per-model flux tallies.  ``capture(nsteps, seed)``

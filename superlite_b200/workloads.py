@@ -452,7 +452,7 @@ def model_batch(nmodel: int = 128, seed: int = 4, ng: int = 2000, nline: int = 5
 
 @dataclasses.dataclass
 class AnalyticBatch:
-    """Independent ejecta models with configs[0] physics (analytic grey
+    """Independent ejecta models with the CPU-runnable case's physics (analytic grey
     opacity, so no composition enters), laid out for slg_set_models."""
     nx: np.ndarray          # shells per model (int32)
     npart: np.ndarray       # particle slots per model (int64)
@@ -471,7 +471,7 @@ def analytic_batch(nmodel: int = 128, seed: int = 4, ng: int = 100, nx_range=(50
     """The batched workload: nmodel models with shells ~ U{nx_range},
     particle budgets log-uniform in npart_range and snapshot times
     log-uniform in t_range_days; per model (seed [seed, m]) T ~ U(6000, 14000)
-    K and the 1 Msun broken power-law density of configs[0]; 100 log groups."""
+    K and a 1 Msun broken power-law density; 100 log groups."""
     rng = np.random.default_rng(seed)
     nxs = (rng.integers(nx_range[0], nx_range[1] + 1, nmodel) if nx is None
            else np.asarray(nx)).astype(np.int32)

@@ -82,7 +82,8 @@ def test_mixed_matches_fp64_statistically(hot, oracle, t_days, kind):
 
 
 def test_mixed_pure_ddmc_config2_physics(hot):
-    """configs[2] physics (every shell optically thick): the DDMC random walk."""
+    """The full-timestep case's physics (256 shells x 2000 groups, every shell
+    optically thick): the DDMC random walk."""
     from superlite_b200 import PACKET_DTYPE
     case = W.opacity_case(ncell=256, ng=2000, nline=500_000, seed=2, t_days=10.0)
     hot.set_groups(case.groups.wl)
