@@ -271,6 +271,67 @@ def ion_table(seed: int = 7, nlev: int = 6) -> IonTable:
     return IonTable(ni, e, nlevel, glev, elev)
 
 
+@dataclasses.dataclass
+class AtomicData:
+    """The reference's atomic data (Data/data.bf_verner, data.ff_sutherland,
+    data.ion and a subset of Atoms/data.atom.*), as parsed into an npz file by
+    tests/golden/make_atomic_data.py."""
+    bf_ph1: np.ndarray      # flat float32, bf_ph1(6,7,30,30)
+    bf_ph2: np.ndarray      # flat float32, bf_ph2(7,30,30)
+    ff_gff: np.ndarray      # flat float64, ff_gff(81,41)
+    ion: "IonTable"
+    lines: np.ndarray       # BBXS_DTYPE, sorted by wl0
+
+    @property
+    def tables(self):
+        return self.bf_ph1, self.bf_ph2, self.ff_gff
+
+
+def ion_table_from_levels(icod, ip_cm, nlev, chi_cm, g, nelem: int = NELEM) -> "IonTable":
+    """ions_read_data (ionsmod.f:652-829) on parsed data.ion records: stage ii of
+    element iz (icod = 100 iz + ii - 1) gets e = h c IP and levels (h c chi, g);
+    ni is the first stage without levels (ionsmod.f:787-794), which becomes the
+    bare ion with one level of weight 1 (:797-806)."""
+    hc = PC_H * PC_C
+    starts = np.concatenate([[0], np.cumsum(nlev)])
+    per = {}
+    for k, code in enumerate(icod):
+        iz, ii = int(code) // 100, int(code) % 100 + 1
+        if iz <= nelem:
+            per[(iz, ii)] = (float(ip_cm[k]), chi_cm[starts[k]:starts[k + 1]], g[starts[k]:starts[k + 1]])
+    ni = np.zeros(nelem, dtype=np.int32)
+    for iz in range(1, nelem + 1):
+        l = 1
+        while l <= iz + 1 and (iz, l) in per and len(per[(iz, l)][1]) > 0:
+            l += 1
+        ni[iz - 1] = l
+    ns = int(ni.max())
+    nl = max(len(v[1]) for v in per.values())
+    e = np.zeros((nelem, ns))
+    nlevel = np.zeros((nelem, ns), dtype=np.int32)
+    glev = np.zeros((nelem, ns, nl))
+    elev = np.zeros((nelem, ns, nl))
+    for iz in range(1, nelem + 1):
+        for ii in range(1, int(ni[iz - 1])):
+            p, c, gg = per[(iz, ii)]
+            e[iz - 1, ii - 1] = hc * p
+            nlevel[iz - 1, ii - 1] = len(c)
+            glev[iz - 1, ii - 1, :len(c)] = gg
+            elev[iz - 1, ii - 1, :len(c)] = hc * np.asarray(c)
+        top = int(ni[iz - 1]) - 1
+        nlevel[iz - 1, top] = 1
+        glev[iz - 1, top, 0] = 1.0
+    return IonTable(ni, e, nlevel, glev, elev)
+
+
+def load_atomic_data(path: str) -> AtomicData:
+    """Read the npz written by tests/golden/make_atomic_data.py."""
+    d = np.load(path)
+    ion = ion_table_from_levels(d["ion_icod"], d["ion_ip_cm"], d["ion_nlev"], d["lev_chi_cm"],
+                                d["lev_g"].astype(np.float64))
+    return AtomicData(d["bf_ph1"], d["bf_ph2"], d["ff_gff"], ion, d["lines"])
+
+
 def composition_state(rho: np.ndarray, massfr: np.ndarray, vol: np.ndarray):
     """massfr2natomfr (GAS/gas_setup.f:101-160) for given mass fractions:
     gas_mass = rho vol, X renormalised to sum 1, number fractions

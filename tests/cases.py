@@ -1,4 +1,6 @@
 """Seeded parity cases shared by the GPU tests (small enough for the oracle)."""
+import os
+
 import numpy as np
 
 from superlite_b200 import workloads as W
@@ -31,3 +33,32 @@ def transport_case(oracle, t_days=5.0, nx=64, ng=100, npart=4000, seed=3, kind="
     prt, isv, emit, nvol, tot = oracle.make_source_particles(grid, groups, temp, L_bol, npart)
     tables = dict(tempinv=tinv, sig=sig, capgrey=capgrey, emitprob=ep, opaclump=ol, cap=cap)
     return dict(grid=grid, groups=groups, temp=temp, rho=rho, tables=tables, prt=prt, isv=isv, params=params)
+
+
+ATOMIC_NPZ = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "atomic_data.npz")
+
+
+def atomic_data():
+    """The reference's atomic data (Verner, Sutherland, data.ion, a subset of
+    Data/Atoms lines), from the committed fixture tests/golden/atomic_data.npz."""
+    return W.load_atomic_data(ATOMIC_NPZ)
+
+
+def reference_opacity_case(oracle, ncell=64, ng=200, nline=20000, seed=11, t_days=10.0, lines="reference"):
+    """opacity_case on the reference's atomic data: real Verner and Sutherland
+    tables, Saha populations (ions_solve_eos + eos_update, via the oracle) from
+    the real data.ion levels for every stage below the bare ion, and either the
+    real line subset (lines="reference", nline ignored) or nline synthetic lines."""
+    import dataclasses
+    A = atomic_data()
+    case = W.opacity_case(ncell=ncell, ng=ng, nline=nline if lines != "reference" else 1, seed=seed,
+                          t_days=t_days, tables=A.tables)
+    if lines == "reference":
+        case = dataclasses.replace(case, lines=A.lines)
+    g = case.gas
+    ion = A.ion
+    q = oracle.partition(ion, float(g.temp[0]))
+    nel, oc, ginv, it = oracle.saha_eos(ion, q, g.temp, g.natom, case.grid.vol, g.natomfr, np.ones(ncell),
+                                        acc=1e-12, noc=ion.nstage - 1)
+    gas = dataclasses.replace(g, nelec=nel, ion_ni=np.ascontiguousarray(ion.ni, dtype=np.int32), oc=oc, ginv=ginv)
+    return dataclasses.replace(case, gas=gas)

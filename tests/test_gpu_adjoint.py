@@ -21,15 +21,21 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-6
 
 
-def _setup(nc=24, ng=120, nline=20000, seed=3, t_days=8.0):
-    case = W.opacity_case(ncell=nc, ng=ng, nline=nline, seed=seed, t_days=t_days)
+def _setup(nc=24, ng=120, nline=20000, seed=3, t_days=8.0, atomic=None):
+    """atomic=None: synthetic tables and ion data; else a workloads.AtomicData
+    (the reference's Verner, Sutherland and data.ion tables)."""
+    case = W.opacity_case(ncell=nc, ng=ng, nline=nline, seed=seed, t_days=t_days,
+                          tables=None if atomic is None else atomic.tables)
+    ion = W.ion_table() if atomic is None else atomic.ion
     hot = HotPath(0)
     hot.set_groups(case.groups.wl)
     hot.set_grid(case.grid.xarr, case.grid.vxarr, case.grid.vol, case.grid.divv)
     g = case.gas
-    hot.set_atomic_data(g.ion_ni, g.oc.shape[1], case.lines, case.bf_ph1, case.bf_ph2, case.ff_gff)
+    nstage = g.oc.shape[1] if atomic is None else ion.nstage - 1
+    hot.set_atomic_data(np.ascontiguousarray(ion.ni, dtype=np.int32), nstage, case.lines, case.bf_ph1, case.bf_ph2,
+                        case.ff_gff)
     amass = [W.ELEM_MASS.get(z, 2.0 * z) for z in range(1, W.NELEM + 1)]
-    D = DifferentiableOpacity(hot, W.ion_table(), q_temp=float(g.temp[0]), elem_mass=amass)
+    D = DifferentiableOpacity(hot, ion, q_temp=float(g.temp[0]), elem_mass=amass)
     dev = D.device
     T = torch.tensor(g.temp, dtype=torch.float64, device=dev)
     R = torch.tensor(g.rho, dtype=torch.float64, device=dev)
@@ -56,9 +62,11 @@ def _L(D, ws, T, R, X):
     return sum((w * o).sum() for w, o in zip(ws, outs))
 
 
+@pytest.mark.parametrize("tables", ["synthetic", "reference"])
 @pytest.mark.parametrize("which", ["temp", "rho", "massfr"])
-def test_adjoint_matches_central_differences(which):
-    hot, D, case, T, R, X = _setup()
+def test_adjoint_matches_central_differences(which, tables):
+    import cases
+    hot, D, case, T, R, X = _setup(atomic=cases.atomic_data() if tables == "reference" else None)
     with torch.no_grad():
         outs = D.opacity(T, R, X)
     ws = _loss_weights(outs, seed=7)

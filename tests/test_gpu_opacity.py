@@ -33,13 +33,7 @@ def _assert_float_close(a, b, max_ulp=1):
     assert np.max(np.abs(ia - ib)) <= max_ulp
 
 
-@pytest.mark.parametrize("flags", [dict(), dict(nobb=True), dict(nobf=True), dict(noff=True),
-                                   dict(nothmson=True), dict(ngs=2, opacmixrossel=0.5)])
-def test_physical_opacity_matches_oracle(hot, oracle, flags):
-    case = cases.opacity_case(ncell=64, ng=200, nline=20000, seed=11)
-    _setup(hot, case)
-    ref = oracle.physical_opacity(case, **flags)
-    got = _gpu_opacity(hot, case, **flags)
+def _assert_opacity_parity(got, ref):
     np.testing.assert_allclose(got["sig"], ref["sig"], rtol=1e-15, atol=0)
     pos = ref["cap64"] > 0
     rel = np.abs(got["cap64"][pos] - ref["cap64"][pos]) / ref["cap64"][pos]
@@ -49,6 +43,45 @@ def test_physical_opacity_matches_oracle(hot, oracle, flags):
     assert np.mean(got["cap"] == ref["cap"]) > 0.999
     np.testing.assert_allclose(got["emiss"], ref["emiss"], rtol=2e-7, atol=0)
     assert got["sanity"] == ref["flags"]
+
+
+@pytest.mark.parametrize("flags", [dict(), dict(nobb=True), dict(nobf=True), dict(noff=True),
+                                   dict(nothmson=True), dict(ngs=2, opacmixrossel=0.5)])
+def test_physical_opacity_matches_oracle(hot, oracle, flags):
+    case = cases.opacity_case(ncell=64, ng=200, nline=20000, seed=11)
+    _setup(hot, case)
+    ref = oracle.physical_opacity(case, **flags)
+    got = _gpu_opacity(hot, case, **flags)
+    _assert_opacity_parity(got, ref)
+
+
+@pytest.mark.parametrize("flags", [dict(), dict(nobb=True, noff=True), dict(nobb=True, nobf=True)])
+def test_physical_opacity_on_reference_atomic_data(hot, oracle, flags):
+    """The reference's own tables: Verner fits (with the nout/einn special
+    cases of bfxsmod.f:104-127), Sutherland Gaunt factors (with the clamp of
+    physical_opacity.f:238 on the real grid), Saha populations from data.ion
+    for all nine bound stages, and 16000 real lines of the ten elements."""
+    case = cases.reference_opacity_case(oracle, ncell=64, ng=200, seed=11, lines="reference")
+    _setup(hot, case)
+    ref = oracle.physical_opacity(case, **flags)
+    got = _gpu_opacity(hot, case, **flags)
+    assert np.all(ref["cap64"] >= 0) and ref["cap64"].max() > 0
+    _assert_opacity_parity(got, ref)
+
+
+def test_physical_opacity_config2_matches_oracle(hot, oracle):
+    """Opacity at the physical-opacity workload's full size (256 shells x 2000
+    groups x 5e5 synthetic lines) on the reference's Verner, Sutherland and
+    data.ion tables, against the single-threaded oracle (about 2 s)."""
+    case = cases.reference_opacity_case(oracle, ncell=256, ng=2000, nline=500_000, seed=2, lines="synthetic")
+    _setup(hot, case)
+    ref = oracle.physical_opacity(case)
+    got = _gpu_opacity(hot, case)
+    _assert_opacity_parity(got, ref)
+    grey, ross = hot.opacity_means(case.gas.temp, ref["sig"], ref["cap"])
+    np.testing.assert_allclose(grey, oracle.planckmean(case.groups.wlinv, case.gas.temp, ref["cap"]), rtol=1e-12)
+    np.testing.assert_allclose(ross, oracle.rossmean(case.groups.wlinv, case.gas.temp, ref["sig"], ref["cap"]),
+                               rtol=1e-12)
 
 
 def test_physical_opacity_config2_shape_properties(hot):
