@@ -41,6 +41,11 @@ extern "C" {
 #define SLG_ERR_UNSORTED (-4)  /* bb line list not sorted by wl0 */
 #define SLG_ERR_OOM (-5)       /* device allocation failed */
 #define SLG_ERR_NOT_BUILT (-6) /* kernel variant not compiled in */
+#define SLG_ERR_TOO_LARGE (-7) /* size beyond a documented limit */
+
+/* Most groups a context or call accepts: per-cell group lists are int16, as
+ * the reference's DDMC lump lists are (integer*2 glumps, diffusion11.f90:49,116). */
+#define SLG_MAX_GROUPS 32767
 
 typedef struct slg_ctx slg_ctx;
 
@@ -68,7 +73,8 @@ const char* slg_last_error(const slg_ctx* ctx);
 const char* slg_version(void);
 
 /* groupmod_init (groupmod.f:29-96): grp_wl(ng+1) in cm, increasing.  Also sets
- * grd_nep = nint(sqrt(ng)), grd_nepg = ceiling(ng/(nep+1)) (gridmod.f:121-122). */
+ * grd_nep = nint(sqrt(ng)), grd_nepg = ceiling(ng/(nep+1)) (gridmod.f:121-122).
+ * ng > SLG_MAX_GROUPS returns SLG_ERR_TOO_LARGE. */
 int slg_set_groups(slg_ctx* ctx, int32_t ng, const double* grp_wl);
 
 /* grid_setup + grid_volume (GRID/grid_setup.f:3-62, GRID/grid_volume.f:66-105):
@@ -319,10 +325,10 @@ int slg_dev_interior_source(slg_ctx* ctx, const double* radtemp, const double* e
                             int64_t npart, uint64_t seed, int64_t* nnew);
 /* ------------------------------------------------------------------ no device allocation */
 
-/* Size limits of slg_particle_advance_static (see below). */
+/* Size limits of slg_particle_advance_static (see below).  Its group count is
+ * also bounded by SLG_MAX_GROUPS, like every other entry point. */
 #define SLG_STATIC_MAX_CELLGROUPS 131072 /* ncell * ng */
 #define SLG_STATIC_MAX_CELLS 4096
-#define SLG_ERR_TOO_LARGE (-7)           /* grid larger than the static limits */
 
 /* Grid and group arrays on the device (grd_xarr, grd_vxarr (nx+1), grd_divv
  * (nx), grp_wl, grp_wlinv (ng+1)), for the entry point below. */
@@ -345,8 +351,10 @@ typedef struct slg_grid_dev {
  * SLG_ERR_TOO_LARGE.  Runs on `stream` (a cudaStream_t, NULL = default) on the
  * current device and returns after the stream has finished it.  The first
  * call on a device looks up the array's device address; make it before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * race, so serialise them. */
+ * stream capture.  The address is kept per device for the life of the
+ * process, so do not call this entry point again after cudaDeviceReset (which
+ * unloads the array).  All calls share the array: calls that overlap on the
+ * GPU race, so serialise them. */
 int slg_particle_advance_static(const slg_grid_dev* grid, const slg_transport_in* in,
                                 slg_packet* prt, int32_t* isvacant, int64_t npart,
                                 uint64_t seed, slg_transport_out* out, void* stream);

@@ -2,7 +2,7 @@
 // Rosseland means of the reference, restated on the CPU.
 // TEST INFRASTRUCTURE ONLY (parity checker for the CUDA product).
 //
-// GAS/physical_opacity.f:3-357, bfxsmod.f:184-272, GAS/analytic_opacity.f90:3-77,
+// GAS/physical_opacity.f:3-357, bfxsmod.f:65-153, GAS/analytic_opacity.f90:3-77,
 // GAS/opacity_planckmean.f:3-27, GAS/opacity_rossmean.f:3-23.
 // Single-threaded: the reference's OpenMP bb loop accumulates into a shared
 // cap(i,igs) without atomics (physical_opacity.f:104-152) and is only exact
@@ -14,7 +14,7 @@
 using namespace orc;
 
 namespace {
-// bfxsmod.f:126-131
+// bfxsmod.f:8-12
 const int ll[7] = {0, 0, 1, 0, 1, 2, 0};
 const int ninn[30] = {0, 0, 1, 1, 1, 1, 1, 1, 1, 1, 3, 3, 3, 3, 3,
                       3, 3, 3, 5, 5, 5, 5, 5, 5, 5, 5, 5, 5, 5, 5};
@@ -33,7 +33,7 @@ inline float sqf(float x) { return x * x; }  // real*4 ** 2, evaluated in single
 
 extern "C" {
 
-// bfxsmod.f:184-272 (Verner et al. 1996 / Verner & Yakovlev 1995 fits).
+// bfxsmod.f:65-153 (Verner et al. 1996 / Verner & Yakovlev 1995 fits).
 double orc_bfxs(const float* ph1, const float* ph2, int nz, int ne, double e) {
   double xs = 0.0;
   if (nz < 1 || nz > 30) return xs;

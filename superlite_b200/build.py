@@ -52,8 +52,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     nvcc = _nvcc()
     cxx = _host_cxx()
     inc = ["-I", os.path.join(ROOT, "include"), "-I", CSRC]
-    common = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--use_fast_math=false"]
-    common = [f for f in common if f != "--use_fast_math=false"]
+    common = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
     if cxx:
         common += ["-ccbin", cxx]
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "slg.h")]

@@ -354,6 +354,8 @@ int slg_transport_totals(slg_ctx* ctx, slg_transport_out* out, int32_t reset) {
 
 int slg_set_groups(slg_ctx* ctx, int32_t ng, const double* grp_wl) {
   if (!ctx || ng < 1 || !grp_wl) return set_error(ctx, SLG_ERR_ARG, "slg_set_groups: bad arguments");
+  if (ng > SLG_MAX_GROUPS)
+    return set_error(ctx, SLG_ERR_TOO_LARGE, "slg_set_groups: %d groups > SLG_MAX_GROUPS (%d)", ng, SLG_MAX_GROUPS);
   for (int k = 0; k < ng; ++k)
     if (!(grp_wl[k + 1] > grp_wl[k]) || !(grp_wl[k] > 0.0))
       return set_error(ctx, SLG_ERR_ARG, "slg_set_groups: wavelength grid not increasing at %d", k);

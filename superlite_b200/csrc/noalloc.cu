@@ -11,7 +11,8 @@
 //
 // Limits and sharing: the array holds the tables of at most
 // SLG_STATIC_MAX_CELLGROUPS (ncell * ng) entries and SLG_STATIC_MAX_CELLS
-// cells; larger grids are rejected with SLG_ERR_TOO_LARGE.  All calls share
+// cells, with at most SLG_MAX_GROUPS groups (group lists are int16); larger
+// grids are rejected with SLG_ERR_TOO_LARGE.  All calls share
 // the one array and it keeps the last call's contents: counters are cleared at
 // the start of every call, and calls that overlap on the GPU (two streams, two
 // host threads) race on it.
@@ -78,7 +79,7 @@ extern "C" int slg_particle_advance_static(const slg_grid_dev* grid, const slg_t
   if (!out->tally || !out->jrad || !out->eamp || (in->dogrdtally && !out->methodswap)) return SLG_ERR_ARG;
   if (in->precision != 0) return SLG_ERR_NOT_BUILT;
   const size_t nx = (size_t)grid->nx, ng = (size_t)grid->ng;
-  if (nx > kMaxCells || nx * ng > kMaxCellGroups) return SLG_ERR_TOO_LARGE;
+  if (nx > kMaxCells || nx * ng > kMaxCellGroups || ng > SLG_MAX_GROUPS) return SLG_ERR_TOO_LARGE;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return SLG_ERR_CUDA;
   unsigned char* base = nullptr;

@@ -2,7 +2,7 @@
 // groups, Verner bound-free, Sutherland free-free), analytic opacity and the
 // Planck / Rosseland means, for sm_100a.
 //
-// Reference: GAS/physical_opacity.f:3-357, bfxsmod.f:184-272,
+// Reference: GAS/physical_opacity.f:3-357, bfxsmod.f:65-153,
 // GAS/analytic_opacity.f90:3-77, GAS/opacity_planckmean.f:17-24,
 // GAS/opacity_rossmean.f:17-21.
 //
@@ -232,7 +232,7 @@ __device__ inline float PH2(const float* t, int k, int nz, int ne) {
 }
 __device__ inline float sqf(float x) { return __fmul_rn(x, x); }  // real*4 ** 2
 
-// bfxsmod.f:184-272
+// bfxsmod.f:65-153
 __device__ double bfxs(const float* __restrict__ ph1, const float* __restrict__ ph2, int nz, int ne,
                        double e) {
   const int ll[7] = {0, 0, 1, 0, 1, 2, 0};

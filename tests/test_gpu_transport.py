@@ -146,6 +146,13 @@ def test_fluxtally_and_sourcetally_match_oracle(hot, oracle):
     assert np.array_equal(vg, vo)
 
 
+def test_set_groups_rejects_more_than_int16_groups(hot):
+    from superlite_b200 import SlgError
+    wl = np.geomspace(1e-5, 3.2e-4, 40001)  # 40000 groups > SLG_MAX_GROUPS (group lists are int16)
+    with pytest.raises(SlgError):
+        hot.set_groups(wl)
+
+
 def test_empty_and_all_vacant(hot, oracle):
     c = cases.transport_case(oracle, t_days=12.0, npart=300)
     _setup(hot, c)

@@ -7,6 +7,7 @@ calls in a row (the shared array must be cleared between calls), with the
 transport tolerances of tests/test_gpu_transport.py.
 """
 import ctypes as C
+import dataclasses
 
 import numpy as np
 import pytest
@@ -27,9 +28,11 @@ def _run_existing(hot, c, tables, prt_t, isv_t, seed, torch):
     tally = torch.zeros(nx, dtype=torch.float64, device="cuda")
     jrad = torch.zeros((nx, ng), dtype=torch.float64, device="cuda")
     eamp = torch.zeros(nx, dtype=torch.float64, device="cuda")
-    out = hot.particle_advance_dev(tables, prt_t, isv_t, tally, jrad, eamp, c["params"], seed=seed)
+    mswap = torch.zeros(nx, dtype=torch.int32, device="cuda") if c["params"].dogrdtally else None
+    out = hot.particle_advance_dev(tables, prt_t, isv_t, tally, jrad, eamp, c["params"], seed=seed,
+                                   methodswap=mswap)
     hot.sync()
-    return out, tally, jrad
+    return out, tally, jrad, mswap
 
 
 def _run_static(lib, c, tables, prt_t, isv_t, seed, torch, grid_arrays):
@@ -43,18 +46,21 @@ def _run_static(lib, c, tables, prt_t, isv_t, seed, torch, grid_arrays):
     tally = torch.full((nx,), 7.0, dtype=torch.float64, device="cuda")   # must be overwritten
     jrad = torch.full((nx, ng), 7.0, dtype=torch.float64, device="cuda")
     eamp = torch.full((nx,), 7.0, dtype=torch.float64, device="cuda")
-    out = capi.SlgTransportOut(ptr(tally), ptr(jrad), ptr(eamp), None, 0.0, 0.0, 0.0)
+    mswap = torch.full((nx,), 7, dtype=torch.int32, device="cuda") if p.dogrdtally else None
+    out = capi.SlgTransportOut(ptr(tally), ptr(jrad), ptr(eamp), ptr(mswap), 0.0, 0.0, 0.0)
     stream = torch.cuda.current_stream().cuda_stream
     rc = lib.slg_particle_advance_static(C.byref(g), C.byref(tin), ptr(prt_t), ptr(isv_t), int(prt_t.shape[0]),
                                          seed, C.byref(out), C.c_void_p(stream))
     assert rc == 0, rc
-    return out, tally, jrad
+    return out, tally, jrad, mswap
 
 
-def test_static_scratch_entry_point_matches_context_entry_point(hot, oracle):
+@pytest.mark.parametrize("dogrdtally", [False, True])
+def test_static_scratch_entry_point_matches_context_entry_point(hot, oracle, dogrdtally):
     import torch
     lib = capi.load()
     c = cases.transport_case(oracle, t_days=6.0, npart=6000, kind="mono")
+    c["params"] = dataclasses.replace(c["params"], dogrdtally=dogrdtally)
     hot.set_groups(c["groups"].wl)
     hot.set_grid(c["grid"].xarr, c["grid"].vxarr, c["grid"].vol, c["grid"].divv)
     t = c["tables"]
@@ -68,9 +74,9 @@ def test_static_scratch_entry_point_matches_context_entry_point(hot, oracle):
     isv0 = torch.as_tensor(c["isv"]).cuda()
     for seed in (11, 12):  # two calls in a row on the shared array
         pa, va = prt0.clone(), isv0.clone()
-        oa, ta, ja = _run_existing(hot, c, tables, pa, va, seed, torch)
+        oa, ta, ja, ma = _run_existing(hot, c, tables, pa, va, seed, torch)
         pb, vb = prt0.clone(), isv0.clone()
-        ob, tb, jb = _run_static(lib, c, tables, pb, vb, seed, torch, grid_arrays)
+        ob, tb, jb, mb = _run_static(lib, c, tables, pb, vb, seed, torch, grid_arrays)
         torch.cuda.synchronize()
         assert oa.nstepimc + oa.nstepddmc > 6000
         for k in ("npckt", "nflux", "nstepimc", "nstepddmc", "nmethodswap", "nstepmax", "nposwarn", "ierr"):
@@ -83,6 +89,9 @@ def test_static_scratch_entry_point_matches_context_entry_point(hot, oracle):
             assert getattr(ob, k) == pytest.approx(getattr(oa, k), rel=1e-9), k
         np.testing.assert_allclose(tb.cpu().numpy(), ta.cpu().numpy(), rtol=1e-9, atol=1e-300)
         np.testing.assert_allclose(jb.cpu().numpy(), ja.cpu().numpy(), rtol=1e-9, atol=1e-300)
+        if dogrdtally:  # grd_methodswap per cell, cleared by the call (it started at 7)
+            assert np.array_equal(mb.cpu().numpy(), ma.cpu().numpy())
+            assert int(ma.sum()) == oa.nmethodswap > 0
 
 
 def test_static_scratch_rejects_large_grids():
@@ -95,3 +104,7 @@ def test_static_scratch_rejects_large_grids():
     out = capi.SlgTransportOut(1, 1, 1, None, 0.0, 0.0, 0.0)
     rc = lib.slg_particle_advance_static(C.byref(big), C.byref(tin), 1, 1, 10, 1, C.byref(out), None)
     assert rc == -7  # SLG_ERR_TOO_LARGE, before any device work
+    # within the cell-group budget but beyond SLG_MAX_GROUPS (group lists are int16)
+    wide = capi.SlgGridDev(2, 40000, 1, 1, 1, 1, 1)
+    rc = lib.slg_particle_advance_static(C.byref(wide), C.byref(tin), 1, 1, 10, 1, C.byref(out), None)
+    assert rc == -7
