@@ -43,11 +43,21 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s"
+# the reference's atomic data (Verner, Sutherland, data.ion, a subset of its
+# line lists), parsed into a committed npz by tests/golden/make_atomic_data.py
+ATOMIC_NPZ = os.path.join(ROOT, "tests", "golden", "atomic_data.npz")
 T_DAYS = 10.0
 SEED_CASE = 2
 L_BOL = 1e42
 # algorithmic bytes of one particle-step: event-based SoA traffic, 2 x (5 x 8 + 4 x 4 + 8) B
 BYTES_PER_STEP = 128.0
+# Warp instructions issued per particle-step by particle_advance_mixed_kernel and
+# the active lanes per warp instruction, from one ncu capture of that kernel on
+# the batched workload at 0.1x particle budgets (smsp__inst_executed.sum /
+# particle-steps of the launch; smsp__thread_inst_executed.sum /
+# smsp__inst_executed.sum): profiles/particle_advance_mixed_batched_128models_npart0.1.md
+MIXED_WARP_INST_PER_STEP = 71.3
+MIXED_LANES_PER_INST = 10.4
 
 
 def parse():
@@ -71,6 +81,8 @@ def parse():
     ap.add_argument("--nmodel", type=int, default=128)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 per-model comparison")
     ap.add_argument("--no-opacity", action="store_true", help="skip the opacity forward/adjoint measurement")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the lines of the CPU-runnable case and of the full timestep beside the batched one")
     ap.add_argument("--npart-scale", type=float, default=1.0,
                     help="scale the models' particle budgets (small cases for profilers; default 1)")
     return ap.parse_args()
@@ -372,11 +384,49 @@ def batched_config(a, world, b):
             "l2": f"inputs larger than L2 (particle array {b.npart.sum() * 64 / 1e9:.1f} GB per GPU)"}
 
 
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _lum_rows(ts):
+    return (ts.lum.cpu().numpy().copy(), ts.lumdev.cpu().numpy().copy(), ts.lumnum.cpu().numpy().copy())
+
+
+def batched_transport(ts, seed, precision, autotune=False):
+    """One step of the batch (sources, opacities, coefficients), then ONE
+    particle-loop launch over all models in `precision` (0: FP64, 1: mixed),
+    the loop timed with CUDA events on the library's stream, then the flux
+    tallies.  The sources depend only on `seed`, so both precisions transport
+    the same particles.  Returns a dict (ms, steps, lum rows, counters)."""
+    from superlite_b200.api import transport_out_dict
+    ts.set_precision(precision)
+    ts.prepare(seed)
+    variant = None
+    if autotune:
+        variant, _ = ts.autotune(seed=seed, nsample=1_000_000)
+    ts.sync()
+    e0, e1 = _events()
+    e0.record(ts.stream)
+    ts.transport(seed)
+    e1.record(ts.stream)
+    ts.flux()
+    ts.sync()
+    c = transport_out_dict(ts._tout)
+    lum, dev, num = _lum_rows(ts)
+    ts.set_precision(1)
+    return {"ms": e0.elapsed_time(e1), "steps": int(c["nstepimc"] + c["nstepddmc"]), "lum": lum, "dev": dev,
+            "num": num, "counters": c, "variant": variant}
+
+
 def fp64_per_model(b, ts, params, local, seed):
     """The plain FP64 form on the same models: one model per call, as the
     single-model C ABI is called by a driver that runs the models one after
     another (each model in its own context; every call completes before the
-    next).  One step; returns (particle-steps/s, steps, seconds, variant)."""
+    next).  Each call's particle loop is timed with CUDA events on its
+    context's stream; the sum of those device times is the FP64 form's time
+    (the host wall time around the calls is reported beside it).  Returns a
+    dict (ms, wall_s, steps, variant, lum rows of the same step)."""
     import torch
     from superlite_b200 import HotPath
     from superlite_b200.capi import ptr
@@ -390,6 +440,7 @@ def fp64_per_model(b, ts, params, local, seed):
         h.set_grid(b.xarr[eo[m]:eo[m + 1]], b.vxarr[eo[m]:eo[m + 1]], b.vol[co[m]:co[m + 1]],
                    b.divv[co[m]:co[m + 1]])
         hots.append(h)
+    ts.set_precision(1)
     ts.prepare(seed)
     ts.sync()
     sl = lambda t, m: t[co[m]:co[m + 1]]
@@ -407,23 +458,54 @@ def fp64_per_model(b, ts, params, local, seed):
     for h in hots:
         h._check(h.lib.slg_set_transport_variant(h.h, int(best.value)))
     hb.sync()
-    outs = []
+    outs, dev_ms = [], 0.0
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for m, h in enumerate(hots):
         tables = dict(tempinv=sl(ts.tempinv, m), sig=sl(ts.sig, m), capgrey=sl(ts.capgrey, m),
                       emitprob=sl(ts.emitprob, m), opaclump=sl(ts.opaclump, m), cap=sl(ts.cap, m))
+        stream = torch.cuda.ExternalStream(h.stream(), device=torch.device("cuda", local))
+        e0, e1 = _events()
+        e0.record(stream)
         outs.append(h.particle_advance_dev(tables, ts.prt[po[m]:po[m + 1]], ts.isv[po[m]:po[m + 1]],
                                            sl(ts.tally, m), sl(ts.jrad, m), sl(ts.eamp, m), params,
                                            seed=seed, precision=0))
+        e1.record(stream)
         h.sync()
-    dt = time.perf_counter() - t0
+        dev_ms += e0.elapsed_time(e1)
+    wall = time.perf_counter() - t0
     steps = sum(o.nstepimc + o.nstepddmc for o in outs)
     ts.flux()  # tally the escaped particles and free their slots in the batched context
     ts.sync()
+    lum, dev, num = _lum_rows(ts)
     for h in hots:
         h.close()
-    return steps / dt, int(steps), dt, int(best.value)
+    return {"ms": dev_ms, "wall_s": wall, "steps": int(steps), "variant": int(best.value), "lum": lum, "dev": dev,
+            "num": num}
+
+
+def luminosity_zscores(A, B, t_days, nbin=4):
+    """Per model and wavelength bin (nbin contiguous bins of groups), z = (L_A -
+    L_B) / sqrt(lumdev_A + lumdev_B), lumdev = sum of e^2 of the escaped
+    particles (fluxtally.f:47-49; an upper bound of the variance of L)."""
+    la, da, lb, db = A["lum"], A["dev"], B["lum"], B["dev"]
+    nm, ng = la.shape
+    edges = np.linspace(0, ng, nbin + 1).astype(int)
+    zs = []
+    for m in range(nm):
+        for a, b in zip(edges[:-1], edges[1:]):
+            v = da[m, a:b].sum() + db[m, a:b].sum()
+            if v > 0:
+                zs.append(((la[m, a:b].sum() - lb[m, a:b].sum()) / math.sqrt(v), m))
+    z = np.array([q[0] for q in zs])
+    worst = sorted(zs, key=lambda q: -abs(q[0]))[:5]
+    tot_a, tot_b = la.sum(axis=1), lb.sum(axis=1)
+    rel = np.abs(tot_a - tot_b) / np.maximum(np.abs(tot_b), 1e-300)
+    return {"comparisons": int(len(z)), "bins_per_model": nbin, "max_abs_z": float(np.abs(z).max()),
+            "frac_abs_z_gt_3": float((np.abs(z) > 3).mean()), "expected_frac_gt_3_if_normal": 0.0027,
+            "worst": [{"model": int(m), "t_days": round(float(t_days[m]), 3), "z": round(float(v), 3)}
+                      for v, m in worst],
+            "median_rel_diff_total_luminosity": float(np.median(rel))}
 
 
 def run_batched(a):
@@ -497,16 +579,26 @@ def run_batched(a):
     peak, peak_kind = measured_peaks()
     tr_rate = (steps_total / a.steps) / (t_tr / 1e3) if t_tr else None
     achieved = BYTES_PER_STEP * tr_rate / 1e9 if tr_rate else None
+    from superlite_b200 import peaks as PK
+    pipes = PK.measure(local)
+    issue_peak = pipes["warp_inst_issue_per_s"]["value"]
+    issue = MIXED_WARP_INST_PER_STEP * tr_rate if tr_rate else None
     res = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded generator, superlite_b200/workloads.py)",
         "config": batched_config(a, world, b),
         "phase_ms_last_warmup_step": {"sources+opacity+coefficients": t_prep, "particle_advance": t_tr},
-        "counters": {k: tot[k] for k in ("npckt", "nflux", "nstepimc", "nstepddmc", "nstepmax", "nmethodswap",
-                                         "ierr")},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if achieved else None,
+        "counters": {**{k: tot[k] for k in ("npckt", "nflux", "nstepimc", "nstepddmc", "nstepmax", "nmethodswap",
+                                            "ierr")},
+                     # events by ptcl2%idist (particle_advance.f90:211-212): -3 (both leaks), -2 (DDMC
+                     # effective scatter), -1, 0, 1 collision, 2 Thomson, 3 Doppler, 4 boundary, 5..7
+                     "ndist": [int(x) for x in tot["ndist"]]},
+        # The particle loop is bound by instruction issue and latency (divergent, dependent gathers
+        # of L2-resident tables), not by HBM: its roofline is the measured warp-instruction issue
+        # rate; the HBM reading on the 128 B per particle-step basis is kept beside it (non-binding).
+        "roofline": {"bound": "issue", "achieved": issue, "peak": issue_peak, "unit": "warp-instructions/s",
+                     "frac": issue / issue_peak if issue else None,
                      # DRAM bytes of one launch: ncu dram__bytes_read.sum + dram__bytes_write.sum of this
                      # kernel on the same batch with particle budgets x 0.1 (4.157e9 B for 2.944e7
                      # particles: the packets read and written once, plus table and tally traffic),
@@ -515,8 +607,17 @@ def run_batched(a):
                      "traffic_basis": "ncu capture of particle_advance_mixed_kernel at 0.1x particle budgets "
                                       "(4.16 GB), scaled by particles",
                      "kernel": "particle_advance_mixed_kernel",
-                     "basis": f"{BYTES_PER_STEP:.0f} B per particle-step x steps of one step / particle_advance "
-                              f"time of the last warm-up step; peak {peak_kind}"},
+                     "basis": f"{MIXED_WARP_INST_PER_STEP} warp instructions per particle-step (ncu) x particle-"
+                              "steps/s of the last warm-up step's particle loop; peak = measured FP32-FMA issue "
+                              "rate of this GPU (slg_pipe_throughput, one warp instruction per cycle per "
+                              "scheduler)",
+                     "simt_lanes_per_warp_instruction": MIXED_LANES_PER_INST,
+                     "hbm": {"achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak if achieved else None, "binding": False,
+                             "basis": f"{BYTES_PER_STEP:.0f} B per particle-step (event-based SoA traffic); "
+                                      f"peak {peak_kind}"}},
+        "pipe_peaks": {k: pipes[k]["value"] for k in ("fp64_fma_flops", "fp64_exp_per_s", "fp32_fma_flops",
+                                                      "int32_imad_per_s", "warp_inst_issue_per_s")},
         "clocks": clocks, "autotune": {"variant": variant, "sample_ms": tune_ms},
         "gpu_launches": None,
     }
@@ -536,19 +637,40 @@ def run_batched(a):
         return float(t.item()) / float(m.item()), int(t.item()), float(m.item())
 
     if not a.no_fp64:
-        rate, st64, dt64, var64 = fp64_per_model(b, ts, params, local, seed0 + 999)
-        rate, st64, dt64 = whole_job(st64, dt64)
-        res["fp64_plain_per_model"] = {"value": rate, "unit": "particle-steps/s", "steps": st64, "seconds": dt64,
-                                       "variant": var64,
-                                       "form": "FP64 particle loop, one call per model (own context), "
-                                               "each completed before the next"}
-        res["mixed_batched_over_fp64_plain"] = value / rate
+        # the three forms on one comparison step (same sources), each particle loop timed the same way:
+        # CUDA events on the launching stream around the loop (cell tables + kernel)
+        S = seed0 + 999
+        mix = batched_transport(ts, S, 1)
+        f64b = batched_transport(ts, S, 0, autotune=True)
+        f64p = fp64_per_model(b, ts, params, local, S)
+        r_mix = whole_job(mix["steps"], mix["ms"] / 1e3)[0]
+        r_f64b = whole_job(f64b["steps"], f64b["ms"] / 1e3)[0]
+        r_f64p, st64, dt64 = whole_job(f64p["steps"], f64p["ms"] / 1e3)
+        res["comparison_step"] = {
+            "timing": "particle loop only, CUDA events on the launching stream, same step (same sources)",
+            "mixed_batched": {"value": r_mix, "unit": "particle-steps/s", "steps": mix["steps"], "ms": mix["ms"]},
+            "fp64_batched": {"value": r_f64b, "unit": "particle-steps/s", "steps": f64b["steps"], "ms": f64b["ms"],
+                             "variant": f64b["variant"],
+                             "form": "FP64 particle loop, all models in one persistent launch"},
+            "fp64_plain_per_model": {"value": r_f64p, "unit": "particle-steps/s", "steps": st64, "ms": f64p["ms"],
+                                     "wall_s": f64p["wall_s"], "variant": f64p["variant"],
+                                     "form": "FP64 particle loop, one call per model (own context), each "
+                                             "completed before the next; sum of the calls' device times"},
+        }
+        res["mixed_batched_over_fp64_plain"] = r_mix / r_f64p
+        res["fp64_batched_over_fp64_plain"] = r_f64b / r_f64p
+        res["mixed_batched_over_fp64_batched"] = r_mix / r_f64b
+        res["mixed_vs_fp64_luminosity"] = luminosity_zscores(mix, f64b, b.t_days)
+        res["mixed_vs_fp64_luminosity"]["pair"] = "mixed batched vs FP64 batched, same source particles"
     if not a.no_e2e:
         e = batched_e2e(a, b, params, local, seed0)
         e["value"], e["particle_steps"], e["seconds"] = whole_job(e["particle_steps"], e["seconds"])
         res["e2e"] = e
+    if not a.no_configs:
+        res["config0"] = config0_measure(a, local, rank, world)
+        res["config2"] = config2_measure(a, local, rank, world)
     if not a.no_opacity:
-        res["opacity"] = opacity_measure(local)
+        res["opacity"] = opacity_measure(local, exp_per_s=pipes["fp64_exp_per_s"]["value"])
         res["opacity_cell_group_evals_per_s"] = res["opacity"]["forward"]["cell_group_evals_per_s"]
     if rank == 0 and world == 1 and not a.no_cpu:
         res["cpu_baseline"] = batched_cpu_baseline(a, b, params)
@@ -600,9 +722,21 @@ def batched_e2e(a, b, params, local, seed0):
                     "allocated inside the timed step)"}
 
 
+def stratified_order(t_days):
+    """Models in an order whose every prefix spreads over the snapshot times:
+    sorted by t, then visited in bit-reversed rank order (0, n/2, n/4, 3n/4 ...)."""
+    n = len(t_days)
+    srt = np.argsort(t_days, kind="stable")
+    bits = max(1, (n - 1).bit_length())
+    ranks = [int(format(i, f"0{bits}b")[::-1], 2) for i in range(1 << bits)]
+    return [int(srt[r]) for r in ranks if r < n]
+
+
 def batched_cpu_baseline(a, b, params, budget_s=20.0):
     """The oracle (C++ restatement of the Fortran, FP64, mzran, OpenMP over
-    particles) on a bounded sample: a few models, a particle sample each."""
+    particles) on a bounded sample: models taken in a stratified order over
+    their snapshot times (every prefix spans early and late models), a
+    particle sample each, until the time budget is spent."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
     from superlite_b200 import workloads as W
@@ -612,7 +746,7 @@ def batched_cpu_baseline(a, b, params, budget_s=20.0):
     steps = 0
     dt = 0.0
     used = []
-    for m in range(len(b.nx)):
+    for m in stratified_order(b.t_days):
         g = W.Grid(int(b.nx[m]), 0.0, b.xarr[eo[m]:eo[m + 1]], b.vxarr[eo[m]:eo[m + 1]],
                    b.vol[co[m]:co[m + 1]], b.divv[co[m]:co[m + 1]])
         T, rho = b.temp[co[m]:co[m + 1]], b.rho[co[m]:co[m + 1]]
@@ -632,32 +766,187 @@ def batched_cpu_baseline(a, b, params, budget_s=20.0):
         used.append((m, sample))
         if dt > budget_s:
             break
+    td = np.array([b.t_days[m] for m, _ in used])
     return {"value": steps / dt, "unit": "particle-steps/s", "cores": cores, "kind": "port",
-            "sample": f"{len(used)} of {len(b.nx)} models, {used[0][1]} particles each (mzran, OpenMP static,1, "
-                      f"FP64 oracle), transport only"}
+            "sample": f"{len(used)} of {len(b.nx)} models in a stratified order over snapshot time "
+                      f"(t = {td.min():.2f}-{td.max():.2f} d, median {np.median(td):.2f} d), {used[0][1]} particles "
+                      f"each (mzran, OpenMP static,1, FP64 oracle), transport only",
+            "models": [m for m, _ in used]}
+
+
+# ------------------------------------------------------------------ the other two transport configurations
+CONFIG0 = dict(nx=64, ng=100, npart=1_000_000, nsnap=20, t0=1.0, t1=30.0, seed=21)
+
+
+def config0_measure(a, local, rank, world):
+    """The CPU-runnable case: 64 shells (v 0-1.5e9 cm/s, 1 Msun broken power law,
+    T ~ U(6000, 14000) K per shell, seeded), analytic grey opacity, 100 groups,
+    1e6 particles per snapshot, 20 snapshots log-spaced in t = 1-30 d, the
+    plain FP64 particle loop (one model per context, as the reference runs it).
+    Every snapshot: sources, opacity, means, leakage, emission probabilities,
+    source tally, particle loop and flux tally on the device; the particle
+    loops and the whole snapshots timed with CUDA events.  Beside it the
+    oracle (mzran, all host cores) on a bounded particle sample of every
+    snapshot."""
+    import torch
+    from superlite_b200 import HotPath, workloads as W
+    from superlite_b200.timestep import BatchTimestep
+    C0 = CONFIG0
+    ts_days = np.geomspace(C0["t0"], C0["t1"], C0["nsnap"])
+    params = W.TransportParams()
+    steps = 0
+    ms_tr = ms_all = 0.0
+    models = []
+    for k, td in enumerate(ts_days):
+        b = W.analytic_batch(nmodel=1, seed=C0["seed"] + 1000 * rank, nx=[C0["nx"]], npart=[C0["npart"]],
+                             t_range_days=(td, td))
+        models.append(b)
+        hot = HotPath(local)
+        ts = BatchTimestep(hot, b, params, precision=0)
+        seed = 100 + k
+        if k == 0:  # warm-up snapshot: the FP64 kernel variant picked on this workload
+            ts.prepare(seed)
+            ts.autotune(seed=seed, nsample=C0["npart"])
+            ts.finish(seed)
+            ts.sync()
+        e0, e1 = _events()
+        e2, e3 = _events()
+        e0.record(ts.stream)
+        ts.prepare(seed)
+        e2.record(ts.stream)
+        ts.transport(seed)
+        e3.record(ts.stream)
+        ts.flux()
+        e1.record(ts.stream)
+        ts.sync()
+        c = ts._tout
+        steps += int(c.nstepimc + c.nstepddmc)
+        ms_tr += e2.elapsed_time(e3)
+        ms_all += e0.elapsed_time(e1)
+        hot.close()
+    res = {"workload": "CPU-runnable case: 64 shells, analytic grey opacity, 100 groups, 1e6 particles, 20 "
+                       "snapshots t = 1-30 d, plain FP64 particle loop",
+           "metric": METRIC, "value": steps / (ms_all / 1e3), "unit": "particle-steps/s",
+           "particle_loop_value": steps / (ms_tr / 1e3), "particle_steps": steps, "ms_all_snapshots": ms_all,
+           "ms_particle_loops": ms_tr, "timing": "CUDA events on the library stream, every phase of every snapshot"}
+    if rank == 0 and world == 1 and not a.no_cpu:
+        res["cpu_baseline"] = config0_cpu(models, params)
+    return res
+
+
+def config0_cpu(models, params, sample=40_000):
+    """The oracle on every snapshot of the CPU-runnable case, a particle sample each."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    from superlite_b200 import workloads as W
+    cores = os.cpu_count() or 1
+    steps, dt, npart = 0, 0.0, 0
+    for k, b in enumerate(models):
+        g = W.Grid(int(b.nx[0]), 0.0, b.xarr, b.vxarr, b.vol, b.divv)
+        T, rho = b.temp, b.rho
+        sig, cap = po.analytic_opacity(b.groups.wlinv, T, rho, kind=1)
+        tinv = 1.0 / T
+        grey = po.planckmean(b.groups.wlinv, T, cap)
+        ol = po.leakage_opacity11(g, b.groups.wlinv, tinv, sig, cap, tauddmc=params.tauddmc, taulump=params.taulump)
+        ep = po.emission_probability(b.groups.wlinv, tinv, cap, grey, b.groups.nep, b.groups.nepg)
+        tt = po.TransportTables(g, b.groups, tinv, sig, cap, grey, ep, ol, params)
+        prt, isv, _, _, _ = po.make_source_particles(g, b.groups, T, L_BOL, sample)
+        st = po.rnd_init(cores, k)
+        t0 = time.perf_counter()
+        r = po.particle_advance(tt, prt, isv, rngmode=0, nthreads=cores, rnd_states=st)
+        dt += time.perf_counter() - t0
+        steps += r["nstepimc"] + r["nstepddmc"]
+        npart = int(b.npart[0])
+    return {"value": steps / dt, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "sample": f"{sample} of {npart} particles in each of the {len(models)} snapshots (mzran, OpenMP "
+                      f"static,1, FP64 oracle), particle loop only, {dt:.1f} s"}
+
+
+def config2_measure(a, local, rank, world, npart=50_000_000):
+    """The full timestep: 256 shells x 2000 groups, physical LTE opacity from
+    5e5 synthetic lines on the reference's Verner, Sutherland and data.ion
+    tables (Saha populations from the device equation of state), 5e7 source
+    particles, DDMC where a shell is optically thick; one step with the FP64
+    particle loop and one with the mixed-precision loop (each after one
+    untimed step), every phase on the device, CUDA events."""
+    import dataclasses
+    import torch
+    from superlite_b200 import HotPath, workloads as W
+    from superlite_b200.timestep import DeviceTimestep
+    A = W.load_atomic_data(ATOMIC_NPZ)
+    case = W.opacity_case(ncell=256, ng=2000, nline=500_000, seed=SEED_CASE, t_days=T_DAYS, tables=A.tables)
+    params = W.TransportParams()
+    out = {"workload": "full timestep: 256 shells x 2000 groups, physical opacity (5e5 synthetic lines, the "
+                       "reference's Verner/Sutherland/data.ion tables), 5e7 particles",
+           "metric": METRIC, "unit": "particle-steps/s", "particles": npart}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        hot = HotPath(local)
+        hot.set_groups(case.groups.wl)
+        hot.set_grid(case.grid.xarr, case.grid.vxarr, case.grid.vol, case.grid.divv)
+        hot.set_ions(A.ion, float(case.gas.temp[0]))
+        g = case.gas
+        nel, oc, ginv, _ = hot.saha_eos(g.temp, g.natom, case.grid.vol, g.natomfr, np.ones(case.grid.nx), acc=1e-10,
+                                        noc=A.ion.nstage - 1)
+        cz = dataclasses.replace(case, gas=dataclasses.replace(g, nelec=nel, oc=oc, ginv=ginv,
+                                                               ion_ni=np.ascontiguousarray(A.ion.ni, np.int32)))
+        ts = DeviceTimestep(hot, cz, params, npart=npart, precision=prec)
+        emit, _ = hot.sourceenergy(g.temp, L_BOL)
+        nvol, _ = hot.sourcenumbers(emit, npart, npart)
+        seed0 = 7000 + 1000 * rank
+        for k in range(2):  # untimed step (and the autotuner), then the timed one
+            hot.interior_source(ts.gas["temp"], emit, nvol, ts.prt, ts.isv, seed=seed0 + 2 * k)
+            e0, e1 = _events()
+            e2, e3 = _events()
+            e0.record(ts.stream)
+            ts.opacity()
+            ts.coefficients()
+            if k == 0:
+                ts.autotune(seed=seed0, nsample=1_000_000)
+            e2.record(ts.stream)
+            ts.transport(seed0 + 2 * k + 1)
+            e3.record(ts.stream)
+            ts.fluxtally()
+            e1.record(ts.stream)
+            c = ts.sync()
+        st = int(c["nstepimc"] + c["nstepddmc"])
+        out[name] = {"value": st / (e2.elapsed_time(e3) / 1e3), "particle_steps": st,
+                     "ms_particle_loop": e2.elapsed_time(e3),
+                     "ms_step_after_sources": e0.elapsed_time(e1),
+                     "steps_per_particle": st / max(int(c["npckt"]), 1)}
+        hot.close()
+        del ts
+        torch.cuda.empty_cache()
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
 
 
 # ------------------------------------------------------------------ opacity forward / adjoint
 OPACITY_SIZES = {1: (256, 2000, 500_000), 4: (4096, 10000, 2_000_000)}
 
 
-def opacity_measure(local, reps=5, which=1):
+def opacity_measure(local, reps=5, which=1, exp_per_s=None):
     """Opacity build of the opacity case (which=1: 256 shells x 2000 groups x
-    5e5 lines) or the opacity case at scale (which=4: 4096 x 10000 x 2e6), Saha populations,
-    FP64, forward and reverse through the device C ABI
+    5e5 lines) or the opacity case at scale (which=4: 4096 x 10000 x 2e6) on the
+    reference's Verner, Sutherland and data.ion tables (Saha populations of
+    every bound stage), FP64, forward and reverse through the device C ABI
     (slg_dev_opacity_grad_forward / _backward): cell-group evaluations per
-    second of each, timed with CUDA events on the library's stream."""
+    second of each, timed with CUDA events on the library's stream.
+    exp_per_s: the measured FP64 exp rate (one exp per line-shell term is the
+    kernels' binding work)."""
+    import numpy as np
     import torch
     from superlite_b200 import HotPath, workloads as W
     from superlite_b200.capi import ptr
     ncell, ngroup, nline = OPACITY_SIZES[which]
-    case = W.opacity_case(ncell=ncell, ng=ngroup, nline=nline, seed=SEED_CASE, t_days=T_DAYS)
+    A = W.load_atomic_data(ATOMIC_NPZ)
+    case = W.opacity_case(ncell=ncell, ng=ngroup, nline=nline, seed=SEED_CASE, t_days=T_DAYS, tables=A.tables)
     hot = HotPath(local)
     hot.set_groups(case.groups.wl)
     hot.set_grid(case.grid.xarr, case.grid.vxarr, case.grid.vol, case.grid.divv)
     g = case.gas
-    hot.set_atomic_data(g.ion_ni, g.oc.shape[1], case.lines, case.bf_ph1, case.bf_ph2, case.ff_gff)
-    hot.set_ions(W.ion_table(), float(g.temp[0]))
+    hot.set_atomic_data(np.ascontiguousarray(A.ion.ni, dtype=np.int32), A.ion.nstage - 1, case.lines, case.bf_ph1,
+                        case.bf_ph2, case.ff_gff)
+    hot.set_ions(A.ion, float(g.temp[0]))
     m = np.ascontiguousarray([W.ELEM_MASS.get(z, 2.0 * z) for z in range(1, W.NELEM + 1)], dtype=np.float64)
     hot._check(hot.lib.slg_set_element_masses(hot.h, len(m), ptr(m)))
     dev = torch.device("cuda", local)
@@ -701,9 +990,16 @@ def opacity_measure(local, reps=5, which=1):
         out[name] = {"ms": ms, "cell_group_evals_per_s": nc * ng / (ms / 1e3)}
     hot.close()
     lines_bytes = 16 * len(case.lines)
-    out["workload"] = f"opacity: {ncell} shells x {ngroup} groups x {nline:.0e} lines, Saha populations, " \
-                      "FP64 (forward: EOS + bb/bf/ff + means + leakage; backward: adjoint of all of it)"
+    out["workload"] = f"opacity: {ncell} shells x {ngroup} groups x {nline:.0e} synthetic lines, the reference's " \
+                      "Verner, Sutherland and data.ion tables, Saha populations, FP64 (forward: EOS + bb/bf/ff + " \
+                      "means + leakage; backward: adjoint of all of it)"
     out["line_shell_terms_per_s"] = {k: nline * ncell / (out[k]["ms"] / 1e3) for k in ("forward", "backward")}
+    if exp_per_s:
+        out["fp64_exp_roof"] = {
+            "peak_exp_per_s": exp_per_s,
+            "frac": {k: out["line_shell_terms_per_s"][k] / exp_per_s for k in ("forward", "backward")},
+            "basis": "line-shell terms/s (one FP64 exp each, the dominant work) / measured FP64 exp rate "
+                     "(slg_pipe_throughput); the whole build's time in the denominator"}
     out["bound"] = "FP64 issue (one exp per line-shell term), not HBM: the algorithmic bytes " \
                    f"({(lines_bytes + 8 * nc * ng * 3) / 1e6:.0f} MB: lines, cap64, dL/dcap) take " \
                    f"{(lines_bytes + 8 * nc * ng * 3) / (measured_peaks()[0] * 1e9) * 1e3:.4f} ms at the measured " \
@@ -799,7 +1095,9 @@ def run_opacity(a):
     import torch
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    r = opacity_measure(local, reps=a.steps, which=4)
+    from superlite_b200 import peaks as PK
+    pipes = PK.measure(local)
+    r = opacity_measure(local, reps=a.steps, which=4, exp_per_s=pipes["fp64_exp_per_s"]["value"])
     res = {"metric": "opacity cell-group evals/s", "value": r["backward"]["cell_group_evals_per_s"],
            "unit": "cell-group evals/s", "n_gpus": 1, "steps": a.steps, "warmup": 3,
            "ms_per_step": r["forward"]["ms"] + r["backward"]["ms"], "higher_is_better": True, "scaling": "weak",

@@ -94,7 +94,8 @@ int slg_set_grid(slg_ctx* ctx, int32_t nx, const double* xarr, const double* vxa
  * renormalises each model to L_bol, slg_models_sourcenumbers fills each
  * model's slots, interior_source writes each model's particles into its own
  * slots, fluxtally returns one row of flx_ng groups per model, and transport
- * (precision 1 only) advances all models' particles in one persistent launch.
+ * (either precision) advances all models' particles in one persistent launch
+ * (per-particle traces, slg_set_trace, are for one-model contexts).
  * Random numbers: model m draws under the key seed + m * SLG_MODEL_SEED_STRIDE
  * with slot numbers counted from the model's first slot, so each model
  * reproduces its own single-model run under that key. */
@@ -421,6 +422,16 @@ int slg_transport_totals(slg_ctx* ctx, slg_transport_out* out, int32_t reset);
 int slg_sync(slg_ctx* ctx);
 /* The context's cudaStream_t, as an opaque handle. */
 void* slg_stream(slg_ctx* ctx);
+
+/* ------------------------------------------------------------------ pipe throughput */
+/* Throughput microbenchmark of one pipe of device `device` (no counterpart in
+ * the reference; the denominators of the kernels' rooflines): which = 0 FP64
+ * fused multiply-add (flop/s, 2 per FMA), 1 FP64 exp (evaluations/s), 2 FP32
+ * fused multiply-add (flop/s), 3 32-bit integer multiply-add (operations/s).
+ * One launch of 8 blocks x 256 threads per SM, `iters` rounds of independent
+ * chains per thread, timed with CUDA events after one warm-up launch; *ms
+ * (optional) receives the launch time.  Allocates and frees its own buffer. */
+int slg_pipe_throughput(int device, int which, int iters, double* ops_per_s, float* ms);
 
 #ifdef __cplusplus
 }

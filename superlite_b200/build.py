@@ -20,7 +20,7 @@ OUT = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT, "libslg.so")
 
 FP64_SOURCES = ["opacity.cu", "grid.cu", "transport.cu", "source.cu", "capi.cu", "noalloc.cu", "eos.cu",
-                "adjoint.cu"]
+                "adjoint.cu", "peaks.cu"]
 MIXED_SOURCES = ["transport_mixed.cu"]
 HEADERS = ["slg_device.cuh", "slg_internal.h", "transport_impl.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -103,6 +103,7 @@ SIGNATURES = {
     "slg_graph_launch": (C.c_int, [vp, C.c_int32]),
     "slg_transport_totals": (C.c_int, [vp, vp, C.c_int32]),
     "slg_stream": (vp, [vp]),
+    "slg_pipe_throughput": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
 }
 
 _LIB = None

@@ -480,8 +480,6 @@ int slg_dev_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packe
   if (ctx->nx < 2) return set_error(ctx, SLG_ERR_ARG, "transport needs at least 2 shells");
   if (in->precision != 0 && in->precision != 1)
     return set_error(ctx, SLG_ERR_NOT_BUILT, "precision %d not available", in->precision);
-  if (ctx->nmodel > 1 && in->precision != 1)
-    return set_error(ctx, SLG_ERR_NOT_BUILT, "transport of several models needs precision 1");
   if (check_model_particles(ctx, npart)) return SLG_ERR_ARG;
   cudaSetDevice(ctx->device);
   const int rc = launch_particle_advance(ctx, in, prt, isvacant, npart, seed, out, nullptr, nullptr);
@@ -638,8 +636,6 @@ int slg_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packet* p
   if (ctx->nx < 2) return set_error(ctx, SLG_ERR_ARG, "transport needs at least 2 shells");
   if (in->precision != 0 && in->precision != 1)
     return set_error(ctx, SLG_ERR_NOT_BUILT, "precision %d not available", in->precision);
-  if (ctx->nmodel > 1 && in->precision != 1)
-    return set_error(ctx, SLG_ERR_NOT_BUILT, "transport of several models needs precision 1");
   if (check_model_particles(ctx, npart)) return SLG_ERR_ARG;
   cudaSetDevice(ctx->device);
   const size_t nc = ctx->nx, ng = ctx->ng, np = (size_t)npart;
@@ -658,6 +654,8 @@ int slg_particle_advance(slg_ctx* ctx, const slg_transport_in* in, slg_packet* p
   o.jrad = out_buf<double>(ctx, H_J, nc * ng, &rc);
   o.eamp = out_buf<double>(ctx, H_K, nc, &rc);
   o.methodswap = out_buf<int32_t>(ctx, H_L, nc, &rc);
+  if (ctx->nmodel > 1 && (ctx->trace_hash || ctx->trace_nstep))
+    return set_error(ctx, SLG_ERR_ARG, "per-particle traces are for one-model contexts");
   uint64_t* dth = ctx->trace_hash ? out_buf<uint64_t>(ctx, H_M, np, &rc) : nullptr;
   int32_t* dtn = ctx->trace_nstep ? out_buf<int32_t>(ctx, H_N, np, &rc) : nullptr;
   if (!rc && dth) cudaMemsetAsync(dth, 0, sizeof(uint64_t) * np, ctx->stream);
@@ -732,8 +730,6 @@ int slg_autotune_transport(slg_ctx* ctx, const slg_transport_in* in, const slg_p
   if (!need_grid(ctx) || ctx->nx < 2) return set_error(ctx, SLG_ERR_STATE, "groups/grid not set");
   if (in->precision != 0 && in->precision != 1)
     return set_error(ctx, SLG_ERR_NOT_BUILT, "precision %d not available", in->precision);
-  if (ctx->nmodel > 1 && in->precision != 1)
-    return set_error(ctx, SLG_ERR_NOT_BUILT, "transport of several models needs precision 1");
   cudaSetDevice(ctx->device);
   int b = 0;
   const int rc = autotune_transport(ctx, in, prt, isvacant, npart, seed, nsample, &b, ms);

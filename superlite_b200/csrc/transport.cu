@@ -47,7 +47,11 @@ __device__ inline void store_flux_packet(slg_packet* p, double mu, double e, dou
 // allocator: 1 -> up to 255 registers (the compiler settles on 128),
 // 5 -> 96, 6 -> 80, 8 -> 64 registers with some spilling.  The autotuner
 // (slg_autotune_transport) picks the fastest on the caller's workload.
-template <bool TRACE, int MINB>
+// MODELS: the slots belong to several independent models (slg_set_models);
+// each particle finds its model once, draws from its model's random key with
+// the model-local slot as counter (as the model would alone), and tallies
+// into its model's cells.
+template <bool TRACE, int MINB, bool MODELS = false>
 __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const TrnArgs A) {
   __shared__ unsigned long long s_cnt[20];
   __shared__ double s_sum[3];
@@ -69,6 +73,8 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
   const uint32_t sw = A.epoch ? (uint32_t)(*A.epoch << 2) : 0u;
   int istep = 0;
   uint64_t h = 0;
+  // the current particle's model: shells, first cell, first shell edge
+  int vnx = A.nx, vco = 0, vxo = 0;
   // register caches of the tallies
   int t_ic = 0;
   double t_acc = 0.0;
@@ -100,8 +106,25 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
             double x, y, z, mu, om, e, e0, wl;
             load_packet(A.prt + ip, x, y, z, mu, om, e, e0, wl);
             atomicAdd(&s_cnt[0], 1ull);
+            int m = 0;
+            long long poff = 0;
+            if (MODELS) {  // models own consecutive slot ranges
+              int lo = 0, hi = A.nmodel - 1;
+              while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(&A.models[mid].poff) <= ip) lo = mid;
+                else hi = mid - 1;
+              }
+              m = lo;
+              poff = __ldg(&A.models[m].poff);
+              vnx = __ldg(&A.models[m].nx);
+              vco = __ldg(&A.models[m].co);
+              vxo = __ldg(&A.models[m].xo);
+            }
+            const double* X = A.xarr + vxo;
+            const double* VX = A.vxarr + vxo;
             p.x = x; p.mu = mu; p.e = e; p.e0 = e0; p.wl = wl; p.dist = 0.0;
-            p.ix = binsrch(x, A.xarr, A.nx + 1, false);
+            p.ix = binsrch(x, X, vnx + 1, false);
             p.ig = binsrch(wl, A.wl, A.ng + 1, false);
             if (p.ix < 1 || p.ig < 1) {  // NaN position or wavelength: library code 1002
               if (A.errorfatal) atomicMin(&A.acc->ierr_key, ((unsigned long long)(ip + 1) << 32) | 1002u);
@@ -110,11 +133,10 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
               p.ig = 1;
             }
             const bool bad = A.isvacant[ip] != 0;
-            const double help = dxd(A, p.ix);
-            const double tau = (A.sig[p.ix - 1] + CAPd(A, p.ig, p.ix)) * help;
+            const double help = dxv(X, p.ix);
+            const double tau = (A.sig[vco + p.ix - 1] + CAPd(A, p.ig, vco + p.ix)) * help;
             p.itype = (A.puretran || tau < A.tauddmc) ? 1 : 2;
-            p.vx = (A.vxarr[p.ix - 1] * (A.xarr[p.ix] - x) + A.vxarr[p.ix] * (x - A.xarr[p.ix - 1])) /
-                   (A.xarr[p.ix] - A.xarr[p.ix - 1]);
+            p.vx = (VX[p.ix - 1] * (X[p.ix] - x) + VX[p.ix] * (x - X[p.ix - 1])) / (X[p.ix] - X[p.ix - 1]);
             if (p.itype == 1) {
               const double labfact = 1.0 - p.vx * p.mu / pc_c;
               p.wl = p.wl * labfact;
@@ -126,7 +148,7 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
             istep = 0;
             nd_p = 0;
             nsw_p = 0;
-            rng.init(A.seed, (uint64_t)ip, sw);
+            rng.init(A.seed + (unsigned long long)m * kModelSeedStride, (uint64_t)(ip - poff), sw);
             if (TRACE) h = 1469598103934665603ull;
             have = !bad;
           }
@@ -137,11 +159,12 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
     if (!have) continue;
     // ---- one event, particle_advance.f90:204-268
     istep++;
-    const int icold = p.ix, igold = p.ig;
+    const MView v{vnx, vco, vxo};
+    const int icold = vco + p.ix, igold = p.ig;  // cell over all models, 1-based
     double eraddens, jrad, eamp = 0.0;
     int ierr;
     if (p.itype == 1 || A.puretran) {
-      transport11_dev(A, p, rng, eraddens, eamp, jrad, evelo, ierr);
+      transport11_dev(A, v, p, rng, eraddens, eamp, jrad, evelo, ierr);
       if (p.itype != 1) {
         nsw_p++;
         if (A.dogrdtally) atomicAdd(&A.methodswap[icold - 1], 1);
@@ -149,7 +172,7 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
       if (!A.noampfact && eamp != 0.0) atomicAdd(&A.eamp[icold - 1], eamp);
     } else {
       nd_p++;
-      diffusion11_dev(A, p, rng, eraddens, jrad, evelo, ierr);
+      diffusion11_dev(A, v, p, rng, eraddens, jrad, evelo, ierr);
       if (p.itype == 1) {
         nsw_p++;
         if (A.dogrdtally) atomicAdd(&A.methodswap[icold - 1], 1);
@@ -182,7 +205,7 @@ __global__ void __launch_bounds__(TRN_BLOCK, MINB) particle_advance_kernel(const
       h = fnv_mix(h, p.stat);
     }
     if (p.itype == 1 && p.stat == 0) {
-      if (p.x > A.xarr[p.ix] || p.x < A.xarr[p.ix - 1] || p.x != p.x) {
+      if (p.x > A.xarr[vxo + p.ix] || p.x < A.xarr[vxo + p.ix - 1] || p.x != p.x) {
         if (ierr == 0) ierr = -99;
       }
     }
@@ -312,25 +335,36 @@ __global__ void sourcetally_kernel(long long npart, const slg_packet* __restrict
   }
 }
 
-template <bool TRACE, int MINB>
+template <bool TRACE, int MINB, bool MODELS = false>
 int launch_one(int num_sms, long long npart, cudaStream_t st, const TrnArgs& A) {
   static int occ = -1;  // resident blocks per SM, queried once (not during a capture)
-  if (occ < 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_kernel<TRACE, MINB>, TRN_BLOCK, 0);
+  if (occ < 0)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, particle_advance_kernel<TRACE, MINB, MODELS>, TRN_BLOCK, 0);
   long long nblk = (long long)num_sms * (occ > 0 ? occ : 4);
   const long long need = (npart + TRN_BLOCK - 1) / TRN_BLOCK;
   if (need < nblk) nblk = need > 0 ? need : 1;
-  particle_advance_kernel<TRACE, MINB><<<(unsigned)nblk, TRN_BLOCK, 0, st>>>(A);
+  particle_advance_kernel<TRACE, MINB, MODELS><<<(unsigned)nblk, TRN_BLOCK, 0, st>>>(A);
   return cudaPeekAtLastError() == cudaSuccess ? SLG_OK : SLG_ERR_CUDA;
 }
 
 }  // namespace
 
 int launch_transport_mixed(int variant, int num_sms, long long npart, cudaStream_t st, const TrnArgs& A);
+int launch_mix_rate_tables(cudaStream_t st, int nc, const int4* cellmap, const TrnArgs& A, float4* mrate,
+                           float* emit32, int16_t* eguide);
 constexpr int kMixedVariants = 4;
 
 // Transport kernel variants (register budget / resident blocks), see MINB.
 constexpr int kTransportVariants = 4;
 int launch_transport_variant(int v, bool trace, int num_sms, long long npart, cudaStream_t st, const TrnArgs& A) {
+  if (A.nmodel > 1) {  // several models: no per-event trace
+    switch (v) {
+      case 1: return launch_one<false, 5, true>(num_sms, npart, st, A);
+      case 2: return launch_one<false, 6, true>(num_sms, npart, st, A);
+      case 3: return launch_one<false, 8, true>(num_sms, npart, st, A);
+      default: return launch_one<false, 1, true>(num_sms, npart, st, A);
+    }
+  }
   switch (v) {
     case 1: return trace ? launch_one<true, 5>(num_sms, npart, st, A) : launch_one<false, 5>(num_sms, npart, st, A);
     case 2: return trace ? launch_one<true, 6>(num_sms, npart, st, A) : launch_one<false, 6>(num_sms, npart, st, A);
@@ -430,7 +464,18 @@ int build_mix_cells(slg_ctx* ctx, const slg_transport_in* in, TrnArgs& A) {
                                                             in->tempinv, in->opaclump, ctx->tables.scal,
                                                             ctx->tables.nlump, rec);
   A.mcell = rec;
-  return cuda_check(ctx, cudaGetLastError(), "mix_cell_kernel");
+  int rc = cuda_check(ctx, cudaGetLastError(), "mix_cell_kernel");
+  if (rc) return rc;
+  // per (cell, group) DDMC rates and per-cell emission CDFs (scratch slots 81-83)
+  auto* mrate = (float4*)scratch(ctx, 81, sizeof(float4) * n);
+  auto* emit32 = (float*)scratch(ctx, 82, sizeof(float) * n);
+  auto* eguide = (int16_t*)scratch(ctx, 83, sizeof(int16_t) * (size_t)nc * (T.guide_m + 1));
+  if (!mrate || !emit32 || !eguide) return SLG_ERR_OOM;
+  A.mrate = mrate;
+  A.emit32 = emit32;
+  A.eguide = eguide;
+  rc = launch_mix_rate_tables(ctx->stream, nc, ctx->nmodel > 1 ? ctx->d_cellmap : nullptr, A, mrate, emit32, eguide);
+  return rc ? set_error(ctx, rc, "mixed rate tables: %s", cudaGetErrorString(cudaGetLastError())) : SLG_OK;
 }
 
 TrnArgs transport_args(slg_ctx* ctx, const slg_transport_in* in, slg_packet* prt, int32_t* isvacant,

@@ -35,11 +35,27 @@ struct TrnArgs {
   int smem_cells = 0;                         // tally cells kept in shared memory (mixed kernel; 0: global)
   const ModelDesc* models = nullptr;
   const MixCell* mcell = nullptr;  // per-cell records (mixed-precision kernel)
+  // mixed-precision kernel: per (cell, group) DDMC branch rates of an unlumped
+  // group, {doplump, opacleak(1), opacleak(2), (1 - emitlump) caplump}, with
+  // sentinels and neighbour flags (see mix_rate_kernel); per cell the emission
+  // CDF over groups divided by capgrey, and its guide table (T.guide_m + 1
+  // entries per cell)
+  const float4* mrate = nullptr;
+  const float* emit32 = nullptr;
+  const int16_t* eguide = nullptr;
 };
 
 struct Ptcl {
   double x, mu, e, e0, wl, vx, dist;
   int ix, ig, itype, stat, idist;  // ic == ix (1-D, no void cells)
+};
+
+// The particle's model: shells nx, first cell co (0-based over every model's
+// cells), first shell edge xo of xarr/vxarr.  A one-model grid is {A.nx, 0, 0}.
+// ix/ic inside the event bodies stay 1-based shells of the particle's model;
+// per-cell arrays are read at co + ic, edges at xo + ix.
+struct MView {
+  int nx, co, xo;
 };
 
 // first_gt: first position q in [0,n) with a[q] > r, else n-1 (the last
@@ -124,6 +140,7 @@ __device__ inline double CAPd(const TrnArgs& A, int ig, int ic) {
   return (double)__ldg(A.cap + (size_t)(ic - 1) * A.ng + (ig - 1));
 }
 __device__ inline double dxd(const TrnArgs& A, int i) { return A.xarr[i] - A.xarr[i - 1]; }
+__device__ inline double dxv(const double* X, int i) { return X[i] - X[i - 1]; }
 
 // GRID/emitgroup.f:3-54 (LTE); ic 1-based.
 __device__ inline int emitgroup_dev(const TrnArgs& A, double r, int ic) {
@@ -147,8 +164,8 @@ __device__ inline int emitgroup_dev(const TrnArgs& A, double r, int ic) {
 
 // One IMC event, transport11.f90:3-515.
 template <class RNG>
-__device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, double& eraddens, double& eamp,
-                                       double& jrad, double& totevelo, int& ierr) {
+__device__ inline void transport11_dev(const TrnArgs& A, const MView& v, Ptcl& p, RNG& rng, double& eraddens,
+                                       double& eamp, double& jrad, double& totevelo, int& ierr) {
   int& ix = p.ix;
   int& ig = p.ig;
   double& x = p.x;
@@ -158,15 +175,18 @@ __device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
   double& wl = p.wl;
   double& vx = p.vx;
   const int ic = ix;
+  const double* const X = A.xarr + v.xo;  // this model's shell edges
+  const double* const VX = A.vxarr + v.xo;
+  const int cb = v.co;                   // this model's first cell
   ierr = 0;
   eraddens = 0.0;
   eamp = 0.0;
   jrad = 0.0;
   double elabfact = 1.0 - mu * vx * cinv;
   const double elabfactold = elabfact;
-  const double* sc = A.T.scal + (size_t)SCAL_N * (ic - 1);
+  const double* sc = A.T.scal + (size_t)SCAL_N * (cb + ic - 1);
   const double far = sc[SCAL_FAR];
-  const double Xa = A.xarr[ix - 1], Xb = A.xarr[ix];
+  const double Xa = X[ix - 1], Xb = X[ix];
   double db;
   int ixnext;
   if (ix == 1 || mu >= -sqrt(1.0 - sq(Xa / x))) {
@@ -177,7 +197,7 @@ __device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
     ixnext = ix - 1;
   }
   if (db != db) { ierr = 1; return; }
-  const double sigc = A.sig[ic - 1];
+  const double sigc = A.sig[cb + ic - 1];
   double dthm, dcol, ddop, r1, r2, help;
   if (sigc > 0.0) {
     r1 = rng.draw();
@@ -185,7 +205,7 @@ __device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
   } else {
     dthm = far;
   }
-  const double capc = CAPd(A, ig, ic);
+  const double capc = CAPd(A, ig, cb + ic);
   if (capc <= 0.0) {
     dcol = far;
   } else {
@@ -193,7 +213,7 @@ __device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
     dcol = -log(r1) / (elabfact * capc);
   }
   const double dvdr = sc[SCAL_DVDR];
-  const double vhelp = A.vxarr[ix - 1] - dvdr * Xa;
+  const double vhelp = VX[ix - 1] - dvdr * Xa;
   if (fabs(vx - vhelp) / pc_c >= 0.1) {
     // Newton-Raphson Doppler distance (transport11.f90:159-199)
     const double epstol = 1e-3;
@@ -223,9 +243,9 @@ __device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
     if (ddop <= 0.0 || it == 100) ddop = far;
   } else {
     if (dvdr > 0.0 && ig < A.ng) {
-      ddop = 3.0 * pc_c / A.divv[ix - 1] * (elabfact - wl * A.wlinv[ig]);
+      ddop = 3.0 * pc_c / A.divv[cb + ix - 1] * (elabfact - wl * A.wlinv[ig]);
     } else if (dvdr < 0.0 && ig > 1) {
-      ddop = 3.0 * pc_c / A.divv[ix - 1] * (elabfact - wl * A.wlinv[ig - 1]);
+      ddop = 3.0 * pc_c / A.divv[cb + ix - 1] * (elabfact - wl * A.wlinv[ig - 1]);
     } else {
       ddop = far;
     }
@@ -243,15 +263,15 @@ __device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
   if (d < 0.0) { ierr = 4; return; }
   const double xold = x;
   x = sqrt(sq(x) + sq(d) + 2.0 * d * x * mu);
-  vx = (A.vxarr[ix - 1] * (Xb - x) + A.vxarr[ix] * (x - Xa)) / dxd(A, ix);
+  vx = (VX[ix - 1] * (Xb - x) + VX[ix] * (x - Xa)) / dxv(X, ix);
   if (x == 0.0) mu = 1.0;
   else mu = (xold * mu + d) / x;
   eraddens = e * sq(elabfact) * d * cinv;
   jrad = pc_c * eraddens;
   elabfact = 1.0 - mu * vx * cinv;
-  if (x < A.xarr[0]) {
-    x = A.xarr[0];
-    vx = A.vxarr[0];
+  if (x < X[0]) {
+    x = X[0];
+    vx = VX[0];
     ix = 1;
     r1 = rng.draw();
     mu = 1.0 - r1;
@@ -280,7 +300,7 @@ __device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
   } else if (d == db) {
     // transport11.f90:290-295.  A grazing exit through the outer edge can leave
     // mu a rounding error below 0; the reference would then index shell nx+1.
-    if ((mu >= 0.0 && ix == A.nx) || ixnext > A.nx) { p.stat = 1; return; }
+    if ((mu >= 0.0 && ix == v.nx) || ixnext > v.nx) { p.stat = 1; return; }
   }
   if (d == dthm) {
     wl = wl * (1.0 - mu * vx * cinv) / elabfact;
@@ -296,8 +316,8 @@ __device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
     e0 = e0 * help;
     if (A.ng != 1) {
       r1 = rng.draw();
-      ig = emitgroup_dev(A, r1, ic);
-      if (((sigc + CAPd(A, ig, ic)) * dxd(A, ix) >= A.tauddmc) && !A.puretran) p.itype = 2;
+      ig = emitgroup_dev(A, r1, cb + ic);
+      if (((sigc + CAPd(A, ig, cb + ic)) * dxv(X, ix) >= A.tauddmc) && !A.puretran) p.itype = 2;
     }
     if (p.itype == 2) {
       totevelo = totevelo + e * vx * mu * cinv;
@@ -310,11 +330,11 @@ __device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
     }
   } else if (d == db && ixnext > ix) {
     const int l = ix + 1;
-    const double capl = CAPd(A, ig, l), sigl = A.sig[l - 1];
-    const double dxl = dxd(A, ix + 1);
+    const double capl = CAPd(A, ig, cb + l), sigl = A.sig[cb + l - 1];
+    const double dxl = dxv(X, ix + 1);
     if ((sigl + capl) * dxl < A.tauddmc || A.puretran) {
-      x = A.xarr[ix];
-      vx = A.vxarr[ix];
+      x = X[ix];
+      vx = VX[ix];
       ix = ix + 1;
     } else {
       mu = (mu - vx * cinv) / (1.0 - vx * mu * cinv);
@@ -333,17 +353,17 @@ __device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
         r2 = rng.draw();
         mu = -(r1 > r2 ? r1 : r2);
         mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
-        x = A.xarr[ix];
-        vx = A.vxarr[ix];
+        x = X[ix];
+        vx = VX[ix];
       }
     }
   } else if (d == db) {
     const int l = ix - 1;
-    const double capl = CAPd(A, ig, l), sigl = A.sig[l - 1];
-    const double dxl = dxd(A, ix - 1);
+    const double capl = CAPd(A, ig, cb + l), sigl = A.sig[cb + l - 1];
+    const double dxl = dxv(X, ix - 1);
     if ((sigl + capl) * dxl < A.tauddmc || A.puretran) {
-      x = A.xarr[ix - 1];
-      vx = A.vxarr[ix - 1];
+      x = X[ix - 1];
+      vx = VX[ix - 1];
       ix = ix - 1;
     } else {
       mu = (mu - vx * cinv) / (1.0 - vx * mu * cinv);
@@ -372,8 +392,8 @@ __device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
         r2 = rng.draw();
         mu = r1 > r2 ? r1 : r2;
         mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
-        x = A.xarr[ix - 1];
-        vx = A.vxarr[ix - 1];
+        x = X[ix - 1];
+        vx = VX[ix - 1];
       }
     }
   } else if (d == ddop) {
@@ -396,7 +416,7 @@ __device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
         wl = wl * elabfact;
       }
     }
-    if (((sigc + CAPd(A, ig, ic)) * dxd(A, ix) >= A.tauddmc) && !A.puretran) {
+    if (((sigc + CAPd(A, ig, cb + ic)) * dxv(X, ix) >= A.tauddmc) && !A.puretran) {
       p.itype = 2;
       totevelo = totevelo + e * vx * mu * cinv;
       e = e * elabfact;
@@ -410,8 +430,8 @@ __device__ inline void transport11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
 
 // One DDMC event, diffusion11.f90:3-633 (LTE).
 template <class RNG>
-__device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, double& eraddens, double& jrad,
-                                       double& totevelo, int& ierr) {
+__device__ inline void diffusion11_dev(const TrnArgs& A, const MView& v, Ptcl& p, RNG& rng, double& eraddens,
+                                       double& jrad, double& totevelo, int& ierr) {
   const int ng = A.ng;
   int& ix = p.ix;
   int& ig = p.ig;
@@ -422,20 +442,23 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
   double& wl = p.wl;
   double& vx = p.vx;
   const int ic = ix;
+  const double* const X = A.xarr + v.xo;  // this model's shell edges
+  const double* const VX = A.vxarr + v.xo;
+  const int cb = v.co;                   // this model's first cell
   ierr = 0;
   eraddens = 0.0;
   jrad = 0.0;
-  const double Xa = A.xarr[ix - 1], Xb = A.xarr[ix];
+  const double Xa = X[ix - 1], Xb = X[ix];
   const double dist = Xb - Xa;
-  const size_t off = (size_t)(ic - 1) * ng;
-  const double* sc = A.T.scal + (size_t)SCAL_N * (ic - 1);
+  const size_t off = (size_t)(cb + ic - 1) * ng;
+  const double* sc = A.T.scal + (size_t)SCAL_N * (cb + ic - 1);
   const double dx3 = sc[SCAL_DX3];
   const double capgreyinv = sc[SCAL_CAPGREYINV];
-  const double sigc = A.sig[ic - 1];
-  const double capc = CAPd(A, ig, ic);
-  const double tinv = A.tempinv[ic - 1];
-  const double divv = A.divv[ix - 1];
-  const int glump = (capc * dist >= A.taulump) ? A.T.nlump[ic - 1] : 0;
+  const double sigc = A.sig[cb + ic - 1];
+  const double capc = CAPd(A, ig, cb + ic);
+  const double tinv = A.tempinv[cb + ic - 1];
+  const double divv = A.divv[cb + ix - 1];
+  const int glump = (capc * dist >= A.taulump) ? A.T.nlump[cb + ic - 1] : 0;
   if ((sigc + capc) * dist < A.tauddmc) { ierr = 100; return; }
   double emitlump, caplump, doplump, r1, r2, help;
   double o1, o2;
@@ -443,7 +466,7 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
     emitlump = sc[SCAL_EMITLUMP];
     caplump = sc[SCAL_CAPLUMP];
     doplump = sc[SCAL_DOPLUMP];
-    const double* OL = A.opaclump + (size_t)11 * (ic - 1);
+    const double* OL = A.opaclump + (size_t)11 * (cb + ic - 1);
     o1 = OL[0];
     o2 = OL[1];
   } else {
@@ -461,8 +484,8 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       o1 = 0.0;
     } else {
       const int l = ix - 1;
-      const double capl = CAPd(A, ig, l), sigl = A.sig[l - 1];
-      const double dxl = Xa - A.xarr[ix - 2];
+      const double capl = CAPd(A, ig, cb + l), sigl = A.sig[cb + l - 1];
+      const double dxl = Xa - X[ix - 2];
       if ((capl + sigl) * dxl < A.tauddmc) {
         const double mfphelp = (capc + sigc) * dist;
         const double ppl = 4.0 / (3.0 * mfphelp + 6.0 * pc_dext);
@@ -474,13 +497,13 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
     }
     bool lhelp;
     double capl = 0.0, sigl = 0.0, dxl = 0.0;
-    if (ix == A.nx) {
+    if (ix == v.nx) {
       lhelp = true;
     } else {
       const int l = ix + 1;
-      capl = CAPd(A, ig, l);
-      sigl = A.sig[l - 1];
-      dxl = A.xarr[ix + 1] - Xb;
+      capl = CAPd(A, ig, cb + l);
+      sigl = A.sig[cb + l - 1];
+      dxl = X[ix + 1] - Xb;
       lhelp = (capl + sigl) * dxl < A.tauddmc;
     }
     if (lhelp) {
@@ -510,7 +533,7 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       iiig = ig;
     } else {
       r1 = rng.draw();
-      const int q = cdf_search(A.T, 0, ic - 1, A.T.cdf_dop + off, glump, r1);
+      const int q = cdf_search(A.T, 0, cb + ic - 1, A.T.cdf_dop + off, glump, r1);
       iiig = divv >= 0.0 ? glumps[q] : glumps[glump - 1 - q];
     }
     if (divv >= 0.0) {
@@ -522,7 +545,7 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       wl = A.wl[ig];
       ig = ig > 1 ? ig : 1;
     }
-    if ((sigc + CAPd(A, ig, ic)) * dist < A.tauddmc) {
+    if ((sigc + CAPd(A, ig, cb + ic)) * dist < A.tauddmc) {
       p.itype = 1;
       r1 = rng.draw();
       mu = 1.0 - 2.0 * r1;
@@ -530,7 +553,7 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       x = pow(r1 * cube(Xb) + (1.0 - r1) * cube(Xa), third_r4);
       x = x < Xb ? x : Xb;
       x = x > Xa ? x : Xa;
-      vx = (A.vxarr[ix - 1] * (Xb - x) + A.vxarr[ix] * (x - Xa)) / dist;
+      vx = (VX[ix - 1] * (Xb - x) + VX[ix] * (x - Xa)) / dist;
       mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
       wl = wl * (1.0 - vx * mu * cinv);
       help = 1.0 / (1.0 - vx * mu * cinv);
@@ -546,7 +569,7 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
     const bool right = r1 >= pa + pdop + pl0;
     p.idist = right ? -4 : -3;
     if (!right && ix == 1) return;
-    if (right && ix == A.nx) {
+    if (right && ix == v.nx) {
       // escape through the outer edge (:438-478)
       p.stat = 1;
       r1 = rng.draw();
@@ -554,12 +577,12 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       mu = r1 > r2 ? r1 : r2;
       if (glump != 0) {
         r1 = rng.draw();
-        ig = glumps[cdf_search(A.T, 2, ic - 1, A.T.cdf_right + off, glump, r1)];
+        ig = glumps[cdf_search(A.T, 2, cb + ic - 1, A.T.cdf_right + off, glump, r1)];
       }
       r1 = rng.draw();
       wl = 1.0 / (r1 * A.wlinv[ig] + (1.0 - r1) * A.wlinv[ig - 1]);
-      x = A.xarr[A.nx];
-      vx = A.vxarr[A.nx];
+      x = X[v.nx];
+      vx = VX[v.nx];
       mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
       mu = mu < 1.0 ? mu : 1.0;
       help = 1.0 / (1.0 - mu * vx * cinv);
@@ -574,15 +597,15 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       iiig = ig;
     } else {
       r1 = rng.draw();
-      iiig = glumps[cdf_search(A.T, right ? 2 : 1, ic - 1, (right ? A.T.cdf_right : A.T.cdf_left) + off, glump, r1)];
+      iiig = glumps[cdf_search(A.T, right ? 2 : 1, cb + ic - 1, (right ? A.T.cdf_right : A.T.cdf_left) + off, glump, r1)];
     }
-    const double dxl = right ? A.xarr[ix + 1] - Xb : Xa - A.xarr[ix - 2];
-    if ((A.sig[l - 1] + CAPd(A, iiig, l)) * dxl < A.tauddmc) {
+    const double dxl = right ? X[ix + 1] - Xb : Xa - X[ix - 2];
+    if ((A.sig[cb + l - 1] + CAPd(A, iiig, cb + l)) * dxl < A.tauddmc) {
       p.itype = 1;
       r1 = rng.draw();
       wl = 1.0 / (r1 * A.wlinv[iiig] + (1.0 - r1) * A.wlinv[iiig - 1]);
       x = right ? Xb : Xa;
-      vx = A.vxarr[right ? ix : ix - 1];
+      vx = VX[right ? ix : ix - 1];
       r1 = rng.draw();
       r2 = rng.draw();
       const double m = r1 > r2 ? r1 : r2;
@@ -602,14 +625,14 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
     if (glump == ng) { ierr = 102; return; }
     if (glump == 0) {
       r1 = rng.draw();
-      iiig = emitgroup_dev(A, r1, ic);
+      iiig = emitgroup_dev(A, r1, cb + ic);
     } else {
       r1 = rng.draw();
-      const int q = cdf_search(A.T, 3, ic - 1, A.T.cdf_scat + off, ng - glump, r1);
+      const int q = cdf_search(A.T, 3, cb + ic - 1, A.T.cdf_scat + off, ng - glump, r1);
       iiig = glumps[ng - 1 - q];
     }
     ig = iiig;
-    if ((sigc + CAPd(A, ig, ic)) * dist < A.tauddmc) {
+    if ((sigc + CAPd(A, ig, cb + ic)) * dist < A.tauddmc) {
       p.itype = 1;
       r1 = rng.draw();
       wl = 1.0 / ((1.0 - r1) * A.wlinv[ig - 1] + r1 * A.wlinv[ig]);
@@ -619,7 +642,7 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       x = pow(r1 * cube(Xb) + (1.0 - r1) * cube(Xa), third_r4);
       x = x < Xb ? x : Xb;
       x = x > Xa ? x : Xa;
-      vx = (A.vxarr[ix - 1] * (Xb - x) + A.vxarr[ix] * (x - Xa)) / dist;
+      vx = (VX[ix - 1] * (Xb - x) + VX[ix] * (x - Xa)) / dist;
       mu = (mu + vx * cinv) / (1.0 + vx * mu * cinv);
       help = 1.0 / (1.0 - vx * mu * cinv);
       totevelo = totevelo + e * (1.0 - help);
@@ -628,8 +651,8 @@ __device__ inline void diffusion11_dev(const TrnArgs& A, Ptcl& p, RNG& rng, doub
       wl = wl * (1.0 - vx * mu * cinv);
     }
   }
-  if (x < A.xarr[0]) { p.stat = 2; return; }
-  const double dv = A.divv[ix - 1];
+  if (x < X[0]) { p.stat = 2; return; }
+  const double dv = A.divv[cb + ix - 1];
   totevelo = totevelo + e * (1.0 - exp(-dv * ddmct / 3.0));
   e = e * exp(-dv * ddmct / 3.0);
   e0 = e0 * exp(-dv * ddmct / 3.0);

@@ -101,14 +101,24 @@ __device__ inline float aberrate(float mu, float b) {
   return fminf(fmaxf(m, -1.0f), 1.0f);
 }
 
-// the particle's model: shells nx, first cell co, first shell edge xo
-struct MView {
-  int nx, co, xo;
-};
-
 // opacity of group ig in cell ic (1-based over all models' cells)
 __device__ inline float capf(const TrnArgs& A, int ig, int ic) {
   return __ldg(A.cap + (size_t)(ic - 1) * A.ng + (ig - 1));
+}
+
+// Sentinels of the rate table's first component (a rate is >= 0).
+constexpr float kRateLumped = -1.0f;  // cap * dist >= taulump in a shell with lumped groups
+constexpr float kRateIMC = -2.0f;     // (sig + cap) * dist < tauddmc: IMC in this shell
+
+// emitgroup (emitgroup.f:3-54) as a search of the shell's emission CDF
+// (running sums of specint0 * cap over the groups, divided by capgrey) through
+// its guide table: the group with the same probability w_g cap_g / capgrey,
+// from one guide load and one round of loads; 1-based.
+__device__ inline int emitgroup_mix(const TrnArgs& A, int gc, float r) {
+  const float* a = A.emit32 + (size_t)gc * A.ng;
+  const int16_t* g = A.eguide + (size_t)gc * (A.T.guide_m + 1);
+  const int k = (int)(r * (float)A.T.guide_m);  // exact: guide_m is a power of two and r < 1
+  return 1 + first_gt_range32(a, g[k], g[k + 1], A.ng, r);
 }
 
 // one IMC event (transport11.f90) in mixed precision
@@ -215,7 +225,7 @@ __device__ inline void transport11_mix(const TrnArgs& A, const MView& v, PtclM& 
     p.e = p.e * help;
     p.e0 = p.e0 * help;
     if (A.ng != 1) {
-      ig = emitgroup_dev(A, (double)rng.draw(), gc + 1);
+      ig = emitgroup_mix(A, gc, rng.draw());
       if (((sigc + capf(A, ig, gc + 1)) * R.dist >= (float)A.tauddmc) && !A.puretran) p.itype = 2;
     }
     if (p.itype == 2) {
@@ -303,62 +313,27 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
   ierr = 0;
   eraddens = 0.0;
   const double Xa = R.xa, Xb = R.xb;
-  const float dist = R.dist;
   const size_t off = (size_t)gc * ng;
-  const float sigc = R.sig;
-  const float capc = capf(A, ig, gc + 1);
   const float divv = R.divv;
-  const float tau_l = (float)A.taulump, tau_d = (float)A.tauddmc;
-  const int glump = (capc * dist >= tau_l) ? R.nlump : 0;
-  if ((sigc + capc) * dist < tau_d) { ierr = 100; return; }
-  float emitlump, caplump, doplump, o1, o2;
+  // this group's rates in this shell (one 16-byte load); lumped groups take the
+  // shell's lumped values from its record
+  const float4 rt = __ldg(A.mrate + off + (ig - 1));
+  if (rt.x == kRateIMC) { ierr = 100; return; }
+  const int glump = rt.x == kRateLumped ? R.nlump : 0;
+  float doplump, o1, o2, r_scat;
   if (glump > 0) {
-    emitlump = R.emitlump;
-    caplump = R.caplump;
     doplump = R.doplump;
     o1 = R.o1;
     o2 = R.o2;
+    r_scat = glump == ng ? 0.0f : (1.0f - R.emitlump) * R.caplump;
   } else {
-    const double tinv = R.tinv;
-    emitlump = (float)(specint0(tinv, A.wlinv, ig) * R.capgreyinv * (double)capc);
-    caplump = capc;
-    const double spec_ig = A.T.specarr[off + ig - 1];
-    const double divvd = A.divv[v.co + ix - 1];
-    if (ig != ng && divv >= 0.f) doplump = (float)(dopspeccalc(tinv, A.wlinv, ig) * divvd / (spec_ig * 3.0 * pc_c));
-    else if (ig != 1 && divv < 0.f) doplump = (float)(-dopspeccalc(tinv, A.wlinv, ig - 1) * divvd / (spec_ig * 3.0 * pc_c));
-    else doplump = 0.f;
-    // x^2 / (x_b^3 - x_a^3) per face, formed in FP64
-    const float fa = R.fa, fb = R.fb;
-    if (ix == 1) {
-      o1 = 0.f;
-    } else {
-      const float capl = capf(A, ig, v.co + ix - 1), sigl = R.sigl;
-      const float dxl = R.dxl;
-      if ((capl + sigl) * dxl < tau_d) {
-        const float ppl = 4.0f / (3.0f * (capc + sigc) * dist + 6.0f * dextf);
-        o1 = 1.5f * ppl * fa;
-      } else {
-        o1 = 2.0f * fa / ((sigc + capc) * dist + (sigl + capl) * dxl);
-      }
-    }
-    bool lhelp = true;
-    float capl = 0.f, sigl = 0.f, dxl = 0.f;
-    if (ix != v.nx) {
-      capl = capf(A, ig, v.co + ix + 1);
-      sigl = R.sigr;
-      dxl = R.dxr;
-      lhelp = (capl + sigl) * dxl < tau_d;
-    }
-    if (lhelp) {
-      const float ppr = 4.0f / (3.0f * (capc + sigc) * dist + 6.0f * dextf);
-      o2 = 1.5f * ppr * fb;
-    } else {
-      o2 = 2.0f * fb / ((sigc + capc) * dist + (sigl + capl) * dxl);
-    }
+    doplump = rt.x;
+    o1 = fabsf(rt.y);  // sign bits: the neighbour is IMC in this group
+    o2 = fabsf(rt.z);
+    r_scat = rt.w;
   }
   // branch rates: Doppler, left leak, right leak, effective scatter
   const float s_dop = doplump, s_left = doplump + o1, s_leak = doplump + (o1 + o2);
-  const float r_scat = glump == ng ? 0.0f : (1.0f - emitlump) * caplump;
   const float total = s_leak + r_scat;
   const float ddmct = fabsf(__fdividef(__logf(rng.draw()), total) * cinvf);
   eraddens = p.e * (double)ddmct;
@@ -381,7 +356,7 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
       wl = (float)A.wl[ig];
       ig = ig > 1 ? ig : 1;
     }
-    if ((sigc + capf(A, ig, gc + 1)) * dist < tau_d) {
+    if (__ldg(&A.mrate[off + ig - 1].x) == kRateIMC) {
       p.itype = 1;
       mu = 1.0f - 2.0f * rng.draw();
       const double rr = (double)rng.draw();
@@ -424,8 +399,11 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
     iiig = glump == 0 ? ig
                       : glumps[cdf_search32(A.T, right ? 2 : 1, gc,
                                             (right ? A.T.cdf32_right : A.T.cdf32_left) + off, glump, rng.draw())];
-    const float dxl = right ? R.dxr : R.dxl;
-    if (((right ? R.sigr : R.sigl) + capf(A, iiig, v.co + l)) * dxl < tau_d) {
+    // IMC in the neighbour for the group that leaks: the sign bit of this
+    // group's leak rate, or the neighbour's rate sentinel for a resolved group
+    const bool to_imc = glump == 0 ? signbit(right ? rt.z : rt.y)
+                                   : __ldg(&A.mrate[(size_t)(v.co + l - 1) * ng + iiig - 1].x) == kRateIMC;
+    if (to_imc) {
       p.itype = 1;
       const float r = rng.draw();
       wl = 1.0f / (r * (float)A.wlinv[iiig] + (1.0f - r) * (float)A.wlinv[iiig - 1]);
@@ -448,13 +426,13 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
     p.idist = -2;
     if (glump == ng) { ierr = 102; return; }
     if (glump == 0) {
-      iiig = emitgroup_dev(A, (double)rng.draw(), gc + 1);
+      iiig = emitgroup_mix(A, gc, rng.draw());
     } else {
       const int q = cdf_search32(A.T, 3, gc, A.T.cdf32_scat + off, ng - glump, rng.draw());
       iiig = glumps[ng - 1 - q];
     }
     ig = iiig;
-    if ((sigc + capf(A, ig, gc + 1)) * dist < tau_d) {
+    if (__ldg(&A.mrate[off + ig - 1].x) == kRateIMC) {
       p.itype = 1;
       const float r = rng.draw();
       wl = 1.0f / ((1.0f - r) * (float)A.wlinv[ig - 1] + r * (float)A.wlinv[ig]);
@@ -480,6 +458,106 @@ __device__ inline void diffusion11_mix(const TrnArgs& A, const MView& v, PtclM& 
   totevelo = totevelo + p.e * (1.0 - decay);
   p.e = p.e * decay;
   p.e0 = p.e0 * decay;
+}
+
+// DDMC branch rates of every (cell, group), as diffusion11_mix formed them per
+// event (diffusion11.f90:154-231): for an unlumped group {doplump,
+// opacleak(1), opacleak(2), (1 - emitlump) caplump}, the Planck factors in FP64
+// rounded once, the leakage coefficients in FP32; the sign bit of opacleak(1)
+// / opacleak(2) set when the left / right neighbour is IMC in this group.  A
+// lumped group (cap dist >= taulump in a shell with lumped groups) gets
+// kRateLumped, a group with (sig + cap) dist < tauddmc kRateIMC (the sanity
+// check of :164-167).  One thread per entry; nc cells over all models.
+__global__ void mix_rate_kernel(const TrnArgs A, int nc, const int4* __restrict__ cellmap, float4* __restrict__ out) {
+  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int ng = A.ng;
+  if (k >= (size_t)nc * ng) return;
+  const int c = (int)(k / ng), ig = (int)(k - (size_t)c * ng) + 1;
+  int i = c + 1, nx = nc;
+  if (cellmap) {
+    const int4 cm = cellmap[c];
+    i = cm.x;
+    nx = cm.y;
+  }
+  const MixCell& R = A.mcell[c];
+  const float tau_l = (float)A.taulump, tau_d = (float)A.tauddmc;
+  const float capc = A.cap[k], dist = R.dist, sigc = R.sig;
+  float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+  if ((sigc + capc) * dist < tau_d) {
+    r.x = kRateIMC;
+  } else if (capc * dist >= tau_l && R.nlump > 0) {
+    r.x = kRateLumped;
+  } else {
+    const double tinv = R.tinv;
+    const float emitlump = (float)(specint0(tinv, A.wlinv, ig) * R.capgreyinv * (double)capc);
+    const double spec_ig = A.T.specarr[k];
+    const double divvd = A.divv[c];
+    float doplump;
+    if (ig != ng && R.divv >= 0.f) doplump = (float)(dopspeccalc(tinv, A.wlinv, ig) * divvd / (spec_ig * 3.0 * pc_c));
+    else if (ig != 1 && R.divv < 0.f) doplump = (float)(-dopspeccalc(tinv, A.wlinv, ig - 1) * divvd / (spec_ig * 3.0 * pc_c));
+    else doplump = 0.f;
+    float o1 = 0.f, o2;
+    bool left_imc = false, right_imc = false;
+    if (i > 1) {
+      const float capl = A.cap[k - ng];
+      if ((capl + R.sigl) * R.dxl < tau_d) {
+        const float ppl = 4.0f / (3.0f * (capc + sigc) * dist + 6.0f * dextf);
+        o1 = 1.5f * ppl * R.fa;
+        left_imc = true;
+      } else {
+        o1 = 2.0f * R.fa / ((sigc + capc) * dist + (R.sigl + capl) * R.dxl);
+      }
+    }
+    bool lhelp = true;
+    float capl = 0.f;
+    if (i != nx) {
+      capl = A.cap[k + ng];
+      lhelp = (capl + R.sigr) * R.dxr < tau_d;
+      right_imc = lhelp;
+    }
+    if (lhelp) {
+      const float ppr = 4.0f / (3.0f * (capc + sigc) * dist + 6.0f * dextf);
+      o2 = 1.5f * ppr * R.fb;
+    } else {
+      o2 = 2.0f * R.fb / ((sigc + capc) * dist + (R.sigr + capl) * R.dxr);
+    }
+    r.x = doplump;
+    r.y = left_imc ? -o1 : o1;
+    r.z = right_imc ? -o2 : o2;
+    r.w = (1.0f - emitlump) * capc;
+  }
+  out[k] = r;
+}
+
+// Emission CDF of every cell over its groups: running sums of specarr * cap in
+// group order (the order of emitprob's bins and of emitgroup's walk inside a
+// bin, emitgroup.f:3-54) divided by capgrey, in FP32, and the guide table of
+// the running sums (entry k = number of sums <= k / guide_m).  One block per cell.
+__global__ void mix_emit_kernel(const TrnArgs A, float* __restrict__ cdf, int16_t* __restrict__ guide) {
+  const int c = blockIdx.x, ng = A.ng, gm = A.T.guide_m;
+  float* a = cdf + (size_t)c * ng;
+  if (threadIdx.x == 0) {
+    const double inv = 1.0 / A.capgrey[c];
+    const double* sp = A.T.specarr + (size_t)c * ng;
+    const float* cp = A.cap + (size_t)c * ng;
+    double s = 0.0;
+    for (int g = 0; g < ng; ++g) {
+      s = s + sp[g] * (double)cp[g];
+      a[g] = (float)(s * inv);
+    }
+  }
+  __syncthreads();
+  int16_t* gd = guide + (size_t)c * (gm + 1);
+  for (int k = threadIdx.x; k <= gm; k += blockDim.x) {
+    const float v = (float)k / (float)gm;  // exact: gm is a power of two
+    int lo = 0, hi = ng;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (a[mid] <= v) lo = mid + 1;
+      else hi = mid;
+    }
+    gd[k] = (int16_t)lo;
+  }
 }
 
 template <int MINB>
@@ -691,6 +769,16 @@ int launch_mixed_one(int num_sms, long long npart, cudaStream_t st, const TrnArg
 }
 
 }  // namespace
+
+// The per-(cell, group) rate table and the emission CDF of a mixed-precision
+// launch (A.mcell, A.T.specarr and the opacities must be in place).
+int launch_mix_rate_tables(cudaStream_t st, int nc, const int4* cellmap, const TrnArgs& A, float4* mrate,
+                           float* emit32, int16_t* eguide) {
+  const size_t n = (size_t)nc * A.ng;
+  mix_rate_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(A, nc, cellmap, mrate);
+  mix_emit_kernel<<<nc, 128, 0, st>>>(A, emit32, eguide);
+  return cudaPeekAtLastError() == cudaSuccess ? SLG_OK : SLG_ERR_CUDA;
+}
 
 // Variants: resident 128-thread blocks per SM requested from the compiler
 // (register budget 128 / 102 / 85 / 73 per thread).

@@ -211,11 +211,22 @@ class BatchTimestep:
 
     def finish(self, seed: int):
         """The particle loop over every model and the per-model flux tallies."""
+        self.transport(seed)
+        self.flux()
+
+    def transport(self, seed: int):
+        """The particle loop over every model (precision as set at construction
+        or by set_precision)."""
         L, h = self.hot.lib, self.hot.h
         self._tout.tot_evelo = self._tout.tot_eout = self._tout.tot_sflux = 0.0
         self._chk(L.slg_dev_particle_advance(h, C.byref(self._tin), ptr(self.prt), ptr(self.isv), self.npart,
                                              2 * seed + 1, C.byref(self._tout)))
-        self.flux()
+
+    def set_precision(self, precision: int):
+        """0: the FP64 particle loop (reference arithmetic) over all models in one
+        launch; 1: the mixed-precision loop."""
+        self.precision = precision
+        self._tin.precision = int(precision)
 
     def flux(self):
         """fluxtally per model (also frees the escaped particles' slots)."""

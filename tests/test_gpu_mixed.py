@@ -6,6 +6,10 @@ statistically: group luminosities (binned) within 3 sigma of Monte Carlo noise,
 estimated from lumdev = sum of e^2 per group (fluxtally.f:47-49), and the
 escaped energy, the deposited energy and the mean number of steps per
 particle against the spread of independent runs.
+
+False-alarm rate: 10 luminosity bins at |z| < 3 (0.27 % each under a normal
+null) and 7 Welch statistics at |t| < 4 (18 dof, 0.08 % each): about 3 % per
+snapshot; the seeds are fixed, so each run of the test is deterministic.
 """
 import numpy as np
 import pytest
@@ -41,7 +45,7 @@ def _welch(a, b):
     return (a.mean() - b.mean()) / se if se > 0 else 0.0
 
 
-@pytest.mark.parametrize("t_days,kind", [(5.0, "grey"), (6.0, "mono"), (20.0, "grey+sig")])
+@pytest.mark.parametrize("t_days,kind", [(1.5, "grey"), (5.0, "grey"), (6.0, "mono"), (20.0, "grey+sig")])
 def test_mixed_matches_fp64_statistically(hot, oracle, t_days, kind):
     """K independent seeds per form.  Steps per particle and the deposited energy
     have heavy-tailed per-particle distributions (a few per cent spread between
@@ -78,7 +82,7 @@ def test_mixed_matches_fp64_statistically(hot, oracle, t_days, kind):
     lum64 = sum(l for _, l, _ in runs[0]); dev64 = sum(d for _, _, d in runs[0])
     lum32 = sum(l for _, l, _ in runs[1]); dev32 = sum(d for _, _, d in runs[1])
     z = _binned_z(lum64, dev64, lum32, dev32)
-    assert np.all(np.abs(z) < 3.5), z
+    assert np.all(np.abs(z) < 3.0), z
 
 
 def test_mixed_pure_ddmc_config2_physics(hot):

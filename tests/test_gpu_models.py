@@ -4,8 +4,9 @@ Each model of a batch runs the same per-cell and per-particle arithmetic as
 its own single-model run: model m draws its random numbers under the key
 seed + m * SLG_MODEL_SEED_STRIDE with slots counted from the model's first
 slot.  So opacities, leakage coefficients, source particles and the particle
-states after the mixed-precision transport are bit-identical; tallies and
-luminosities are sums formed with atomics in a different order (rtol 1e-12).
+states after the transport (FP64 or mixed precision) are bit-identical;
+tallies and luminosities are sums formed with atomics in a different order
+(rtol 1e-12).
 """
 import numpy as np
 import pytest
@@ -29,7 +30,7 @@ def _tables(hot, temp, natom, nelec, vol, mass, natomfr, oc, ginv):
     return dict(tempinv=tinv, sig=op["sig"], capgrey=grey, emitprob=ep, opaclump=ol, cap=op["cap"])
 
 
-def _run_batch(b, seed_src, seed_tr, params):
+def _run_batch(b, seed_src, seed_tr, params, precision=1):
     hot = HotPath(0)
     hot.set_groups(b.groups.wl)
     hot.set_models(b.nx, b.npart, b.xarr, b.vxarr, b.vol, b.divv)
@@ -44,13 +45,13 @@ def _run_batch(b, seed_src, seed_tr, params):
     isv = np.ones(n, dtype=np.int32)
     hot.interior_source(g.temp, emit, nvol, prt, isv, seed=seed_src)
     src = prt.copy()
-    r = hot.particle_advance(tab, prt, isv, params, seed=seed_tr, precision=1)
+    r = hot.particle_advance(tab, prt, isv, params, seed=seed_tr, precision=precision)
     lum, dev, num = hot.fluxtally(prt, isv, b.groups.wl)
     hot.close()
     return dict(tab=tab, emit=emit, nvol=nvol, nnew=nnew, src=src, prt=prt, isv=isv, r=r, lum=lum, dev=dev, num=num)
 
 
-def _run_one(c, npart, seed_src, seed_tr, params):
+def _run_one(c, npart, seed_src, seed_tr, params, precision=1):
     hot = HotPath(0)
     hot.set_groups(c.groups.wl)
     hot.set_grid(c.grid.xarr, c.grid.vxarr, c.grid.vol, c.grid.divv)
@@ -63,19 +64,20 @@ def _run_one(c, npart, seed_src, seed_tr, params):
     isv = np.ones(npart, dtype=np.int32)
     hot.interior_source(g.temp, emit, nvol, prt, isv, seed=seed_src)
     src = prt.copy()
-    r = hot.particle_advance(tab, prt, isv, params, seed=seed_tr, precision=1)
+    r = hot.particle_advance(tab, prt, isv, params, seed=seed_tr, precision=precision)
     lum, dev, num = hot.fluxtally(prt, isv, c.groups.wl)
     hot.close()
     return dict(tab=tab, emit=emit, nvol=nvol, nnew=nnew, src=src, prt=prt, isv=isv, r=r, lum=lum, dev=dev, num=num)
 
 
+@pytest.mark.parametrize("precision", [1, 0])
 @pytest.mark.parametrize("t_days", [(4.0, 8.0), (15.0, 30.0)])
-def test_models_match_single_model_runs(t_days):
+def test_models_match_single_model_runs(t_days, precision):
     b = W.model_batch(nmodel=3, seed=9, ng=100, nline=20000, nx=[20, 35, 50], npart=[3000, 5000, 2000],
                       t_range_days=t_days)
     params = W.TransportParams()
     s_src, s_tr = 77, 1234
-    B = _run_batch(b, s_src, s_tr, params)
+    B = _run_batch(b, s_src, s_tr, params, precision)
     assert B["r"]["ierr"] == 0
     steps = 0
     for m, c in enumerate(b.models):
@@ -83,7 +85,8 @@ def test_models_match_single_model_runs(t_days):
         cs = slice(co, co + int(b.nx[m]))
         po = int(b.npart[:m].sum())
         ps = slice(po, po + int(b.npart[m]))
-        S = _run_one(c, int(b.npart[m]), (s_src + m * STRIDE) & MASK, (s_tr + m * STRIDE) & MASK, params)
+        S = _run_one(c, int(b.npart[m]), (s_src + m * STRIDE) & MASK, (s_tr + m * STRIDE) & MASK, params,
+                     precision)
         assert S["r"]["ierr"] == 0
         for k in ("sig", "capgrey", "opaclump", "emitprob", "cap"):
             np.testing.assert_array_equal(B["tab"][k][cs], S["tab"][k], err_msg=k)
@@ -118,7 +121,8 @@ def test_models_source_stays_in_model_slots():
     hot.close()
 
 
-def test_models_edge_cases():
+@pytest.mark.parametrize("precision", [1, 0])
+def test_models_edge_cases(precision):
     """Ragged batches: two- and three-shell models beside a 40-shell one, and a
     call whose slots are all vacant (nothing to transport, zero counters)."""
     params = W.TransportParams()
@@ -136,7 +140,7 @@ def test_models_edge_cases():
     prt = np.zeros(n, dtype=PACKET_DTYPE)
     isv = np.ones(n, dtype=np.int32)
     # all slots vacant: the loop has nothing to do
-    r0 = hot.particle_advance(tab, prt, isv, params, seed=1, precision=1)
+    r0 = hot.particle_advance(tab, prt, isv, params, seed=1, precision=precision)
     assert r0["ierr"] == 0 and r0["npckt"] == 0 and r0["nstepimc"] + r0["nstepddmc"] == 0
     # sources in every model, then one step over all three
     emit, _ = hot.sourceenergy(b.temp, L_BOL)
@@ -144,7 +148,7 @@ def test_models_edge_cases():
     assert nnew <= n
     hot.interior_source(b.temp, emit, nvol, prt, isv, seed=2)
     assert int((isv == 0).sum()) == nnew
-    r = hot.particle_advance(tab, prt, isv, params, seed=3, precision=1)
+    r = hot.particle_advance(tab, prt, isv, params, seed=3, precision=precision)
     assert r["ierr"] == 0 and r["npckt"] == nnew
     lum, dev, num = hot.fluxtally(prt, isv, b.groups.wl)
     lum = np.asarray(lum).reshape(3, -1)

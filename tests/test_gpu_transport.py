@@ -146,6 +146,33 @@ def test_fluxtally_and_sourcetally_match_oracle(hot, oracle):
     assert np.array_equal(vg, vo)
 
 
+def _physical_case(oracle, ncell, ng, nline, npart, seed=2, t_days=10.0):
+    """A transport case on the physical opacities of the physical-opacity
+    workload (every shell optically thick: a pure DDMC random walk)."""
+    case = W.opacity_case(ncell=ncell, ng=ng, nline=nline, seed=seed, t_days=t_days)
+    op = oracle.physical_opacity(case)
+    g = case.gas
+    tinv = 1.0 / g.temp
+    grey = oracle.planckmean(case.groups.wlinv, g.temp, op["cap"])
+    params = W.TransportParams()
+    ol = oracle.leakage_opacity11(case.grid, case.groups.wlinv, tinv, op["sig"], op["cap"])
+    ep = oracle.emission_probability(case.groups.wlinv, tinv, op["cap"], grey, case.groups.nep, case.groups.nepg)
+    prt, isv, _, _, _ = oracle.make_source_particles(case.grid, case.groups, g.temp, 1e42, npart)
+    tables = dict(tempinv=tinv, sig=op["sig"], capgrey=grey, emitprob=ep, opaclump=ol, cap=op["cap"])
+    return dict(grid=case.grid, groups=case.groups, tables=tables, prt=prt, isv=isv, params=params)
+
+
+def test_event_sequences_pure_ddmc_2000_groups(hot, oracle):
+    """The full-timestep workload's physics at full size (256 shells x 2000
+    groups, 5e5 lines): 256-entry guide tables and the 8-ary searches over
+    2000-group running sums, every event a DDMC event; 400 particles, about
+    1.4e6 events, each particle's event sequence identical to the oracle's."""
+    c = _physical_case(oracle, 256, 2000, 500_000, 400)
+    ref, got, o, g = _run_both(hot, oracle, c, seed=3)
+    assert ref["nstepimc"] == 0 and ref["nstepddmc"] > 400 * 1000
+    _compare(ref, got, o, g)
+
+
 def test_set_groups_rejects_more_than_int16_groups(hot):
     from superlite_b200 import SlgError
     wl = np.geomspace(1e-5, 3.2e-4, 40001)  # 40000 groups > SLG_MAX_GROUPS (group lists are int16)
