@@ -293,6 +293,38 @@ __global__ void bf_table_kernel(int ngsub, int maxact, const int* __restrict__ p
   xstab[t] = bfxs(ph1, ph2, iz, iz - ii + 1, en);
 }
 
+// Per-line factors that do not depend on the shell, for the binned lines of
+// sub-groups 1..ngsub (lines outside the grid get zeros and are never read):
+// pg = phi(igs) * gxs, the first product of the reference's expression
+// (physical_opacity.f:148-149), so the evaluation order of that product is
+// kept; chi = chilw in FP64; and the line's population row
+// slot = (iz - 1) nst + (ii - 1) of grndlev.
+__global__ void decode_lines_kernel(const slg_bbxs* __restrict__ bb, int64_t nline, const int* __restrict__ lstart,
+                                    int ngsub, const double* __restrict__ wlsub, int nst, double2* __restrict__ lpc,
+                                    int* __restrict__ lslot) {
+  const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= nline) return;
+  // sub-group of line l: the largest igs with lstart[igs] <= l
+  int lo = 0, hi = ngsub + 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (lstart[mid] <= l) lo = mid;
+    else hi = mid - 1;
+  }
+  const int igs = lo;
+  if (igs < 1 || igs > ngsub) {
+    lpc[l] = make_double2(0.0, 0.0);
+    lslot[l] = 0;
+    return;
+  }
+  const slg_bbxs r = bb[l];
+  const double wa = wlsub[igs - 1], wb = wlsub[igs];
+  const double wl = 0.5 * (wa + wb);
+  const double phi = wl * wl / ((wb - wa) * pc_c);
+  lpc[l] = make_double2(phi * (double)r.gxs, (double)r.chilw);
+  lslot[l] = (r.iz - 1) * nst + (r.ii - 1);
+}
+
 struct OpacArgs {
   int nc, ng, ngs, ngsub, nelem, nst, maxact;
   int nobb, nobf, noff;
@@ -302,6 +334,8 @@ struct OpacArgs {
   const double* grp_wl;
   const int* lstart;        // (ngsub+2)+1 offsets by igs
   const slg_bbxs* bb;
+  const double2* lpc;       // per line {phi(igs) gxs, chilw} (decode_lines_kernel)
+  const int* lslot;         // per line population row of grndlev
   const double* grndlev;    // [slot][cell]
   const double* oc;         // [slot][cell]
   const int16_t* act_slot;  // active slots, reference order
@@ -323,7 +357,8 @@ struct OpacArgs {
 };
 
 // One sub-group igs for shell i: bb, bf and ff in the reference's order.
-__device__ inline double subgroup_opacity(const OpacArgs& A, int i, int igs, bool live) {
+// etab: the exp table (kExp2Tab64) in shared memory.
+__device__ inline double subgroup_opacity(const OpacArgs& A, int i, int igs, bool live, const double* etab) {
   double cap = 0.0;
   if (!live) return cap;
   const double h = A.hckt[i];
@@ -333,19 +368,19 @@ __device__ inline double subgroup_opacity(const OpacArgs& A, int i, int igs, boo
       const double wa = A.wlsub[igs - 1], wb = A.wlsub[igs];
       const double wl = 0.5 * (wa + wb);
       const double wlinv = 1.0 / wl;
-      const double dwl = wb - wa;
       const double expfac = 1.0 - exp(-(h * wlinv));
-      const double phi = wl * wl / (dwl * pc_c);
+      // sum over the sub-group's lines of phi gxs ocg exp(-chilw h), times the
+      // stimulated-emission factor once (the reference multiplies each term by
+      // it; the sum of positive terms differs by rounding only)
+      double sbb = 0.0;
       for (int l = l0; l < l1; ++l) {
-        const float4 rec = __ldg(reinterpret_cast<const float4*>(A.bb) + l);
-        const float gxs = rec.y, chilw = rec.z;
-        const uint32_t izii = __float_as_uint(rec.w);
-        const int iz = (int)(int16_t)(izii & 0xffffu), ii = (int)(int16_t)(izii >> 16);
-        const double ocg = A.grndlev[((size_t)(iz - 1) * A.nst + (ii - 1)) * A.nc + i];
+        const double2 pc = __ldg(A.lpc + l);
+        const int slot = __ldg(A.lslot + l);
+        const double ocg = A.grndlev[(size_t)slot * A.nc + i];
         if (ocg <= 0.0) continue;
-        const double caphelp = phi * (double)gxs * ocg * exp(-((double)chilw * h)) * expfac;
-        cap = cap + caphelp;
+        sbb = sbb + pc.x * ocg * exp_tang(-(pc.y * h), etab);
       }
+      cap = cap + sbb * expfac;
     }
   }
   if (!A.nobf) {
@@ -390,6 +425,9 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_fwd_kernel(const OpacArg
   __shared__ float tcap[OPAC_CT][OPAC_GT + 1];
   __shared__ float tem[OPAC_CT][OPAC_GT + 1];
   __shared__ double tcapd[OPAC_CT][OPAC_GT + 1];
+  __shared__ double etab[64];
+  exp_table_load(etab);
+  __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ig = blockIdx.y * OPAC_GT + warp + 1;  // 1-based group
   const int i = blockIdx.x * OPAC_CT + lane;       // 0-based shell
@@ -398,12 +436,12 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_fwd_kernel(const OpacArg
   double cap = 0.0;
   if (valid) {
     if (A.ngs == 1) {
-      cap = subgroup_opacity(A, i, ig, live);
+      cap = subgroup_opacity(A, i, ig, live, etab);
     } else {
       // collapse subgridding, physical_opacity.f:252-264
       double sp = 0.0, sr = 0.0;
       for (int s = 1; s <= A.ngs; ++s) {
-        const double v = subgroup_opacity(A, i, (ig - 1) * A.ngs + s, live);
+        const double v = subgroup_opacity(A, i, (ig - 1) * A.ngs + s, live, etab);
         if (v > 0.0) { sp = sp + v; sr = sr + 1.0 / v; }
       }
       const double help = 1.0 / A.ngs;
@@ -624,6 +662,8 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArg
   double* s_t = s_fr + (size_t)(A.nelem + 1) * 32;   // [warp][32]
   double* s_h = s_t + OPAC_GT * 32;
   const int ntot = (2 * nslot + A.nelem + 1) * 32;
+  __shared__ double etab[64];
+  exp_table_load(etab);
   for (int k = threadIdx.x; k < ntot; k += blockDim.x) sm[k] = 0.0;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -642,20 +682,17 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArg
         const double wlinv = 1.0 / wl;
         const double eh = exp(-(h * wlinv));
         const double expfac = 1.0 - eh;
-        const double phi = wl * wl / ((wb - wa) * pc_c);
         double capbb = 0.0, schi = 0.0;
         for (int l = l0; l < l1; ++l) {
-          const float4 rec = __ldg(reinterpret_cast<const float4*>(A.bb) + l);
-          const uint32_t izii = __float_as_uint(rec.w);
-          const int iz = (int)(int16_t)(izii & 0xffffu), ii = (int)(int16_t)(izii >> 16);
-          const int slot = (iz - 1) * A.nst + (ii - 1);
-          const double base = phi * (double)rec.y * exp(-((double)rec.z * h)) * expfac;  // d cap / d grndlev
+          const double2 pc = __ldg(A.lpc + l);
+          const int slot = __ldg(A.lslot + l);
+          const double base = pc.x * exp_tang(-(pc.y * h), etab) * expfac;  // d cap / d grndlev
           atomicAdd(&s_grnd[slot * 32 + lane], u * base);
           const double ocg = A.grndlev[(size_t)slot * A.nc + i];
           if (ocg > 0.0) {
             const double c = base * ocg;
             capbb = capbb + c;
-            schi = schi + c * (double)rec.z;
+            schi = schi + c * pc.y;
           }
         }
         // h = hc/kT: d exp(-chi h)/dT = chi h/T exp(..), d expfac/dT = -(h/T) wlinv eh
@@ -803,6 +840,8 @@ static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_f
   cudaMemsetAsync(d_active, 0, sizeof(int) * (nslot + 1), st);
   wlsub_kernel<<<(nedge_pad + 255) / 256, 256, 0, st>>>(ng, ngs, nedge_pad, ctx->d_wl, d_wlsub);
   const bool do_bb = ctx->nline > 0 && !flags->nobb;
+  double2* d_lpc = nullptr;
+  int* d_lslot = nullptr;
   if (do_bb) {
     const size_t shm = 16 + sizeof(double) * nedge_pad + sizeof(unsigned int) * (nedge + 1);
     if (shm > 220 * 1024)
@@ -817,6 +856,11 @@ static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_f
     bin_lines_kernel<<<nb, 256, shm, st>>>(ctx->d_bb, ctx->nline, d_wlsub, nedge, nedge_pad, d_counts,
                                            d_flags);
     scan_counts_kernel<<<1, 1024, 0, st>>>(d_counts, nedge + 1, d_lstart);
+    d_lpc = (double2*)scratch(ctx, 84, sizeof(double2) * (size_t)ctx->nline);
+    d_lslot = (int*)scratch(ctx, 85, sizeof(int) * (size_t)ctx->nline);
+    if (!d_lpc || !d_lslot) return SLG_ERR_OOM;
+    decode_lines_kernel<<<(unsigned)((ctx->nline + 255) / 256), 256, 0, st>>>(ctx->d_bb, ctx->nline, d_lstart, ngsub,
+                                                                              d_wlsub, nst, d_lpc, d_lslot);
   } else {
     cudaMemsetAsync(d_lstart, 0, sizeof(int) * (nedge + 3), st);
   }
@@ -837,6 +881,7 @@ static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_f
   A.nobb = !do_bb; A.nobf = !do_bf; A.noff = flags->noff;
   A.mix = flags->opacmixrossel;
   A.wlsub = d_wlsub; A.grp_wl = ctx->d_wl; A.lstart = d_lstart; A.bb = ctx->d_bb;
+  A.lpc = d_lpc; A.lslot = d_lslot;
   A.grndlev = d_grnd; A.oc = gas->oc; A.act_slot = d_act; A.xstab = d_xs;
   A.hckt = d_hckt; A.hlparr = d_hlp; A.mass = gas->mass; A.natomfr = gas->natomfr; A.temp = gas->temp;
   A.ffigg = d_ffigg; A.ffdgg = d_ffdgg; A.gff = ctx->d_gff;

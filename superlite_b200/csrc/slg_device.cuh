@@ -40,6 +40,61 @@ constexpr double e6c = e4c * e2c;
 constexpr double c2c = pc_c * pc_c;
 constexpr double c4c = c2c * c2c;
 constexpr double cthomson = 8.0 * pc_pi * e4c / (3.0 * (pc_me * pc_me) * c4c);  // physical_opacity.f:51
+
+// ---- exp(x) by Tang's table-driven method (P. T. P. Tang, "Table-driven
+// implementation of the exponential function in IEEE floating-point
+// arithmetic", ACM TOMS 15 (1989) 144-157), for the opacity build's inner
+// loops, whose one exp per line-shell term is their binding work:
+//   x = (64 m + j) ln2/64 + r,  |r| <= ln2/128,  exp(x) = 2^m 2^(j/64) e^r,
+// with ln2/64 split in a 36-bit head (so that n * head is exact for |n| <
+// 2^17) and its remainder, e^r - 1 by its Taylor polynomial of degree 5
+// (truncation below 4e-17 relative), 2^(j/64) from a 64-entry table and 2^m
+// added to the exponent field.  Arguments outside [-700, 700] go to exp().
+constexpr double kExpInvL = 92.33248261689366;        // 64 / ln 2
+constexpr double kExpL1 = 0.010830424696223417;       // ln2/64, 36 significant bits
+constexpr double kExpL2 = 2.572804622327669e-14;      // ln2/64 - kExpL1
+// 2^(j/64), j = 0..63, correctly rounded
+static __constant__ double kExp2Tab64[64] = {
+    1.0, 1.0108892860517005, 1.0218971486541166, 1.0330248790212284,
+    1.0442737824274138, 1.0556451783605572, 1.0671404006768237, 1.0787607977571199,
+    1.0905077326652577, 1.102382583307841, 1.1143867425958924, 1.1265216186082418,
+    1.1387886347566916, 1.1511892299529827, 1.1637248587775775, 1.1763969916502812,
+    1.189207115002721, 1.202156731452703, 1.215247359980469, 1.22848053610687,
+    1.241857812073484, 1.255380757024691, 1.2690509571917332, 1.2828700160787783,
+    1.2968395546510096, 1.3109612115247644, 1.3252366431597413, 1.339667524053303,
+    1.3542555469368927, 1.3690024229745905, 1.383909881963832, 1.3989796725383112,
+    1.4142135623730951, 1.42961333839197, 1.4451808069770467, 1.460917794180647,
+    1.4768261459394993, 1.4929077282912648, 1.5091644275934228, 1.5255981507445384,
+    1.5422108254079407, 1.559004400237837, 1.5759808451078865, 1.593142151342267,
+    1.6104903319492543, 1.6280274218573478, 1.645755478153965, 1.6636765803267364,
+    1.681792830507429, 1.7001063537185235, 1.718619298122478, 1.7373338352737062,
+    1.7562521603732995, 1.7753764925265212, 1.7947090750031072, 1.8142521755003989,
+    1.8340080864093424, 1.8539791250833855, 1.8741676341103, 1.8945759815869656,
+    1.9152065613971474, 1.9360617934922943, 1.9571441241754002, 1.978456026387951,
+};
+
+// Copies kExp2Tab64 into a block's shared array (call from every thread, then
+// __syncthreads()).
+__device__ inline void exp_table_load(double* s_tab) {
+  for (int k = threadIdx.x; k < 64; k += blockDim.x) s_tab[k] = kExp2Tab64[k];
+}
+
+// tab: kExp2Tab64 in shared memory.
+__device__ inline double exp_tang(double x, const double* tab) {
+  if (!(fabs(x) <= 700.0)) return exp(x);  // also NaN
+  const double n = rint(x * kExpInvL);
+  const int ni = (int)n;
+  double r = fma(-n, kExpL1, x);
+  r = fma(-n, kExpL2, r);
+  double p = fma(r, 1.0 / 120.0, 1.0 / 24.0);
+  p = fma(r, p, 1.0 / 6.0);
+  p = fma(r, p, 0.5);
+  p = fma(r, p, 1.0);
+  p = p * r;  // e^r - 1
+  const double s = tab[ni & 63];
+  const double v = fma(s, p, s);
+  return __longlong_as_double(__double_as_longlong(v) + ((long long)(ni >> 6) << 52));
+}
 constexpr double ff_c1a = 4.0 * e6c / (3.0 * pc_h * pc_me * c4c);              // physical_opacity.f:32
 constexpr double ff_c1b = pc_pi2 / (3.0 * pc_me * pc_h * pc_c);                 // argument of its sqrt
 // Fortran `1.0/3.0` is a real*4 quotient promoted to real*8 as an exponent.
