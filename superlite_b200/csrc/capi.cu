@@ -256,7 +256,7 @@ void slg_destroy(slg_ctx* ctx) {
   free_dev(ctx->d_gff); free_dev(ctx->d_acc);
   free_dev(ctx->d_totals); free_dev(ctx->d_epoch); free_dev(ctx->d_models); free_dev(ctx->d_cellmap);
   free_dev(ctx->d_eos_ni); free_dev(ctx->d_eos_e); free_dev(ctx->d_eos_q); free_dev(ctx->d_eos_g1);
-  free_dev(ctx->d_amass);
+  free_dev(ctx->d_amass); free_dev(ctx->d_lrow_of_slot); free_dev(ctx->d_slot_of_lrow);
   if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
   if (ctx->h_acc) cudaFreeHost(ctx->h_acc);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -420,10 +420,32 @@ int slg_set_atomic_data(slg_ctx* ctx, int32_t nelem, int32_t nstage, const int32
     rc = cuda_check(ctx, cudaMalloc(&ctx->d_gff, sizeof(double) * 81 * 41), "alloc gff");
     if (!rc) rc = cuda_check(ctx, cudaMemcpy(ctx->d_gff, ff_gff, sizeof(double) * 81 * 41, cudaMemcpyHostToDevice), "gff");
   }
+  // the population rows the lines reference (the opacity adjoint accumulates
+  // d cap / d population for those rows only)
+  const int nslot = nelem * nstage;
+  std::vector<int16_t> row_of(nslot, (int16_t)-1), slot_of;
+  for (int64_t l = 0; l < nline; ++l) {
+    const int sl = (bb_xs[l].iz - 1) * nstage + (bb_xs[l].ii - 1);
+    if (row_of[sl] < 0) {
+      row_of[sl] = (int16_t)slot_of.size();
+      slot_of.push_back((int16_t)sl);
+    }
+  }
+  free_dev(ctx->d_lrow_of_slot); free_dev(ctx->d_slot_of_lrow);
+  ctx->d_lrow_of_slot = ctx->d_slot_of_lrow = nullptr;
+  if (!rc) rc = cuda_check(ctx, cudaMalloc(&ctx->d_lrow_of_slot, sizeof(int16_t) * nslot), "alloc row map");
+  if (!rc) rc = cuda_check(ctx, cudaMemcpy(ctx->d_lrow_of_slot, row_of.data(), sizeof(int16_t) * nslot,
+                                          cudaMemcpyHostToDevice), "row map");
+  if (!rc && !slot_of.empty()) {
+    rc = cuda_check(ctx, cudaMalloc(&ctx->d_slot_of_lrow, sizeof(int16_t) * slot_of.size()), "alloc slot map");
+    if (!rc) rc = cuda_check(ctx, cudaMemcpy(ctx->d_slot_of_lrow, slot_of.data(), sizeof(int16_t) * slot_of.size(),
+                                            cudaMemcpyHostToDevice), "slot map");
+  }
   if (rc) return rc;
   ctx->nelem = nelem;
   ctx->nstage = nstage;
   ctx->nline = nline;
+  ctx->nlrow = (int)slot_of.size();
   ctx->h_ion_ni.assign(ion_ni, ion_ni + nelem);
   return SLG_OK;
 }

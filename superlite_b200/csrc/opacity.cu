@@ -298,9 +298,11 @@ __global__ void bf_table_kernel(int ngsub, int maxact, const int* __restrict__ p
 // pg = phi(igs) * gxs, the first product of the reference's expression
 // (physical_opacity.f:148-149), so the evaluation order of that product is
 // kept; chi = chilw in FP64; and the line's population row
-// slot = (iz - 1) nst + (ii - 1) of grndlev.
+// slot = (iz - 1) nst + (ii - 1) of grndlev in the low 16 bits, the slot's
+// row among the rows the lines reference (lrow_of_slot) in the high 16 bits.
 __global__ void decode_lines_kernel(const slg_bbxs* __restrict__ bb, int64_t nline, const int* __restrict__ lstart,
-                                    int ngsub, const double* __restrict__ wlsub, int nst, double2* __restrict__ lpc,
+                                    int ngsub, const double* __restrict__ wlsub, int nst,
+                                    const int16_t* __restrict__ lrow_of_slot, double2* __restrict__ lpc,
                                     int* __restrict__ lslot) {
   const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= nline) return;
@@ -322,7 +324,8 @@ __global__ void decode_lines_kernel(const slg_bbxs* __restrict__ bb, int64_t nli
   const double wl = 0.5 * (wa + wb);
   const double phi = wl * wl / ((wb - wa) * pc_c);
   lpc[l] = make_double2(phi * (double)r.gxs, (double)r.chilw);
-  lslot[l] = (r.iz - 1) * nst + (r.ii - 1);
+  const int slot = (r.iz - 1) * nst + (r.ii - 1);
+  lslot[l] = slot | ((int)lrow_of_slot[slot] << 16);
 }
 
 struct OpacArgs {
@@ -335,7 +338,9 @@ struct OpacArgs {
   const int* lstart;        // (ngsub+2)+1 offsets by igs
   const slg_bbxs* bb;
   const double2* lpc;       // per line {phi(igs) gxs, chilw} (decode_lines_kernel)
-  const int* lslot;         // per line population row of grndlev
+  const int* lslot;         // per line: population slot (low 16 bits), line row (high 16 bits)
+  const int16_t* slot_of_lrow;  // line row -> slot
+  int nlrow;                // population rows the lines reference
   const double* grndlev;    // [slot][cell]
   const double* oc;         // [slot][cell]
   const int16_t* act_slot;  // active slots, reference order
@@ -375,7 +380,7 @@ __device__ inline double subgroup_opacity(const OpacArgs& A, int i, int igs, boo
       double sbb = 0.0;
       for (int l = l0; l < l1; ++l) {
         const double2 pc = __ldg(A.lpc + l);
-        const int slot = __ldg(A.lslot + l);
+        const int slot = __ldg(A.lslot + l) & 0xffff;
         const double ocg = A.grndlev[(size_t)slot * A.nc + i];
         if (ocg <= 0.0) continue;
         sbb = sbb + pc.x * ocg * exp_tang(-(pc.y * h), etab);
@@ -655,13 +660,12 @@ struct OpacBwd {
 // lines of each group, with per-(ion, shell) sums gathered in shared memory.
 __global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArgs A, const OpacBwd B) {
   extern __shared__ double sm[];
-  const int nslot = A.nelem * A.nst;
-  double* s_grnd = sm;                               // [slot][32]
-  double* s_oc = sm + (size_t)nslot * 32;            // [slot][32]
-  double* s_fr = s_oc + (size_t)nslot * 32;          // [nelem+1][32]
+  const int nrow = A.nlrow;                          // population rows the lines reference
+  double* s_grnd = sm;                               // [line row][32]
+  double* s_fr = sm + (size_t)nrow * 32;             // [nelem+1][32]
   double* s_t = s_fr + (size_t)(A.nelem + 1) * 32;   // [warp][32]
   double* s_h = s_t + OPAC_GT * 32;
-  const int ntot = (2 * nslot + A.nelem + 1) * 32;
+  const int ntot = (nrow + A.nelem + 1) * 32;
   __shared__ double etab[64];
   exp_table_load(etab);
   for (int k = threadIdx.x; k < ntot; k += blockDim.x) sm[k] = 0.0;
@@ -685,9 +689,10 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArg
         double capbb = 0.0, schi = 0.0;
         for (int l = l0; l < l1; ++l) {
           const double2 pc = __ldg(A.lpc + l);
-          const int slot = __ldg(A.lslot + l);
+          const int sr = __ldg(A.lslot + l);
+          const int slot = sr & 0xffff, row = sr >> 16;
           const double base = pc.x * exp_tang(-(pc.y * h), etab) * expfac;  // d cap / d grndlev
-          atomicAdd(&s_grnd[slot * 32 + lane], u * base);
+          atomicAdd(&s_grnd[row * 32 + lane], u * base);
           const double ocg = A.grndlev[(size_t)slot * A.nc + i];
           if (ocg > 0.0) {
             const double c = base * ocg;
@@ -699,14 +704,7 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArg
         gt = gt + u * ((h / T) * schi - capbb * (h / T) * wlinv * eh / expfac);
       }
     }
-    if (!A.nobf) {
-      const double* xs = A.xstab + (size_t)(ig - 1) * A.maxact;
-      const int nact = *A.pnact;
-      for (int a = 0; a < nact; ++a) {
-        const double x = xs[a];
-        if (x != 0.0) atomicAdd(&s_oc[A.act_slot[a] * 32 + lane], u * x * pc_mbarn);
-      }
-    }
+    // bound-free: bf_bwd_kernel
     if (!A.noff) {
       const double wl = A.wlsub[ig - 1];
       const double wlinv = 1.0 / wl;
@@ -764,9 +762,29 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArg
     const double v = sm[k];
     const int row = k >> 5, c = blockIdx.x * OPAC_CT + (k & 31);
     if (v == 0.0 || c >= A.nc) continue;
-    if (row < nslot) atomicAdd(&B.ggrnd[(size_t)row * A.nc + c], v);
-    else if (row < 2 * nslot) atomicAdd(&B.goc[(size_t)(row - nslot) * A.nc + c], v);
-    else atomicAdd(&B.gfr[(size_t)c * (A.nelem + 1) + (row - 2 * nslot)], v);
+    if (row < nrow) atomicAdd(&B.ggrnd[(size_t)A.slot_of_lrow[row] * A.nc + c], v);
+    else atomicAdd(&B.gfr[(size_t)c * (A.nelem + 1) + (row - nrow)], v);
+  }
+}
+
+// Bound-free part of the adjoint (physical_opacity.f:163-195, ngs = 1):
+// d cap(g, i) / d oc(slot, i) = xs(g, slot) mbarn, so
+// goc(slot, i) += sum_g gcap(g, i) xs(g, slot) mbarn over the active slots.
+// One block per shell, one thread per active slot; added after
+// opacity_bwd_kernel and before opac_cell_bwd_kernel (single writer per entry).
+__global__ void bf_bwd_kernel(const OpacArgs A, const OpacBwd B) {
+  const int i = blockIdx.x;
+  if (i >= A.nc || !(A.mass[i] > 0.0)) return;
+  const int nact = *A.pnact;
+  const double* u = B.gcap + (size_t)i * A.ng;
+  for (int a = threadIdx.x; a < nact; a += blockDim.x) {
+    double acc = 0.0;
+    for (int g = 0; g < A.ng; ++g) {
+      const double x = A.xstab[(size_t)g * A.maxact + a];
+      const double ug = u[g];
+      if (x != 0.0 && ug != 0.0) acc = acc + ug * x * pc_mbarn;
+    }
+    if (acc != 0.0) B.goc[(size_t)A.act_slot[a] * A.nc + i] += acc;
   }
 }
 
@@ -859,8 +877,8 @@ static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_f
     d_lpc = (double2*)scratch(ctx, 84, sizeof(double2) * (size_t)ctx->nline);
     d_lslot = (int*)scratch(ctx, 85, sizeof(int) * (size_t)ctx->nline);
     if (!d_lpc || !d_lslot) return SLG_ERR_OOM;
-    decode_lines_kernel<<<(unsigned)((ctx->nline + 255) / 256), 256, 0, st>>>(ctx->d_bb, ctx->nline, d_lstart, ngsub,
-                                                                              d_wlsub, nst, d_lpc, d_lslot);
+    decode_lines_kernel<<<(unsigned)((ctx->nline + 255) / 256), 256, 0, st>>>(
+        ctx->d_bb, ctx->nline, d_lstart, ngsub, d_wlsub, nst, ctx->d_lrow_of_slot, d_lpc, d_lslot);
   } else {
     cudaMemsetAsync(d_lstart, 0, sizeof(int) * (nedge + 3), st);
   }
@@ -881,7 +899,7 @@ static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_f
   A.nobb = !do_bb; A.nobf = !do_bf; A.noff = flags->noff;
   A.mix = flags->opacmixrossel;
   A.wlsub = d_wlsub; A.grp_wl = ctx->d_wl; A.lstart = d_lstart; A.bb = ctx->d_bb;
-  A.lpc = d_lpc; A.lslot = d_lslot;
+  A.lpc = d_lpc; A.lslot = d_lslot; A.slot_of_lrow = ctx->d_slot_of_lrow; A.nlrow = ctx->nlrow;
   A.grndlev = d_grnd; A.oc = gas->oc; A.act_slot = d_act; A.xstab = d_xs;
   A.hckt = d_hckt; A.hlparr = d_hlp; A.mass = gas->mass; A.natomfr = gas->natomfr; A.temp = gas->temp;
   A.ffigg = d_ffigg; A.ffdgg = d_ffdgg; A.gff = ctx->d_gff;
@@ -947,8 +965,8 @@ int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, con
   cudaMemsetAsync(goc, 0, sizeof(double) * (size_t)nslot * nc, st);
   cudaMemsetAsync(gfr, 0, sizeof(double) * (size_t)nc * (A.nelem + 1), st);
   OpacBwd B{gcap, gT, ggrnd, goc, ghlp, gfr};
-  const size_t shm = sizeof(double) * ((size_t)(2 * nslot + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
-  if (shm > 200 * 1024) return set_error(ctx, SLG_ERR_ARG, "opacity adjoint: too many ion slots (%d)", nslot);
+  const size_t shm = sizeof(double) * ((size_t)(A.nlrow + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
+  if (shm > 200 * 1024) return set_error(ctx, SLG_ERR_ARG, "opacity adjoint: too many ion slots (%d)", A.nlrow);
   static size_t shm_set = 0;  // raised only when needed
   if (shm > 48 * 1024 && shm > shm_set) {
     cudaFuncSetAttribute(opacity_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -956,6 +974,7 @@ int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, con
   }
   dim3 grid((nc + OPAC_CT - 1) / OPAC_CT, (A.ng + OPAC_GT - 1) / OPAC_GT);
   opacity_bwd_kernel<<<grid, OPAC_GT * 32, shm, st>>>(A, B);
+  if (!A.nobf) bf_bwd_kernel<<<nc, 128, 0, st>>>(A, B);
   opac_cell_bwd_kernel<<<(nc + 127) / 128, 128, 0, st>>>(nc, A.nelem, A.nst, ctx->d_ion_ni, gas->natom, gas->nelec,
                                                          gas->vol, gas->mass, gas->ginv, 0, ggrnd, ghlp, gsig, goc,
                                                          gnelec, gnatom);

@@ -110,6 +110,11 @@ struct slg_ctx {
   int32_t* d_ion_ni = nullptr;
   std::vector<int32_t> h_ion_ni;
   slg_bbxs* d_bb = nullptr;
+  // population rows (slot = (iz-1) nstage + ii-1) that the lines reference:
+  // d_lrow_of_slot[slot] = compact row or -1, d_slot_of_lrow[row] = slot
+  int nlrow = 0;
+  int16_t* d_lrow_of_slot = nullptr;
+  int16_t* d_slot_of_lrow = nullptr;
   float* d_ph1 = nullptr;
   float* d_ph2 = nullptr;
   double* d_gff = nullptr;
