@@ -56,8 +56,8 @@ BYTES_PER_STEP = 128.0
 # the batched workload at 0.1x particle budgets (smsp__inst_executed.sum /
 # particle-steps of the launch; smsp__thread_inst_executed.sum /
 # smsp__inst_executed.sum): profiles/particle_advance_mixed_batched_128models_npart0.1.md
-MIXED_WARP_INST_PER_STEP = 71.3
-MIXED_LANES_PER_INST = 10.4
+MIXED_WARP_INST_PER_STEP = 51.1
+MIXED_LANES_PER_INST = 9.95
 
 
 def parse():
@@ -79,6 +79,9 @@ def parse():
                     help="batched: many models in one persistent launch, graph-captured steps; "
                          "timestep: one 256-shell model on physical opacities")
     ap.add_argument("--nmodel", type=int, default=128)
+    ap.add_argument("--opacity-size", type=int, default=4, choices=[1, 4],
+                    help="--workload opacity: 4 = 4096 shells x 10000 groups x 2e6 lines (default), "
+                         "1 = 256 x 2000 x 5e5")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 per-model comparison")
     ap.add_argument("--no-opacity", action="store_true", help="skip the opacity forward/adjoint measurement")
     ap.add_argument("--no-configs", action="store_true",
@@ -1097,7 +1100,7 @@ def run_opacity(a):
     torch.cuda.set_device(local)
     from superlite_b200 import peaks as PK
     pipes = PK.measure(local)
-    r = opacity_measure(local, reps=a.steps, which=4, exp_per_s=pipes["fp64_exp_per_s"]["value"])
+    r = opacity_measure(local, reps=a.steps, which=a.opacity_size, exp_per_s=pipes["fp64_exp_per_s"]["value"])
     res = {"metric": "opacity cell-group evals/s", "value": r["backward"]["cell_group_evals_per_s"],
            "unit": "cell-group evals/s", "n_gpus": 1, "steps": a.steps, "warmup": 3,
            "ms_per_step": r["forward"]["ms"] + r["backward"]["ms"], "higher_is_better": True, "scaling": "weak",
