@@ -154,18 +154,22 @@ __global__ void opac_cell_prep_kernel(int nc, int nelem, int nst, const int32_t*
                                       double* __restrict__ hckt, double* __restrict__ gas_sig,
                                       double* __restrict__ hlparr, double* __restrict__ grndlev,
                                       int* __restrict__ ffigg, double* __restrict__ ffdgg) {
+  // one thread per (shell i, element iz = blockIdx.y + 1)
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nc) return;
   const double h = pc_hc / (pc_kb * temp[i]);
-  hckt[i] = h;
-  double s = 0.0;
-  if (!nothmson) {
-    s = cthomson * nelec[i] * natom[i] / vol[i];
-    if (mass[i] <= 0.0) s = 0.0;
+  if (blockIdx.y == 0) {
+    hckt[i] = h;
+    double s = 0.0;
+    if (!nothmson) {
+      s = cthomson * nelec[i] * natom[i] / vol[i];
+      if (mass[i] <= 0.0) s = 0.0;
+    }
+    gas_sig[i] = s;
+    hlparr[i] = sq(natom[i] / vol[i]) * nelec[i];
   }
-  gas_sig[i] = s;
-  hlparr[i] = sq(natom[i] / vol[i]) * nelec[i];
-  for (int iz = 1; iz <= nelem; ++iz) {
+  {
+    const int iz = blockIdx.y + 1;
     const int lim = min(iz, ion_ni[iz - 1] - 1);
     for (int ii = 1; ii <= nst; ++ii) {
       const size_t k = (size_t)(iz - 1) * nst + (ii - 1);
@@ -341,6 +345,7 @@ struct OpacArgs {
   const int* lslot;         // per line: population slot (low 16 bits), line row (high 16 bits)
   const int16_t* slot_of_lrow;  // line row -> slot
   int nlrow;                // population rows the lines reference
+  int stage_rows = 0;       // forward: stage those rows of a block's shells in shared memory
   const double* grndlev;    // [slot][cell]
   const double* oc;         // [slot][cell]
   const int16_t* act_slot;  // active slots, reference order
@@ -361,9 +366,12 @@ struct OpacArgs {
   int* flags;
 };
 
-// One sub-group igs for shell i: bb, bf and ff in the reference's order.
-// etab: the exp table (kExp2Tab64) in shared memory.
-__device__ inline double subgroup_opacity(const OpacArgs& A, int i, int igs, bool live, const double* etab) {
+// One sub-group igs for shell i (lane `lane` of its block): bb, bf and ff in
+// the reference's order.  etab: the exp table (kExp2Tab64) in shared memory;
+// s_g: the block's population rows [line row][lane] in shared memory, or null
+// (read grndlev).
+__device__ inline double subgroup_opacity(const OpacArgs& A, int i, int lane, int igs, bool live, const double* etab,
+                                          const double* s_g) {
   double cap = 0.0;
   if (!live) return cap;
   const double h = A.hckt[i];
@@ -377,11 +385,34 @@ __device__ inline double subgroup_opacity(const OpacArgs& A, int i, int igs, boo
       // sum over the sub-group's lines of phi gxs ocg exp(-chilw h), times the
       // stimulated-emission factor once (the reference multiplies each term by
       // it; the sum of positive terms differs by rounding only)
+      // four lines per round: their loads and exps are independent; the terms
+      // are still added one after another in line order, and a term of an
+      // unpopulated ion adds +0 (the reference skips it: the same sum)
       double sbb = 0.0;
-      for (int l = l0; l < l1; ++l) {
+      int l = l0;
+      for (; l + 4 <= l1; l += 4) {
+        double2 pc[4];
+        int sr[4];
+        double og[4], t[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          pc[q] = __ldg(A.lpc + l + q);
+          sr[q] = __ldg(A.lslot + l + q);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          og[q] = s_g ? s_g[(sr[q] >> 16) * 32 + lane] : A.grndlev[(size_t)(sr[q] & 0xffff) * A.nc + i];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) t[q] = !(og[q] <= 0.0) ? pc[q].x * og[q] * exp_tang(-(pc[q].y * h), etab) : 0.0;
+        sbb = sbb + t[0];
+        sbb = sbb + t[1];
+        sbb = sbb + t[2];
+        sbb = sbb + t[3];
+      }
+      for (; l < l1; ++l) {
         const double2 pc = __ldg(A.lpc + l);
-        const int slot = __ldg(A.lslot + l) & 0xffff;
-        const double ocg = A.grndlev[(size_t)slot * A.nc + i];
+        const int sr = __ldg(A.lslot + l);
+        const double ocg = s_g ? s_g[(sr >> 16) * 32 + lane] : A.grndlev[(size_t)(sr & 0xffff) * A.nc + i];
         if (ocg <= 0.0) continue;
         sbb = sbb + pc.x * ocg * exp_tang(-(pc.y * h), etab);
       }
@@ -431,8 +462,16 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_fwd_kernel(const OpacArg
   __shared__ float tem[OPAC_CT][OPAC_GT + 1];
   __shared__ double tcapd[OPAC_CT][OPAC_GT + 1];
   __shared__ double etab[64];
+  extern __shared__ double s_rows[];  // [line row][lane] populations of this block's shells (A.stage_rows)
   exp_table_load(etab);
+  if (A.stage_rows) {
+    for (int k = threadIdx.x; k < A.nlrow * 32; k += blockDim.x) {
+      const int ii = blockIdx.x * OPAC_CT + (k & 31);
+      s_rows[k] = ii < A.nc ? A.grndlev[(size_t)A.slot_of_lrow[k >> 5] * A.nc + ii] : 0.0;
+    }
+  }
   __syncthreads();
+  const double* s_g = A.stage_rows ? s_rows : nullptr;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ig = blockIdx.y * OPAC_GT + warp + 1;  // 1-based group
   const int i = blockIdx.x * OPAC_CT + lane;       // 0-based shell
@@ -441,12 +480,12 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_fwd_kernel(const OpacArg
   double cap = 0.0;
   if (valid) {
     if (A.ngs == 1) {
-      cap = subgroup_opacity(A, i, ig, live, etab);
+      cap = subgroup_opacity(A, i, lane, ig, live, etab, s_g);
     } else {
       // collapse subgridding, physical_opacity.f:252-264
       double sp = 0.0, sr = 0.0;
       for (int s = 1; s <= A.ngs; ++s) {
-        const double v = subgroup_opacity(A, i, (ig - 1) * A.ngs + s, live, etab);
+        const double v = subgroup_opacity(A, i, lane, (ig - 1) * A.ngs + s, live, etab, s_g);
         if (v > 0.0) { sp = sp + v; sr = sr + 1.0 / v; }
       }
       const double help = 1.0 / A.ngs;
@@ -665,10 +704,15 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArg
   double* s_fr = sm + (size_t)nrow * 32;             // [nelem+1][32]
   double* s_t = s_fr + (size_t)(A.nelem + 1) * 32;   // [warp][32]
   double* s_h = s_t + OPAC_GT * 32;
+  double* s_g = s_h + OPAC_GT * 32;                  // [line row][32] populations of this block's shells
   const int ntot = (nrow + A.nelem + 1) * 32;
   __shared__ double etab[64];
   exp_table_load(etab);
   for (int k = threadIdx.x; k < ntot; k += blockDim.x) sm[k] = 0.0;
+  for (int k = threadIdx.x; k < nrow * 32; k += blockDim.x) {
+    const int ii = blockIdx.x * OPAC_CT + (k & 31);
+    s_g[k] = ii < A.nc ? A.grndlev[(size_t)A.slot_of_lrow[k >> 5] * A.nc + ii] : 0.0;
+  }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ig = blockIdx.y * OPAC_GT + warp + 1;
@@ -687,13 +731,32 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArg
         const double eh = exp(-(h * wlinv));
         const double expfac = 1.0 - eh;
         double capbb = 0.0, schi = 0.0;
-        for (int l = l0; l < l1; ++l) {
+        int l = l0;
+        for (; l + 2 <= l1; l += 2) {  // two lines per round: independent loads and exps
+          const double2 pa = __ldg(A.lpc + l), pb = __ldg(A.lpc + l + 1);
+          const int ra = __ldg(A.lslot + l) >> 16, rb = __ldg(A.lslot + l + 1) >> 16;
+          const double ba = pa.x * exp_tang(-(pa.y * h), etab) * expfac;  // d cap / d grndlev
+          const double bb = pb.x * exp_tang(-(pb.y * h), etab) * expfac;
+          const double oa = s_g[ra * 32 + lane], ob = s_g[rb * 32 + lane];
+          atomicAdd(&s_grnd[ra * 32 + lane], u * ba);
+          atomicAdd(&s_grnd[rb * 32 + lane], u * bb);
+          if (oa > 0.0) {
+            const double c = ba * oa;
+            capbb = capbb + c;
+            schi = schi + c * pa.y;
+          }
+          if (ob > 0.0) {
+            const double c = bb * ob;
+            capbb = capbb + c;
+            schi = schi + c * pb.y;
+          }
+        }
+        for (; l < l1; ++l) {
           const double2 pc = __ldg(A.lpc + l);
-          const int sr = __ldg(A.lslot + l);
-          const int slot = sr & 0xffff, row = sr >> 16;
+          const int row = __ldg(A.lslot + l) >> 16;
           const double base = pc.x * exp_tang(-(pc.y * h), etab) * expfac;  // d cap / d grndlev
           atomicAdd(&s_grnd[row * 32 + lane], u * base);
-          const double ocg = A.grndlev[(size_t)slot * A.nc + i];
+          const double ocg = s_g[row * 32 + lane];
           if (ocg > 0.0) {
             const double c = base * ocg;
             capbb = capbb + c;
@@ -770,21 +833,36 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArg
 // Bound-free part of the adjoint (physical_opacity.f:163-195, ngs = 1):
 // d cap(g, i) / d oc(slot, i) = xs(g, slot) mbarn, so
 // goc(slot, i) += sum_g gcap(g, i) xs(g, slot) mbarn over the active slots.
-// One block per shell, one thread per active slot; added after
-// opacity_bwd_kernel and before opac_cell_bwd_kernel (single writer per entry).
-__global__ void bf_bwd_kernel(const OpacArgs A, const OpacBwd B) {
+// One block of BFB_WARPS warps per shell: warp w sums the groups g = w, w +
+// BFB_WARPS, ... for 32 slots at a time (lane = slot, the table row is read
+// coalesced), the warps' partial sums are added through shared memory.  Runs
+// after opacity_bwd_kernel and before opac_cell_bwd_kernel (one writer per entry).
+constexpr int BFB_WARPS = 8;
+__global__ void __launch_bounds__(BFB_WARPS * 32) bf_bwd_kernel(const OpacArgs A, const OpacBwd B) {
+  extern __shared__ double part[];  // [warp][active slot]
   const int i = blockIdx.x;
   if (i >= A.nc || !(A.mass[i] > 0.0)) return;
   const int nact = *A.pnact;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double* u = B.gcap + (size_t)i * A.ng;
-  for (int a = threadIdx.x; a < nact; a += blockDim.x) {
+  for (int a0 = 0; a0 < nact; a0 += 32) {
+    const int a = a0 + lane;
     double acc = 0.0;
-    for (int g = 0; g < A.ng; ++g) {
-      const double x = A.xstab[(size_t)g * A.maxact + a];
-      const double ug = u[g];
-      if (x != 0.0 && ug != 0.0) acc = acc + ug * x * pc_mbarn;
+    if (a < nact) {
+#pragma unroll 4
+      for (int g = warp; g < A.ng; g += BFB_WARPS) {
+        const double x = A.xstab[(size_t)g * A.maxact + a];
+        const double ug = u[g];
+        if (x != 0.0 && ug != 0.0) acc = acc + ug * x * pc_mbarn;
+      }
+      part[warp * A.maxact + a] = acc;
     }
-    if (acc != 0.0) B.goc[(size_t)A.act_slot[a] * A.nc + i] += acc;
+  }
+  __syncthreads();
+  for (int a = threadIdx.x; a < nact; a += blockDim.x) {
+    double sum = 0.0;
+    for (int w = 0; w < BFB_WARPS; ++w) sum = sum + part[w * A.maxact + a];
+    if (sum != 0.0) B.goc[(size_t)A.act_slot[a] * A.nc + i] += sum;
   }
 }
 
@@ -825,6 +903,14 @@ __global__ void opac_cell_bwd_kernel(int nc, int nelem, int nst, const int32_t* 
 }  // namespace
 
 // ============================================================ launchers
+// Shared memory of opacity_fwd_kernel's staged population rows (sets
+// A.stage_rows); rows beyond 40 KB are read from grndlev instead.
+static size_t fwd_rows_smem(OpacArgs& A) {
+  const size_t b = sizeof(double) * 32 * (size_t)A.nlrow;
+  A.stage_rows = (!A.nobb && A.nlrow > 0 && b <= 40 * 1024) ? 1 : 0;
+  return A.stage_rows ? b : 0;
+}
+
 // Everything the opacity kernels read, queued on the stream: sub-group edges,
 // the line binning, per-cell terms (and gas_sig) and the bound-free table.
 static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_flags* flags, double* gas_sig,
@@ -882,7 +968,7 @@ static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_f
   } else {
     cudaMemsetAsync(d_lstart, 0, sizeof(int) * (nedge + 3), st);
   }
-  opac_cell_prep_kernel<<<(nc + 127) / 128, 128, 0, st>>>(
+  opac_cell_prep_kernel<<<dim3((nc + 127) / 128, nelem), 128, 0, st>>>(
       nc, nelem, nst, ctx->d_ion_ni, gas->temp, gas->natom, gas->nelec, gas->vol, gas->mass, gas->oc,
       gas->ginv, flags->nothmson, d_hckt, gas_sig, d_hlp, d_grnd, d_ffigg, d_ffdgg);
   const bool do_bf = !flags->nobf;
@@ -916,7 +1002,8 @@ int launch_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_
   if (rc) return rc;
   A.cap32 = gas_cap; A.emiss32 = gas_emiss; A.cap64 = cap64;
   dim3 grid((A.nc + OPAC_CT - 1) / OPAC_CT, (A.ng + OPAC_GT - 1) / OPAC_GT);
-  opacity_fwd_kernel<<<grid, OPAC_GT * 32, 0, ctx->stream>>>(A);
+  const size_t shm = fwd_rows_smem(A);
+  opacity_fwd_kernel<<<grid, OPAC_GT * 32, shm, ctx->stream>>>(A);
   return cuda_check(ctx, cudaGetLastError(), "opacity_fwd launch");
 }
 
@@ -930,7 +1017,8 @@ int launch_physical_opacity64(slg_ctx* ctx, const slg_gas* gas, double* gas_sig,
   if (rc) return rc;
   A.cap32 = gas_cap; A.emiss32 = gas_emiss; A.capg64 = capg64;
   dim3 grid((A.nc + OPAC_CT - 1) / OPAC_CT, (A.ng + OPAC_GT - 1) / OPAC_GT);
-  opacity_fwd_kernel<<<grid, OPAC_GT * 32, 0, ctx->stream>>>(A);
+  const size_t shm = fwd_rows_smem(A);
+  opacity_fwd_kernel<<<grid, OPAC_GT * 32, shm, ctx->stream>>>(A);
   return cuda_check(ctx, cudaGetLastError(), "opacity_fwd launch");
 }
 
@@ -965,7 +1053,7 @@ int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, con
   cudaMemsetAsync(goc, 0, sizeof(double) * (size_t)nslot * nc, st);
   cudaMemsetAsync(gfr, 0, sizeof(double) * (size_t)nc * (A.nelem + 1), st);
   OpacBwd B{gcap, gT, ggrnd, goc, ghlp, gfr};
-  const size_t shm = sizeof(double) * ((size_t)(A.nlrow + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
+  const size_t shm = sizeof(double) * ((size_t)(2 * A.nlrow + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
   if (shm > 200 * 1024) return set_error(ctx, SLG_ERR_ARG, "opacity adjoint: too many ion slots (%d)", A.nlrow);
   static size_t shm_set = 0;  // raised only when needed
   if (shm > 48 * 1024 && shm > shm_set) {
@@ -974,7 +1062,16 @@ int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, con
   }
   dim3 grid((nc + OPAC_CT - 1) / OPAC_CT, (A.ng + OPAC_GT - 1) / OPAC_GT);
   opacity_bwd_kernel<<<grid, OPAC_GT * 32, shm, st>>>(A, B);
-  if (!A.nobf) bf_bwd_kernel<<<nc, 128, 0, st>>>(A, B);
+  if (!A.nobf) {
+    const size_t bshm = sizeof(double) * BFB_WARPS * (size_t)A.maxact;
+    if (bshm > 200 * 1024) return set_error(ctx, SLG_ERR_ARG, "opacity adjoint: too many ion slots (%d)", A.maxact);
+    static size_t bshm_set = 0;
+    if (bshm > 48 * 1024 && bshm > bshm_set) {
+      cudaFuncSetAttribute(bf_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      bshm_set = 200 * 1024;
+    }
+    bf_bwd_kernel<<<nc, BFB_WARPS * 32, bshm, st>>>(A, B);
+  }
   opac_cell_bwd_kernel<<<(nc + 127) / 128, 128, 0, st>>>(nc, A.nelem, A.nst, ctx->d_ion_ni, gas->natom, gas->nelec,
                                                          gas->vol, gas->mass, gas->ginv, 0, ggrnd, ghlp, gsig, goc,
                                                          gnelec, gnatom);

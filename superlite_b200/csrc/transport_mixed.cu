@@ -106,12 +106,6 @@ __device__ inline float capf(const TrnArgs& A, int ig, int ic) {
   return __ldg(A.cap + (size_t)(ic - 1) * A.ng + (ig - 1));
 }
 
-// Start loading the line holding *p into L1 (no register is written, so the
-// thread does not wait for it).
-__device__ inline void prefetch_l1(const void* p) {
-  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-}
-
 // Sentinels of the rate table's first component (a rate is >= 0).
 constexpr float kRateLumped = -1.0f;  // cap * dist >= taulump in a shell with lumped groups
 constexpr float kRateIMC = -2.0f;     // (sig + cap) * dist < tauddmc: IMC in this shell
@@ -664,15 +658,6 @@ __global__ void __launch_bounds__(MIX_BLOCK, MINB) particle_advance_mixed_kernel
     if (__all_sync(0xffffffffu, !have && queue_done)) break;
     if (!have) continue;
     istep++;
-    {
-      // The event's first reads -- its shell's record and this group's rate
-      // (DDMC) or opacity (IMC) entry -- are known here: start them towards L1
-      // so that their L2 latency overlaps the Philox rounds below.
-      const size_t gcell = (size_t)(vco + p.ix - 1);
-      prefetch_l1(A.mcell + gcell);
-      if (p.itype == 1 || A.puretran) prefetch_l1(A.cap + gcell * A.ng + (p.ig - 1));
-      else prefetch_l1(A.mrate + gcell * A.ng + (p.ig - 1));
-    }
     rng.begin_event((uint32_t)istep);
     const MView v{vnx, vco, vxo};
     const int icold = v.co + p.ix, igold = p.ig;  // cell over all models, 1-based
