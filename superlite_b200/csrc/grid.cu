@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(GB) leakage_bwd_kernel(const LeakArgsT<double>
   const double speclump = ol[6], ol1 = ol[0], ol2 = ol[1];
   const double u1 = u[0], u2 = u[1], u7 = u[6], u8 = u[7], u11 = u[10];
   const double vterm = 3.0 * A.vol[i - 1] / pc_pi4;
-  double gs = 0.0, gt = 0.0;
+  double gs = 0.0, gt = 0.0, gsl = 0.0, gsr = 0.0;  // gsl, gsr: the neighbours' sigma, reduced once per block
   for (int ig = threadIdx.x + 1; ig <= ng; ig += GB) {
     const double cg = capl[ig - 1];
     if (!(cg * dist >= A.taulump && (sigl + cg) * dist >= A.tauddmc)) continue;
@@ -305,11 +305,11 @@ __global__ void __launch_bounds__(GB) leakage_bwd_kernel(const LeakArgsT<double>
     gs += ua * da + ub * db;
     if (lint) {
       atomicAdd(&gcap[(size_t)(c - 1) * ng + ig - 1], ua * dal);
-      atomicAdd(&gsig[c - 1], ua * dal);
+      gsl += ua * dal;
     }
     if (rint) {
       atomicAdd(&gcap[(size_t)(c + 1) * ng + ig - 1], ub * dbr);
-      atomicAdd(&gsig[c + 1], ub * dbr);
+      gsr += ub * dbr;
     }
   }
   if (u11 != 0.0) {
@@ -329,9 +329,13 @@ __global__ void __launch_bounds__(GB) leakage_bwd_kernel(const LeakArgsT<double>
   }
   gs = block_sum(gs, sh);
   gt = block_sum(gt, sh);
+  gsl = block_sum(gsl, sh);
+  gsr = block_sum(gsr, sh);
   if (threadIdx.x == 0) {
     atomicAdd(&gsig[c], gs);
     gT[c] += gt;
+    if (gsl != 0.0) atomicAdd(&gsig[c - 1], gsl);
+    if (gsr != 0.0) atomicAdd(&gsig[c + 1], gsr);
   }
 }
 

@@ -193,19 +193,26 @@ __global__ void ion_active_kernel(int nc, const double* __restrict__ oc, int* __
 }
 
 // Active slots in the reference's loop order (iz ascending, ii = 1..min(iz,ni-1)),
-// physical_opacity.f:180-181.  Single thread; nelem*nst is at most a few hundred.
+// physical_opacity.f:180-181: that order is increasing slot = (iz-1) nst + (ii-1),
+// so one warp compacts the valid, populated slots 32 at a time with a ballot.
 __global__ void ion_compact_kernel(int nelem, int nst, const int32_t* __restrict__ ion_ni,
                                    const int* __restrict__ active, int16_t* __restrict__ act_slot,
                                    int* __restrict__ nact) {
+  const int lane = threadIdx.x & 31;
+  const int nslot = nelem * nst;
   int n = 0;
-  for (int iz = 1; iz <= nelem; ++iz) {
-    const int lim = min(iz, ion_ni[iz - 1] - 1);
-    for (int ii = 1; ii <= lim && ii <= nst; ++ii) {
-      const int s = (iz - 1) * nst + (ii - 1);
-      if (active[s]) act_slot[n++] = (int16_t)s;
+  for (int k0 = 0; k0 < nslot; k0 += 32) {
+    const int k = k0 + lane;
+    bool ok = false;
+    if (k < nslot) {
+      const int iz = k / nst + 1, ii = k % nst + 1;
+      ok = ii <= min(iz, ion_ni[iz - 1] - 1) && active[k] != 0;
     }
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    if (ok) act_slot[n + __popc(m & ((1u << lane) - 1u))] = (int16_t)k;
+    n += __popc(m);
   }
-  *nact = n;
+  if (lane == 0) *nact = n;
 }
 
 // Sub-group edges wlsub (physical_opacity.f:65-78), padded with DBL_MAX.
@@ -833,10 +840,11 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArg
 // Bound-free part of the adjoint (physical_opacity.f:163-195, ngs = 1):
 // d cap(g, i) / d oc(slot, i) = xs(g, slot) mbarn, so
 // goc(slot, i) += sum_g gcap(g, i) xs(g, slot) mbarn over the active slots.
-// One block of BFB_WARPS warps per shell: warp w sums the groups g = w, w +
-// BFB_WARPS, ... for 32 slots at a time (lane = slot, the table row is read
-// coalesced), the warps' partial sums are added through shared memory.  Runs
-// after opacity_bwd_kernel and before opac_cell_bwd_kernel (one writer per entry).
+// Blocks of BFB_WARPS warps per (shell, chunk of groups): warp w sums the
+// chunk's groups g = w, w + BFB_WARPS, ... for 32 slots at a time (lane =
+// slot, the table row is read coalesced), the warps' partial sums are added
+// through shared memory and the chunks' sums with atomics.  Runs after
+// opacity_bwd_kernel and before opac_cell_bwd_kernel.
 constexpr int BFB_WARPS = 8;
 __global__ void __launch_bounds__(BFB_WARPS * 32) bf_bwd_kernel(const OpacArgs A, const OpacBwd B) {
   extern __shared__ double part[];  // [warp][active slot]
@@ -845,12 +853,15 @@ __global__ void __launch_bounds__(BFB_WARPS * 32) bf_bwd_kernel(const OpacArgs A
   const int nact = *A.pnact;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double* u = B.gcap + (size_t)i * A.ng;
+  // this block's share of the groups: chunk blockIdx.y of gridDim.y
+  const int gchunk = (A.ng + gridDim.y - 1) / gridDim.y;
+  const int g0 = blockIdx.y * gchunk, g1 = min(A.ng, g0 + gchunk);
   for (int a0 = 0; a0 < nact; a0 += 32) {
     const int a = a0 + lane;
     double acc = 0.0;
     if (a < nact) {
 #pragma unroll 4
-      for (int g = warp; g < A.ng; g += BFB_WARPS) {
+      for (int g = g0 + warp; g < g1; g += BFB_WARPS) {
         const double x = A.xstab[(size_t)g * A.maxact + a];
         const double ug = u[g];
         if (x != 0.0 && ug != 0.0) acc = acc + ug * x * pc_mbarn;
@@ -862,7 +873,7 @@ __global__ void __launch_bounds__(BFB_WARPS * 32) bf_bwd_kernel(const OpacArgs A
   for (int a = threadIdx.x; a < nact; a += blockDim.x) {
     double sum = 0.0;
     for (int w = 0; w < BFB_WARPS; ++w) sum = sum + part[w * A.maxact + a];
-    if (sum != 0.0) B.goc[(size_t)A.act_slot[a] * A.nc + i] += sum;
+    if (sum != 0.0) atomicAdd(&B.goc[(size_t)A.act_slot[a] * A.nc + i], sum);
   }
 }
 
@@ -875,20 +886,26 @@ __global__ void opac_cell_bwd_kernel(int nc, int nelem, int nst, const int32_t* 
                                      const double* __restrict__ ggrnd, const double* __restrict__ ghlp,
                                      const double* __restrict__ gsig, double* __restrict__ goc,
                                      double* __restrict__ gnelec, double* __restrict__ gnatom) {
+  // one thread per (shell i, element iz = blockIdx.y + 1); element 1's threads
+  // also write the shell's scalars
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nc) return;
   if (!(mass[i] > 0.0)) {
-    gnelec[i] = 0.0;
-    gnatom[i] = 0.0;
+    if (blockIdx.y == 0) {
+      gnelec[i] = 0.0;
+      gnatom[i] = 0.0;
+    }
     return;
   }
-  for (int iz = 1; iz <= nelem; ++iz) {
+  {
+    const int iz = blockIdx.y + 1;
     const int lim = min(iz, ion_ni[iz - 1] - 1);
     for (int ii = 1; ii <= lim && ii <= nst; ++ii) {
       const size_t k = ((size_t)(iz - 1) * nst + (ii - 1)) * nc + i;
       goc[k] += ggrnd[k] * ginv[k];
     }
   }
+  if (blockIdx.y != 0) return;
   const double nd = natom[i] / vol[i];
   double gne = ghlp[i] * nd * nd;
   double gna = ghlp[i] * 2.0 * nd * nelec[i] / vol[i];
@@ -975,7 +992,7 @@ static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_f
   if (do_bf) {
     dim3 ga((nc + 255) / 256 < 8 ? (nc + 255) / 256 : 8, nslot);
     ion_active_kernel<<<ga, 256, 0, st>>>(nc, gas->oc, d_active);
-    ion_compact_kernel<<<1, 1, 0, st>>>(nelem, nst, ctx->d_ion_ni, d_active, d_act, d_nact);
+    ion_compact_kernel<<<1, 32, 0, st>>>(nelem, nst, ctx->d_ion_ni, d_active, d_act, d_nact);
     const int64_t nt = (int64_t)ngsub * nslot;
     bf_table_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(ngsub, nslot, d_nact, d_act, nst, d_wlsub,
                                                                   ctx->d_ph1, ctx->d_ph2, d_xs);
@@ -1070,9 +1087,12 @@ int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, con
       cudaFuncSetAttribute(bf_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
       bshm_set = 200 * 1024;
     }
-    bf_bwd_kernel<<<nc, BFB_WARPS * 32, bshm, st>>>(A, B);
+    // enough blocks to fill the GPU several times: group chunks of >= 64 groups
+    int nsplit = (4 * ctx->num_sms + nc - 1) / nc;
+    nsplit = nsplit < 1 ? 1 : (nsplit > (A.ng + 63) / 64 ? (A.ng + 63) / 64 : nsplit);
+    bf_bwd_kernel<<<dim3(nc, nsplit), BFB_WARPS * 32, bshm, st>>>(A, B);
   }
-  opac_cell_bwd_kernel<<<(nc + 127) / 128, 128, 0, st>>>(nc, A.nelem, A.nst, ctx->d_ion_ni, gas->natom, gas->nelec,
+  opac_cell_bwd_kernel<<<dim3((nc + 127) / 128, A.nelem), 128, 0, st>>>(nc, A.nelem, A.nst, ctx->d_ion_ni, gas->natom, gas->nelec,
                                                          gas->vol, gas->mass, gas->ginv, 0, ggrnd, ghlp, gsig, goc,
                                                          gnelec, gnatom);
   return cuda_check(ctx, cudaGetLastError(), "opacity adjoint launch");
