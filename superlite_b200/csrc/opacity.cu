@@ -839,41 +839,44 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArg
 
 // Bound-free part of the adjoint (physical_opacity.f:163-195, ngs = 1):
 // d cap(g, i) / d oc(slot, i) = xs(g, slot) mbarn, so
-// goc(slot, i) += sum_g gcap(g, i) xs(g, slot) mbarn over the active slots.
-// Blocks of BFB_WARPS warps per (shell, chunk of groups): warp w sums the
-// chunk's groups g = w, w + BFB_WARPS, ... for 32 slots at a time (lane =
-// slot, the table row is read coalesced), the warps' partial sums are added
-// through shared memory and the chunks' sums with atomics.  Runs after
-// opacity_bwd_kernel and before opac_cell_bwd_kernel.
-constexpr int BFB_WARPS = 8;
-__global__ void __launch_bounds__(BFB_WARPS * 32) bf_bwd_kernel(const OpacArgs A, const OpacBwd B) {
-  extern __shared__ double part[];  // [warp][active slot]
-  const int i = blockIdx.x;
-  if (i >= A.nc || !(A.mass[i] > 0.0)) return;
+// goc(act_slot(a), i) += mbarn sum_g gcap(g, i) xs(g, a) over the active slots a
+// -- a product of the (shell, group) gradient with the (group, slot) table.
+// Tiled like a matrix product: a block computes 32 shells x 32 slots, staging
+// 32 groups of both operands in shared memory per round; thread (tx, ty)
+// holds shell tx and slots ty, ty + 8, ty + 16, ty + 24.  Runs after
+// opacity_bwd_kernel and before opac_cell_bwd_kernel (one writer per entry).
+constexpr int BFB_T = 32;
+__global__ void __launch_bounds__(BFB_T * 8) bf_bwd_kernel(const OpacArgs A, const OpacBwd B) {
+  __shared__ double su[BFB_T][BFB_T + 1];  // [shell][group]
+  __shared__ double sx[BFB_T][BFB_T + 1];  // [group][slot]
   const int nact = *A.pnact;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const double* u = B.gcap + (size_t)i * A.ng;
-  // this block's share of the groups: chunk blockIdx.y of gridDim.y
-  const int gchunk = (A.ng + gridDim.y - 1) / gridDim.y;
-  const int g0 = blockIdx.y * gchunk, g1 = min(A.ng, g0 + gchunk);
-  for (int a0 = 0; a0 < nact; a0 += 32) {
-    const int a = a0 + lane;
-    double acc = 0.0;
-    if (a < nact) {
-#pragma unroll 4
-      for (int g = g0 + warp; g < g1; g += BFB_WARPS) {
-        const double x = A.xstab[(size_t)g * A.maxact + a];
-        const double ug = u[g];
-        if (x != 0.0 && ug != 0.0) acc = acc + ug * x * pc_mbarn;
-      }
-      part[warp * A.maxact + a] = acc;
+  const int a0 = blockIdx.y * BFB_T;
+  if (a0 >= nact) return;  // uniform over the block
+  const int i0 = blockIdx.x * BFB_T;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int g0 = 0; g0 < A.ng; g0 += BFB_T) {
+    for (int k = threadIdx.x; k < BFB_T * BFB_T; k += blockDim.x) {
+      const int r = k >> 5, q = k & 31;  // su: shell r, group q (coalesced over groups); sx: group r, slot q
+      const int ii = i0 + r, g = g0 + q, gr = g0 + r, a = a0 + q;
+      su[r][q] = (ii < A.nc && g < A.ng) ? B.gcap[(size_t)ii * A.ng + g] : 0.0;
+      sx[r][q] = (gr < A.ng && a < nact) ? A.xstab[(size_t)gr * A.maxact + a] : 0.0;
     }
+    __syncthreads();
+#pragma unroll 8
+    for (int q = 0; q < BFB_T; ++q) {
+      const double u = su[tx][q];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[j] = acc[j] + u * sx[q][ty + 8 * j];
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  for (int a = threadIdx.x; a < nact; a += blockDim.x) {
-    double sum = 0.0;
-    for (int w = 0; w < BFB_WARPS; ++w) sum = sum + part[w * A.maxact + a];
-    if (sum != 0.0) atomicAdd(&B.goc[(size_t)A.act_slot[a] * A.nc + i], sum);
+  const int i = i0 + tx;
+  if (i >= A.nc || !(A.mass[i] > 0.0)) return;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int a = a0 + ty + 8 * j;
+    if (a < nact && acc[j] != 0.0) B.goc[(size_t)A.act_slot[a] * A.nc + i] += acc[j] * pc_mbarn;
   }
 }
 
@@ -1080,17 +1083,8 @@ int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, con
   dim3 grid((nc + OPAC_CT - 1) / OPAC_CT, (A.ng + OPAC_GT - 1) / OPAC_GT);
   opacity_bwd_kernel<<<grid, OPAC_GT * 32, shm, st>>>(A, B);
   if (!A.nobf) {
-    const size_t bshm = sizeof(double) * BFB_WARPS * (size_t)A.maxact;
-    if (bshm > 200 * 1024) return set_error(ctx, SLG_ERR_ARG, "opacity adjoint: too many ion slots (%d)", A.maxact);
-    static size_t bshm_set = 0;
-    if (bshm > 48 * 1024 && bshm > bshm_set) {
-      cudaFuncSetAttribute(bf_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-      bshm_set = 200 * 1024;
-    }
-    // enough blocks to fill the GPU several times: group chunks of >= 64 groups
-    int nsplit = (4 * ctx->num_sms + nc - 1) / nc;
-    nsplit = nsplit < 1 ? 1 : (nsplit > (A.ng + 63) / 64 ? (A.ng + 63) / 64 : nsplit);
-    bf_bwd_kernel<<<dim3(nc, nsplit), BFB_WARPS * 32, bshm, st>>>(A, B);
+    const dim3 bgrid((nc + BFB_T - 1) / BFB_T, (A.maxact + BFB_T - 1) / BFB_T);
+    bf_bwd_kernel<<<bgrid, BFB_T * 8, 0, st>>>(A, B);
   }
   opac_cell_bwd_kernel<<<dim3((nc + 127) / 128, A.nelem), 128, 0, st>>>(nc, A.nelem, A.nst, ctx->d_ion_ni, gas->natom, gas->nelec,
                                                          gas->vol, gas->mass, gas->ginv, 0, ggrnd, ghlp, gsig, goc,
