@@ -79,11 +79,15 @@ __device__ inline void exp_table_load(double* s_tab) {
   for (int k = threadIdx.x; k < 64; k += blockDim.x) s_tab[k] = kExp2Tab64[k];
 }
 
-// tab: kExp2Tab64 in shared memory.
+// tab: kExp2Tab64 in shared memory.  n = nearest integer of x 64/ln2 by the
+// add-and-subtract of 1.5 2^52 (|x 64/ln2| < 2^31, so the sum's low 32 bits
+// are n in two's complement and the difference is n exactly).
 __device__ inline double exp_tang(double x, const double* tab) {
   if (!(fabs(x) <= 700.0)) return exp(x);  // also NaN
-  const double n = rint(x * kExpInvL);
-  const int ni = (int)n;
+  constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
+  const double big = fma(x, kExpInvL, kRound);
+  const int ni = (int)__double2loint(big);
+  const double n = big - kRound;
   double r = fma(-n, kExpL1, x);
   r = fma(-n, kExpL2, r);
   double p = fma(r, 1.0 / 120.0, 1.0 / 24.0);
