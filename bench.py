@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=None,
                     help="timed steps (default 1 for the batched workload, whose step runs about a minute; 3 otherwise)")
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--no-tune-steps", dest="tune_steps", action="store_false",
+                    help="batched workload: keep the sample autotuner's variant instead of timing each variant on "
+                         "one whole untimed step")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--npart", type=float, default=5e7)
     ap.add_argument("--ncell", type=int, default=256)
@@ -531,13 +534,30 @@ def run_batched(a):
     stream = ts.stream
     seed0 = 1000 * (rank + 1)
     # warm-up 1: sources and opacities, the autotuner on a sample of this
-    # step's particles, then the particle loop with the chosen variant
+    # step's particles (the first 1e6 slots), then the particle loop with the
+    # chosen variant
     ts.prepare(seed0 - 1)
     variant, tune_ms = ts.autotune(seed=seed0 - 1, nsample=1_000_000)
     ts.finish(seed0 - 1)
     ts.sync()
-    # warm-ups 2..W (uncaptured); the last one also times its phases
+    # the kernel variants on whole steps (untimed, beside the warm-ups): the
+    # sample above comes from the first models' particles only, so each variant
+    # runs one full particle loop, timed with CUDA events, and the fastest is
+    # kept for the warm-ups and the timed steps
     ev_p = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    full_ms = {}
+    if a.tune_steps:
+        for v in range(4):
+            hot._check(hot.lib.slg_set_transport_variant(hot.h, v))
+            ts.prepare(seed0 - 10 - v)
+            ev_p[1].record(stream)
+            ts.finish(seed0 - 10 - v)
+            ev_p[2].record(stream)
+            ts.sync()
+            full_ms[v] = ev_p[1].elapsed_time(ev_p[2])
+        variant = min(full_ms, key=full_ms.get)
+        hot._check(hot.lib.slg_set_transport_variant(hot.h, variant))
+    # warm-ups 2..W (uncaptured); the last one also times its phases
     t_prep = t_tr = None
     for k in range(1, a.warmup):
         if k == a.warmup - 1:
@@ -621,7 +641,8 @@ def run_batched(a):
                                       f"peak {peak_kind}"}},
         "pipe_peaks": {k: pipes[k]["value"] for k in ("fp64_fma_flops", "fp64_exp_per_s", "fp32_fma_flops",
                                                       "int32_imad_per_s", "warp_inst_issue_per_s")},
-        "clocks": clocks, "autotune": {"variant": variant, "sample_ms": tune_ms},
+        "clocks": clocks, "autotune": {"variant": variant, "sample_ms": tune_ms,
+                                       "particle_loop_ms_by_variant": {str(k): v for k, v in full_ms.items()} or None},
         "gpu_launches": None,
     }
     # kernels of one step: 6 (sources) + 1 (analytic opacity) + 1 (means) + 1 (leakage) + 1 (emitprob)

@@ -318,7 +318,9 @@ int slg_dev_sourcetally(slg_ctx* ctx, int64_t npart, const slg_packet* prt,
 int slg_autotune_transport(slg_ctx* ctx, const slg_transport_in* in, const slg_packet* prt,
                            const int32_t* isvacant, int64_t npart, uint64_t seed,
                            int64_t nsample, int32_t* best, float* ms);
-/* Select a transport kernel variant (0..3) explicitly. */
+/* Select the transport kernel variant (0..3, register budget / resident
+ * blocks, as slg_autotune_transport times them) of both precisions explicitly,
+ * e.g. after timing each on full launches of the caller's own workload. */
 int slg_set_transport_variant(slg_ctx* ctx, int32_t variant);
 /* radtemp, prt and isvacant on the device; emit and nvol are host arrays. */
 int slg_dev_interior_source(slg_ctx* ctx, const double* radtemp, const double* emit,

@@ -761,7 +761,8 @@ int slg_autotune_transport(slg_ctx* ctx, const slg_transport_in* in, const slg_p
 
 int slg_set_transport_variant(slg_ctx* ctx, int32_t variant) {
   if (!ctx || variant < 0 || variant > 3) return set_error(ctx, SLG_ERR_ARG, "variant must be 0..3");
-  ctx->trn_variant = variant;
+  ctx->trn_variant = variant;  // FP64 loop
+  ctx->mix_variant = variant;  // mixed-precision loop
   return SLG_OK;
 }
 
