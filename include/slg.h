@@ -106,7 +106,8 @@ int slg_set_models(slg_ctx* ctx, int32_t nmodel, const int32_t* nx, const int64_
 /* Permanent atomic data after bcast_permanent (mpimod_mpi.f:23-501):
  * ion_el(iz)%ni (nelem), the bb line list sorted by wl0 (read_bbxs_data.f:84),
  * bf_ph1(6,7,30,30), bf_ph2(7,30,30) (bfxsmod.f:14) and ff_gff(81,41)
- * (ffxsmod.f:18-20).  nstage = slots per element in the oc/ginv arrays. */
+ * (ffxsmod.f:18-20).  nstage = slots per element in the oc/ginv arrays
+ * (1..64; nelem 1..30). */
 int slg_set_atomic_data(slg_ctx* ctx, int32_t nelem, int32_t nstage, const int32_t* ion_ni,
                         int64_t nline, const slg_bbxs* bb_xs, const float* bf_ph1,
                         const float* bf_ph2, const double* ff_gff);
@@ -434,6 +435,11 @@ void* slg_stream(slg_ctx* ctx);
  * chains per thread, timed with CUDA events after one warm-up launch; *ms
  * (optional) receives the launch time.  Allocates and frees its own buffer. */
 int slg_pipe_throughput(int device, int which, int iters, double* ops_per_s, float* ms);
+
+/* y[k] = the opacity kernels' FP64 exp (Tang's table-driven method) of x[k]
+ * on device `device`, k < n (host arrays; no counterpart in the reference: an
+ * accuracy check of that exp against a host libm).  Synchronous. */
+int slg_exp_eval(int device, int64_t n, const double* x, double* y);
 
 #ifdef __cplusplus
 }

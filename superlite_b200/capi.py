@@ -104,6 +104,7 @@ SIGNATURES = {
     "slg_transport_totals": (C.c_int, [vp, vp, C.c_int32]),
     "slg_stream": (vp, [vp]),
     "slg_pipe_throughput": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
+    "slg_exp_eval": (C.c_int, [C.c_int, C.c_int64, C.c_void_p, C.c_void_p]),
 }
 
 _LIB = None

@@ -4,6 +4,7 @@
 // buffers, call the device-pointer form on the context's stream, copy the
 // outputs back and synchronise.  Device-pointer entry points only queue work.
 #include <cuda_runtime.h>
+#include <cmath>
 #include <cstdarg>
 #include <cstring>
 #include <algorithm>
@@ -391,7 +392,7 @@ int slg_set_models(slg_ctx* ctx, int32_t nmodel, const int32_t* nx, const int64_
 
 int slg_set_atomic_data(slg_ctx* ctx, int32_t nelem, int32_t nstage, const int32_t* ion_ni, int64_t nline,
                         const slg_bbxs* bb_xs, const float* bf_ph1, const float* bf_ph2, const double* ff_gff) {
-  if (!ctx || nelem < 1 || nelem > 30 || nstage < 1 || !ion_ni || nline < 0 || (nline > 0 && !bb_xs))
+  if (!ctx || nelem < 1 || nelem > 30 || nstage < 1 || nstage > 64 || !ion_ni || nline < 0 || (nline > 0 && !bb_xs))
     return set_error(ctx, SLG_ERR_ARG, "slg_set_atomic_data: bad arguments");
   if (nline > 0x7fffffffLL) return set_error(ctx, SLG_ERR_ARG, "slg_set_atomic_data: too many lines");
   for (int64_t l = 0; l + 1 < nline; ++l)
@@ -424,6 +425,14 @@ int slg_set_atomic_data(slg_ctx* ctx, int32_t nelem, int32_t nstage, const int32
   // d cap / d population for those rows only)
   const int nslot = nelem * nstage;
   std::vector<int16_t> row_of(nslot, (int16_t)-1), slot_of;
+  // the largest lower-level energy: the opacity kernels skip the range check
+  // of their exp for a shell with hc/kT * chimax <= 700 (infinite when a
+  // value is negative or NaN: every term is then checked)
+  double chimax = 0.0;
+  for (int64_t l = 0; l < nline; ++l) {
+    const double c = (double)bb_xs[l].chilw;
+    chimax = (c >= 0.0 && chimax < INFINITY) ? (c > chimax ? c : chimax) : INFINITY;
+  }
   for (int64_t l = 0; l < nline; ++l) {
     const int sl = (bb_xs[l].iz - 1) * nstage + (bb_xs[l].ii - 1);
     if (row_of[sl] < 0) {
@@ -446,6 +455,7 @@ int slg_set_atomic_data(slg_ctx* ctx, int32_t nelem, int32_t nstage, const int32
   ctx->nstage = nstage;
   ctx->nline = nline;
   ctx->nlrow = (int)slot_of.size();
+  ctx->line_chimax = chimax;
   ctx->h_ion_ni.assign(ion_ni, ion_ni + nelem);
   return SLG_OK;
 }

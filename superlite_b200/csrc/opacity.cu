@@ -185,6 +185,42 @@ __global__ void opac_cell_prep_kernel(int nc, int nelem, int nst, const int32_t*
   }
 }
 
+// Free-free, summed over elements once per shell.  For fixed table columns
+// (igg, dgg) of each element, the reference's bilinear gff (physical_opacity.f:
+// 234-237) is linear in the row weights (1 - du, du):
+//   g_z = (1 - du) Gz[iu - 1] + du Gz[iu],  Gz[j] = (1 - dgg) G[j, igg - 1] + dgg G[j, igg],
+// so sum_z z^2 fr_z g_z = (1 - du) S[iu - 1] + du S[iu] with
+// S[j] = sum_z z^2 fr_z Gz[j] over the elements without the gff >= 1 clamp
+// (:238, nonlinear); those are flagged in ffclamp (bit iz - 1) and added per
+// group.  Elements with fr = 0 add +0 in the reference (:240-241) and are left
+// out.  The sum is re-associated (one product by help per group instead of one
+// per element): a rounding-level difference.
+// One thread per (shell, table row j).
+__global__ void ff_sum_kernel(int nc, int nelem, const double* __restrict__ natomfr, const int* __restrict__ ffigg,
+                              const double* __restrict__ ffdgg, const double* __restrict__ G,
+                              double* __restrict__ ffsum, unsigned* __restrict__ ffclamp) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nc * FF_NU) return;
+  const int i = (int)(t / FF_NU), j = (int)(t % FF_NU);
+  const double* nfr = natomfr + (size_t)(nelem + 1) * i;
+  double S = 0.0;
+  unsigned clamp = 0;
+  for (int iz = 1; iz <= nelem; ++iz) {
+    const double fr = nfr[iz];
+    if (fr == 0.0) continue;
+    const int igg = ffigg[(size_t)(iz - 1) * nc + i];
+    if (igg < 0) {
+      clamp |= 1u << (iz - 1);
+      continue;
+    }
+    const double dgg = ffdgg[(size_t)(iz - 1) * nc + i];
+    const double gz = (1.0 - dgg) * G[j + FF_NU * (igg - 1)] + dgg * G[j + FF_NU * igg];
+    S = S + (double)(iz * iz) * fr * gz;
+  }
+  ffsum[(size_t)i * FF_NU + j] = S;
+  if (j == 0) ffclamp[i] = clamp;
+}
+
 // Which ion slots (iz,ii) carry any population: 1 if any cell has oc != 0.
 __global__ void ion_active_kernel(int nc, const double* __restrict__ oc, int* __restrict__ active) {
   const int k = blockIdx.y;
@@ -301,20 +337,71 @@ __global__ void bf_table_kernel(int ngsub, int maxact, const int* __restrict__ p
   const int iz = slot / nst + 1, ii = slot % nst + 1;
   const double wl = wlsub[igs - 1];
   const double en = pc_hc / (pc_ev * wl);
-  xstab[t] = bfxs(ph1, ph2, iz, iz - ii + 1, en);
+  xstab[t] = bfxs(ph1, ph2, iz, iz - ii + 1, en) * pc_mbarn;  // physical_opacity.f:185-186: xs*pc_mbarn first
 }
 
-// Per-line factors that do not depend on the shell, for the binned lines of
-// sub-groups 1..ngsub (lines outside the grid get zeros and are never read):
+// Per sub-group, the xstab entries with a nonzero cross section, in slot
+// order (one warp per sub-group, ballot compaction): xsc = bfxs * pc_mbarn,
+// bslot = the ion slot, bnnz = their count.  The reference skips xs == 0
+// (physical_opacity.f:184), so summing over the compacted entries adds the
+// same terms in the same order.
+__global__ void bf_compact_kernel(int ngsub, int maxact, const int* __restrict__ pnact,
+                                  const int16_t* __restrict__ act_slot, const double* __restrict__ xstab,
+                                  double* __restrict__ xsc, int* __restrict__ bslot, int* __restrict__ bnnz) {
+  const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (w >= ngsub) return;
+  const int nact = *pnact;
+  const size_t base = (size_t)w * maxact;
+  int k = 0;
+  for (int a0 = 0; a0 < nact; a0 += 32) {
+    const int a = a0 + lane;
+    const double x = a < nact ? xstab[base + a] : 0.0;
+    const bool nz = x != 0.0;
+    const unsigned m = __ballot_sync(0xffffffffu, nz);
+    if (nz) {
+      const int pos = k + __popc(m & ((1u << lane) - 1u));
+      xsc[base + pos] = x;
+      bslot[base + pos] = act_slot[a];
+    }
+    k += __popc(m);
+  }
+  if (lane == 0) bnnz[w] = k;
+}
+
+// One line's shell-independent factors, 16 bytes (one vector load per line):
 // pg = phi(igs) * gxs, the first product of the reference's expression
 // (physical_opacity.f:148-149), so the evaluation order of that product is
-// kept; chi = chilw in FP64; and the line's population row
-// slot = (iz - 1) nst + (ii - 1) of grndlev in the low 16 bits, the slot's
-// row among the rows the lines reference (lrow_of_slot) in the high 16 bits.
+// kept; and chilw in FP64 with two indices in the low 29 bits of its
+// mantissa.  chilw is single precision in the line record (as in the
+// reference's bbxs type), so those bits of its FP64 value are zero: masking
+// them off gives chilw exactly, without a conversion per line.  The indices:
+// bits 0..10 the line's row among the population rows the lines reference
+// (lrow_of_slot), bits 11..26 its population slot (iz - 1) nst + (ii - 1).
+struct __align__(16) LineTerm {
+  double pg;
+  double chi_idx;
+};
+constexpr int kLineRowBits = 11;
+constexpr unsigned kLineIdxMask = 0x1fffffffu;
+
+struct LineVals {
+  double pg, chi;
+  unsigned idx;
+};
+
+__device__ __forceinline__ LineVals load_line(const LineTerm* p) {
+  const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+  const unsigned lo = (unsigned)__double2loint(v.y);
+  return LineVals{v.x, __hiloint2double(__double2hiint(v.y), (int)(lo & ~kLineIdxMask)), lo & kLineIdxMask};
+}
+__device__ __forceinline__ int line_row(unsigned idx) { return (int)(idx & ((1u << kLineRowBits) - 1)); }
+__device__ __forceinline__ int line_slot(unsigned idx) { return (int)(idx >> kLineRowBits); }
+
+// The LineTerm of each binned line of sub-groups 1..ngsub (lines outside the
+// grid get zeros and are never read).
 __global__ void decode_lines_kernel(const slg_bbxs* __restrict__ bb, int64_t nline, const int* __restrict__ lstart,
                                     int ngsub, const double* __restrict__ wlsub, int nst,
-                                    const int16_t* __restrict__ lrow_of_slot, double2* __restrict__ lpc,
-                                    int* __restrict__ lslot) {
+                                    const int16_t* __restrict__ lrow_of_slot, LineTerm* __restrict__ lt) {
   const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= nline) return;
   // sub-group of line l: the largest igs with lstart[igs] <= l
@@ -325,18 +412,19 @@ __global__ void decode_lines_kernel(const slg_bbxs* __restrict__ bb, int64_t nli
     else hi = mid - 1;
   }
   const int igs = lo;
-  if (igs < 1 || igs > ngsub) {
-    lpc[l] = make_double2(0.0, 0.0);
-    lslot[l] = 0;
-    return;
+  LineTerm t{0.0, 0.0};
+  if (igs >= 1 && igs <= ngsub) {
+    const slg_bbxs r = bb[l];
+    const double wa = wlsub[igs - 1], wb = wlsub[igs];
+    const double wl = 0.5 * (wa + wb);
+    const double phi = wl * wl / ((wb - wa) * pc_c);
+    const int slot = (r.iz - 1) * nst + (r.ii - 1);
+    const double chi = (double)r.chilw;  // low 29 mantissa bits zero
+    const unsigned idx = ((unsigned)slot << kLineRowBits) | (unsigned)lrow_of_slot[slot];
+    t = LineTerm{phi * (double)r.gxs,
+                 __hiloint2double(__double2hiint(chi), (int)((unsigned)__double2loint(chi) | idx))};
   }
-  const slg_bbxs r = bb[l];
-  const double wa = wlsub[igs - 1], wb = wlsub[igs];
-  const double wl = 0.5 * (wa + wb);
-  const double phi = wl * wl / ((wb - wa) * pc_c);
-  lpc[l] = make_double2(phi * (double)r.gxs, (double)r.chilw);
-  const int slot = (r.iz - 1) * nst + (r.ii - 1);
-  lslot[l] = slot | ((int)lrow_of_slot[slot] << 16);
+  lt[l] = t;
 }
 
 struct OpacArgs {
@@ -348,15 +436,18 @@ struct OpacArgs {
   const double* grp_wl;
   const int* lstart;        // (ngsub+2)+1 offsets by igs
   const slg_bbxs* bb;
-  const double2* lpc;       // per line {phi(igs) gxs, chilw} (decode_lines_kernel)
-  const int* lslot;         // per line: population slot (low 16 bits), line row (high 16 bits)
+  const LineTerm* lt;       // per binned line (decode_lines_kernel)
+  double chimax;            // largest chilw of the lines (infinite: check every exp argument)
   const int16_t* slot_of_lrow;  // line row -> slot
   int nlrow;                // population rows the lines reference
   int stage_rows = 0;       // forward: stage those rows of a block's shells in shared memory
   const double* grndlev;    // [slot][cell]
   const double* oc;         // [slot][cell]
   const int16_t* act_slot;  // active slots, reference order
-  const double* xstab;      // [(igs-1)*maxact + a]
+  const double* xstab;      // [(igs-1)*maxact + a]: bfxs * pc_mbarn
+  const double* xsc;        // the nonzero entries of xstab per sub-group (bf_compact_kernel)
+  const int* bslot;         // their ion slots
+  const int* bnnz;          // their count per sub-group
   const double* hckt;
   const double* hlparr;
   const double* mass;
@@ -364,6 +455,8 @@ struct OpacArgs {
   const double* temp;
   const int* ffigg;         // [iz-1][cell], negative: apply gff >= 1
   const double* ffdgg;
+  const double* ffsum;      // [cell][81]: sum over unclamped elements of z^2 fr gff at each table row
+  const unsigned* ffclamp;  // [cell]: elements (bit iz-1) with fr != 0 under the gff >= 1 clamp
   const double* gff;        // (81,41)
   double ffc1;
   float* cap32;             // (ng, ncell)
@@ -372,6 +465,37 @@ struct OpacArgs {
   double* capg64 = nullptr; // (ng, ncell) optional: cap before sngl() in gas_cap's layout
   int* flags;
 };
+
+// Sum over n lines of pg * og * exp(-chi h), og the staged population of the
+// line's row for this lane's shell; four lines per round: their loads and exps
+// are independent, and the terms are added one after another in line order.
+// INRANGE: the caller has shown -chi h in [-700, 0] for every line.
+template <bool INRANGE>
+__device__ __forceinline__ double bb_sum_staged(const LineTerm* lt, int n, double h, const double* s_gl,
+                                                const double* etab) {
+  double sbb = 0.0;
+  int k = 0;
+  for (; k + 4 <= n; k += 4) {
+    LineVals t[4];
+    double og[4], e[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) t[q] = load_line(lt + k + q);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) og[q] = s_gl[line_row(t[q].idx) << 5];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      e[q] = INRANGE ? exp_tang_inrange(-(t[q].chi * h), etab) : exp_tang(-(t[q].chi * h), etab);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) sbb = sbb + t[q].pg * og[q] * e[q];
+  }
+  for (; k < n; ++k) {
+    const LineVals t = load_line(lt + k);
+    const double og = s_gl[line_row(t.idx) << 5];
+    const double e = INRANGE ? exp_tang_inrange(-(t.chi * h), etab) : exp_tang(-(t.chi * h), etab);
+    sbb = sbb + t.pg * og * e;
+  }
+  return sbb;
+}
 
 // One sub-group igs for shell i (lane `lane` of its block): bb, bf and ff in
 // the reference's order.  etab: the exp table (kExp2Tab64) in shared memory;
@@ -392,50 +516,35 @@ __device__ inline double subgroup_opacity(const OpacArgs& A, int i, int lane, in
       // sum over the sub-group's lines of phi gxs ocg exp(-chilw h), times the
       // stimulated-emission factor once (the reference multiplies each term by
       // it; the sum of positive terms differs by rounding only)
-      // four lines per round: their loads and exps are independent; the terms
-      // are still added one after another in line order, and a term of an
-      // unpopulated ion adds +0 (the reference skips it: the same sum)
-      double sbb = 0.0;
-      int l = l0;
-      for (; l + 4 <= l1; l += 4) {
-        double2 pc[4];
-        int sr[4];
-        double og[4], t[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          pc[q] = __ldg(A.lpc + l + q);
-          sr[q] = __ldg(A.lslot + l + q);
+      const LineTerm* lt = A.lt + l0;
+      const int n = l1 - l0;
+      double sbb;
+      // h * chimax <= 700: every exp argument -chi h lies in [-700, 0], where
+      // exp_tang needs no range check
+      const bool inrange = h >= 0.0 && h * A.chimax <= 700.0;
+      if (s_g) {
+        // staged populations are clamped at zero, so a term of an unpopulated
+        // ion adds +0 (the reference skips it: the same sum)
+        const double* s_gl = s_g + lane;
+        sbb = inrange ? bb_sum_staged<true>(lt, n, h, s_gl, etab) : bb_sum_staged<false>(lt, n, h, s_gl, etab);
+      } else {
+        sbb = 0.0;
+        for (int k = 0; k < n; ++k) {
+          const LineVals t = load_line(lt + k);
+          const double ocg = A.grndlev[(size_t)line_slot(t.idx) * A.nc + i];
+          if (ocg <= 0.0) continue;
+          sbb = sbb + t.pg * ocg * exp_tang(-(t.chi * h), etab);
         }
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-          og[q] = s_g ? s_g[(sr[q] >> 16) * 32 + lane] : A.grndlev[(size_t)(sr[q] & 0xffff) * A.nc + i];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) t[q] = !(og[q] <= 0.0) ? pc[q].x * og[q] * exp_tang(-(pc[q].y * h), etab) : 0.0;
-        sbb = sbb + t[0];
-        sbb = sbb + t[1];
-        sbb = sbb + t[2];
-        sbb = sbb + t[3];
-      }
-      for (; l < l1; ++l) {
-        const double2 pc = __ldg(A.lpc + l);
-        const int sr = __ldg(A.lslot + l);
-        const double ocg = s_g ? s_g[(sr >> 16) * 32 + lane] : A.grndlev[(size_t)(sr & 0xffff) * A.nc + i];
-        if (ocg <= 0.0) continue;
-        sbb = sbb + pc.x * ocg * exp_tang(-(pc.y * h), etab);
       }
       cap = cap + sbb * expfac;
     }
   }
   if (!A.nobf) {
-    const double* xs = A.xstab + (size_t)(igs - 1) * A.maxact;
-    const int nact = *A.pnact;
-    for (int a = 0; a < nact; ++a) {
-      const double x = xs[a];
-      if (x == 0.0) continue;
-      const double o = A.oc[(size_t)A.act_slot[a] * A.nc + i];
-      if (o == 0.0) continue;  // adds +0 in the reference
-      cap = cap + x * pc_mbarn * o;
-    }
+    const size_t base = (size_t)(igs - 1) * A.maxact;
+    const int n = A.bnnz[igs - 1];
+    const double* oci = A.oc + i;
+    for (int k = 0; k < n; ++k)  // bfxs * pc_mbarn (the reference's first product) * population
+      cap = cap + __ldg(A.xsc + base + k) * oci[(size_t)__ldg(A.bslot + base + k) * A.nc];
   }
   if (!A.noff) {
     const double wl = A.wlsub[igs - 1];
@@ -445,26 +554,26 @@ __device__ inline double subgroup_opacity(const OpacArgs& A, int i, int lane, in
     const int iu = ru < 1.0 ? 1 : (ru >= (double)(FF_NU - 1) ? FF_NU - 1 : (int)floor(ru));
     const double du = ru - iu;
     const double help = A.ffc1 * sqrt(h) * (1.0 - exp(-u)) * cube(wl) * A.hlparr[i];
-    const double* nfr = A.natomfr + (size_t)(A.nelem + 1) * i;
-    for (int iz = 1; iz <= A.nelem; ++iz) {
-      const double fr = nfr[iz];
-      if (fr == 0.0) continue;  // adds +0 in the reference
-      int igg = A.ffigg[(size_t)(iz - 1) * A.nc + i];
-      const bool clamp1 = igg < 0;
-      igg = clamp1 ? -igg : igg;
+    // sum over elements of z^2 fr gff (ff_sum_kernel), the clamped ones here
+    const double* S = A.ffsum + (size_t)i * FF_NU;
+    double sg = (1.0 - du) * __ldg(S + iu - 1) + du * __ldg(S + iu);
+    for (unsigned m = __ldg(A.ffclamp + i); m; m &= m - 1) {
+      const int iz = __ffs(m);
+      const int igg = -A.ffigg[(size_t)(iz - 1) * A.nc + i];
       const double dgg = A.ffdgg[(size_t)(iz - 1) * A.nc + i];
       const double* G = A.gff;
       double g = (1.0 - du) * (1.0 - dgg) * G[(iu - 1) + FF_NU * (igg - 1)] +
                  du * (1.0 - dgg) * G[iu + FF_NU * (igg - 1)] +
                  (1.0 - du) * dgg * G[(iu - 1) + FF_NU * igg] + du * dgg * G[iu + FF_NU * igg];
-      if (clamp1) g = g > 1.0 ? g : 1.0;
-      cap = cap + help * g * (double)(iz * iz) * fr;
+      g = g > 1.0 ? g : 1.0;
+      sg = sg + (double)(iz * iz) * A.natomfr[(size_t)(A.nelem + 1) * i + iz] * g;
     }
+    cap = cap + help * sg;
   }
   return cap;
 }
 
-__global__ void __launch_bounds__(OPAC_GT * 32) opacity_fwd_kernel(const OpacArgs A) {
+__global__ void __launch_bounds__(OPAC_GT * 32, 5) opacity_fwd_kernel(const OpacArgs A) {
   __shared__ float tcap[OPAC_CT][OPAC_GT + 1];
   __shared__ float tem[OPAC_CT][OPAC_GT + 1];
   __shared__ double tcapd[OPAC_CT][OPAC_GT + 1];
@@ -474,7 +583,8 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_fwd_kernel(const OpacArg
   if (A.stage_rows) {
     for (int k = threadIdx.x; k < A.nlrow * 32; k += blockDim.x) {
       const int ii = blockIdx.x * OPAC_CT + (k & 31);
-      s_rows[k] = ii < A.nc ? A.grndlev[(size_t)A.slot_of_lrow[k >> 5] * A.nc + ii] : 0.0;
+      const double v = ii < A.nc ? A.grndlev[(size_t)A.slot_of_lrow[k >> 5] * A.nc + ii] : 0.0;
+      s_rows[k] = v < 0.0 ? 0.0 : v;  // the reference skips lines with ocg <= 0
     }
   }
   __syncthreads();
@@ -702,9 +812,55 @@ struct OpacBwd {
   double* gfr;         // (0:nelem, ncell), added to
 };
 
+// The bound-bound part of the adjoint for one (shell, group): adds
+// ue * d cap / d grndlev / expfac = ue * pg * exp(-chi h) of every line to its
+// row's shared accumulator (s_acc_l[row * 32]; ue = u * expfac), and returns
+// the sums over lines of pg exp(-chi h) og (capbb / expfac) and of the same
+// times chi (the T-derivative's weight).  Staged populations are clamped at
+// zero, so an unpopulated ion's term is +0 as the forward's skip.  Four lines
+// per round: independent loads and exps.
+template <bool INRANGE>
+__device__ __forceinline__ void bb_adjoint_staged(const LineTerm* lt, int n, double h, double ue,
+                                                  const double* s_gl, double* s_acc_l, const double* etab,
+                                                  double& sbb, double& schi) {
+  int k = 0;
+  for (; k + 4 <= n; k += 4) {
+    LineVals t[4];
+    int r[4];
+    double e[4], o[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) t[q] = load_line(lt + k + q);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      r[q] = line_row(t[q].idx) << 5;
+      o[q] = s_gl[r[q]];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      e[q] = t[q].pg * (INRANGE ? exp_tang_inrange(-(t[q].chi * h), etab) : exp_tang(-(t[q].chi * h), etab));
+#pragma unroll
+    for (int q = 0; q < 4; ++q) atomicAdd(s_acc_l + r[q], ue * e[q]);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double x = e[q] * o[q];
+      sbb = sbb + x;
+      schi = schi + x * t[q].chi;
+    }
+  }
+  for (; k < n; ++k) {
+    const LineVals t = load_line(lt + k);
+    const int r = line_row(t.idx) << 5;
+    const double e = t.pg * (INRANGE ? exp_tang_inrange(-(t.chi * h), etab) : exp_tang(-(t.chi * h), etab));
+    atomicAdd(s_acc_l + r, ue * e);
+    const double x = e * s_gl[r];
+    sbb = sbb + x;
+    schi = schi + x * t.chi;
+  }
+}
+
 // Adjoint of subgroup_opacity (ngs = 1): bb, bf and ff in one pass over the
 // lines of each group, with per-(ion, shell) sums gathered in shared memory.
-__global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArgs A, const OpacBwd B) {
+__global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const OpacArgs A, const OpacBwd B) {
   extern __shared__ double sm[];
   const int nrow = A.nlrow;                          // population rows the lines reference
   double* s_grnd = sm;                               // [line row][32]
@@ -718,7 +874,8 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArg
   for (int k = threadIdx.x; k < ntot; k += blockDim.x) sm[k] = 0.0;
   for (int k = threadIdx.x; k < nrow * 32; k += blockDim.x) {
     const int ii = blockIdx.x * OPAC_CT + (k & 31);
-    s_g[k] = ii < A.nc ? A.grndlev[(size_t)A.slot_of_lrow[k >> 5] * A.nc + ii] : 0.0;
+    const double v = ii < A.nc ? A.grndlev[(size_t)A.slot_of_lrow[k >> 5] * A.nc + ii] : 0.0;
+    s_g[k] = v < 0.0 ? 0.0 : v;  // the forward skips lines with ocg <= 0: a zero term
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -737,39 +894,15 @@ __global__ void __launch_bounds__(OPAC_GT * 32) opacity_bwd_kernel(const OpacArg
         const double wlinv = 1.0 / wl;
         const double eh = exp(-(h * wlinv));
         const double expfac = 1.0 - eh;
-        double capbb = 0.0, schi = 0.0;
-        int l = l0;
-        for (; l + 2 <= l1; l += 2) {  // two lines per round: independent loads and exps
-          const double2 pa = __ldg(A.lpc + l), pb = __ldg(A.lpc + l + 1);
-          const int ra = __ldg(A.lslot + l) >> 16, rb = __ldg(A.lslot + l + 1) >> 16;
-          const double ba = pa.x * exp_tang(-(pa.y * h), etab) * expfac;  // d cap / d grndlev
-          const double bb = pb.x * exp_tang(-(pb.y * h), etab) * expfac;
-          const double oa = s_g[ra * 32 + lane], ob = s_g[rb * 32 + lane];
-          atomicAdd(&s_grnd[ra * 32 + lane], u * ba);
-          atomicAdd(&s_grnd[rb * 32 + lane], u * bb);
-          if (oa > 0.0) {
-            const double c = ba * oa;
-            capbb = capbb + c;
-            schi = schi + c * pa.y;
-          }
-          if (ob > 0.0) {
-            const double c = bb * ob;
-            capbb = capbb + c;
-            schi = schi + c * pb.y;
-          }
-        }
-        for (; l < l1; ++l) {
-          const double2 pc = __ldg(A.lpc + l);
-          const int row = __ldg(A.lslot + l) >> 16;
-          const double base = pc.x * exp_tang(-(pc.y * h), etab) * expfac;  // d cap / d grndlev
-          atomicAdd(&s_grnd[row * 32 + lane], u * base);
-          const double ocg = s_g[row * 32 + lane];
-          if (ocg > 0.0) {
-            const double c = base * ocg;
-            capbb = capbb + c;
-            schi = schi + c * pc.y;
-          }
-        }
+        double sbb = 0.0, schi = 0.0;
+        const double ue = u * expfac;
+        const bool inrange = h >= 0.0 && h * A.chimax <= 700.0;  // as in the forward
+        if (inrange)
+          bb_adjoint_staged<true>(A.lt + l0, l1 - l0, h, ue, s_g + lane, s_grnd + lane, etab, sbb, schi);
+        else
+          bb_adjoint_staged<false>(A.lt + l0, l1 - l0, h, ue, s_g + lane, s_grnd + lane, etab, sbb, schi);
+        const double capbb = sbb * expfac;
+        schi = schi * expfac;
         // h = hc/kT: d exp(-chi h)/dT = chi h/T exp(..), d expfac/dT = -(h/T) wlinv eh
         gt = gt + u * ((h / T) * schi - capbb * (h / T) * wlinv * eh / expfac);
       }
@@ -876,7 +1009,7 @@ __global__ void __launch_bounds__(BFB_T * 8) bf_bwd_kernel(const OpacArgs A, con
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const int a = a0 + ty + 8 * j;
-    if (a < nact && acc[j] != 0.0) B.goc[(size_t)A.act_slot[a] * A.nc + i] += acc[j] * pc_mbarn;
+    if (a < nact && acc[j] != 0.0) B.goc[(size_t)A.act_slot[a] * A.nc + i] += acc[j];  // xstab holds * pc_mbarn
   }
 }
 
@@ -964,8 +1097,7 @@ static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_f
   cudaMemsetAsync(d_active, 0, sizeof(int) * (nslot + 1), st);
   wlsub_kernel<<<(nedge_pad + 255) / 256, 256, 0, st>>>(ng, ngs, nedge_pad, ctx->d_wl, d_wlsub);
   const bool do_bb = ctx->nline > 0 && !flags->nobb;
-  double2* d_lpc = nullptr;
-  int* d_lslot = nullptr;
+  LineTerm* d_lt = nullptr;
   if (do_bb) {
     const size_t shm = 16 + sizeof(double) * nedge_pad + sizeof(unsigned int) * (nedge + 1);
     if (shm > 220 * 1024)
@@ -980,18 +1112,29 @@ static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_f
     bin_lines_kernel<<<nb, 256, shm, st>>>(ctx->d_bb, ctx->nline, d_wlsub, nedge, nedge_pad, d_counts,
                                            d_flags);
     scan_counts_kernel<<<1, 1024, 0, st>>>(d_counts, nedge + 1, d_lstart);
-    d_lpc = (double2*)scratch(ctx, 84, sizeof(double2) * (size_t)ctx->nline);
-    d_lslot = (int*)scratch(ctx, 85, sizeof(int) * (size_t)ctx->nline);
-    if (!d_lpc || !d_lslot) return SLG_ERR_OOM;
+    d_lt = (LineTerm*)scratch(ctx, 84, sizeof(LineTerm) * (size_t)ctx->nline);
+    if (!d_lt) return SLG_ERR_OOM;
     decode_lines_kernel<<<(unsigned)((ctx->nline + 255) / 256), 256, 0, st>>>(
-        ctx->d_bb, ctx->nline, d_lstart, ngsub, d_wlsub, nst, ctx->d_lrow_of_slot, d_lpc, d_lslot);
+        ctx->d_bb, ctx->nline, d_lstart, ngsub, d_wlsub, nst, ctx->d_lrow_of_slot, d_lt);
   } else {
     cudaMemsetAsync(d_lstart, 0, sizeof(int) * (nedge + 3), st);
   }
   opac_cell_prep_kernel<<<dim3((nc + 127) / 128, nelem), 128, 0, st>>>(
       nc, nelem, nst, ctx->d_ion_ni, gas->temp, gas->natom, gas->nelec, gas->vol, gas->mass, gas->oc,
       gas->ginv, flags->nothmson, d_hckt, gas_sig, d_hlp, d_grnd, d_ffigg, d_ffdgg);
+  double* d_ffsum = nullptr;
+  unsigned* d_ffclamp = nullptr;
+  if (!flags->noff && ctx->d_gff) {
+    d_ffsum = (double*)scratch(ctx, 88, sizeof(double) * (size_t)nc * FF_NU);
+    d_ffclamp = (unsigned*)scratch(ctx, 89, sizeof(unsigned) * (size_t)nc);
+    if (!d_ffsum || !d_ffclamp) return SLG_ERR_OOM;
+    const int64_t nt = (int64_t)nc * FF_NU;
+    ff_sum_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(nc, nelem, gas->natomfr, d_ffigg, d_ffdgg,
+                                                                ctx->d_gff, d_ffsum, d_ffclamp);
+  }
   const bool do_bf = !flags->nobf;
+  double* d_xsc = nullptr;
+  int *d_bslot = nullptr, *d_bnnz = nullptr;
   if (do_bf) {
     dim3 ga((nc + 255) / 256 < 8 ? (nc + 255) / 256 : 8, nslot);
     ion_active_kernel<<<ga, 256, 0, st>>>(nc, gas->oc, d_active);
@@ -999,16 +1142,23 @@ static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_f
     const int64_t nt = (int64_t)ngsub * nslot;
     bf_table_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(ngsub, nslot, d_nact, d_act, nst, d_wlsub,
                                                                   ctx->d_ph1, ctx->d_ph2, d_xs);
+    d_xsc = (double*)scratch(ctx, 85, sizeof(double) * (size_t)ngsub * nslot);
+    d_bslot = (int*)scratch(ctx, 86, sizeof(int) * (size_t)ngsub * nslot);
+    d_bnnz = (int*)scratch(ctx, 87, sizeof(int) * (size_t)ngsub);
+    if (!d_xsc || !d_bslot || !d_bnnz) return SLG_ERR_OOM;
+    bf_compact_kernel<<<(ngsub + 7) / 8, 256, 0, st>>>(ngsub, nslot, d_nact, d_act, d_xs, d_xsc, d_bslot, d_bnnz);
   }
   A.nc = nc; A.ng = ng; A.ngs = ngs; A.ngsub = ngsub; A.nelem = nelem; A.nst = nst; A.maxact = nslot;
   A.pnact = d_nact;
   A.nobb = !do_bb; A.nobf = !do_bf; A.noff = flags->noff;
   A.mix = flags->opacmixrossel;
   A.wlsub = d_wlsub; A.grp_wl = ctx->d_wl; A.lstart = d_lstart; A.bb = ctx->d_bb;
-  A.lpc = d_lpc; A.lslot = d_lslot; A.slot_of_lrow = ctx->d_slot_of_lrow; A.nlrow = ctx->nlrow;
+  A.lt = d_lt; A.chimax = ctx->line_chimax; A.slot_of_lrow = ctx->d_slot_of_lrow; A.nlrow = ctx->nlrow;
   A.grndlev = d_grnd; A.oc = gas->oc; A.act_slot = d_act; A.xstab = d_xs;
+  A.xsc = d_xsc; A.bslot = d_bslot; A.bnnz = d_bnnz;
   A.hckt = d_hckt; A.hlparr = d_hlp; A.mass = gas->mass; A.natomfr = gas->natomfr; A.temp = gas->temp;
   A.ffigg = d_ffigg; A.ffdgg = d_ffdgg; A.gff = ctx->d_gff;
+  A.ffsum = d_ffsum; A.ffclamp = d_ffclamp;
   A.ffc1 = ff_c1a * sqrt(ff_c1b);
   A.cap32 = nullptr; A.emiss32 = nullptr; A.cap64 = nullptr; A.capg64 = nullptr; A.flags = d_flags;
   if (!ctx->d_gff && !A.noff) return set_error(ctx, SLG_ERR_STATE, "free-free table not set");

@@ -8,9 +8,13 @@
 // work to keep the pipe full) for `iters` rounds on a grid of 8 blocks of 256
 // threads per SM, and writes one value so that the work cannot be removed.
 // The host entry point times one launch with CUDA events on a private stream.
+//
+// slg_exp_eval evaluates the opacity kernels' table-driven FP64 exp
+// (exp_tang, slg_device.cuh) on given arguments, for accuracy tests.
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "slg.h"
+#include "slg_device.cuh"
 
 namespace {
 
@@ -75,7 +79,34 @@ __global__ void __launch_bounds__(PK_BLOCK) imad_kernel(int iters, uint32_t a, u
   out[(size_t)blockIdx.x * blockDim.x + threadIdx.x] = (double)s;
 }
 
+__global__ void exp_eval_kernel(int64_t n, const double* __restrict__ x, double* __restrict__ y) {
+  __shared__ double tab[64];
+  slg::exp_table_load(tab);
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = slg::exp_tang(x[i], tab);
+}
+
 }  // namespace
+
+extern "C" int slg_exp_eval(int device, int64_t n, const double* x, double* y) {
+  if (n < 0 || (n > 0 && (!x || !y))) return SLG_ERR_ARG;
+  if (n == 0) return SLG_OK;
+  if (cudaSetDevice(device) != cudaSuccess) return SLG_ERR_CUDA;
+  double* d = nullptr;
+  if (cudaMalloc(&d, sizeof(double) * 2 * (size_t)n) != cudaSuccess) return SLG_ERR_OOM;
+  int rc = SLG_OK;
+  if (cudaMemcpy(d, x, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess) rc = SLG_ERR_CUDA;
+  if (!rc) {
+    const int64_t nb = (n + 255) / 256;
+    exp_eval_kernel<<<(unsigned)(nb < 4096 ? nb : 4096), 256>>>(n, d, d + n);
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpy(y, d + n, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = SLG_ERR_CUDA;
+  }
+  cudaFree(d);
+  return rc;
+}
 
 extern "C" int slg_pipe_throughput(int device, int which, int iters, double* ops_per_s, float* ms) {
   if (!ops_per_s || iters < 1 || which < 0 || which > 3) return SLG_ERR_ARG;

@@ -81,9 +81,10 @@ __device__ inline void exp_table_load(double* s_tab) {
 
 // tab: kExp2Tab64 in shared memory.  n = nearest integer of x 64/ln2 by the
 // add-and-subtract of 1.5 2^52 (|x 64/ln2| < 2^31, so the sum's low 32 bits
-// are n in two's complement and the difference is n exactly).
-__device__ inline double exp_tang(double x, const double* tab) {
-  if (!(fabs(x) <= 700.0)) return exp(x);  // also NaN
+// are n in two's complement and the difference is n exactly).  This form
+// requires x in [-700, 700] and does not check it: the result's exponent
+// field is formed by an integer add, valid for normal results only.
+__device__ __forceinline__ double exp_tang_inrange(double x, const double* tab) {
   constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
   const double big = fma(x, kExpInvL, kRound);
   const int ni = (int)__double2loint(big);
@@ -96,8 +97,13 @@ __device__ inline double exp_tang(double x, const double* tab) {
   p = fma(r, p, 1.0);
   p = p * r;  // e^r - 1
   const double s = tab[ni & 63];
-  const double v = fma(s, p, s);
-  return __longlong_as_double(__double_as_longlong(v) + ((long long)(ni >> 6) << 52));
+  const double v = fma(s, p, s);  // in [0.99, 2): adding n/64's integer part to the exponent field stays normal
+  return __hiloint2double(__double2hiint(v) + (ni >> 6) * (1 << 20), __double2loint(v));
+}
+// Any x: outside [-700, 700], and for NaN, CUDA's exp.
+__device__ inline double exp_tang(double x, const double* tab) {
+  if (!(fabs(x) <= 700.0)) return exp(x);  // also NaN
+  return exp_tang_inrange(x, tab);
 }
 constexpr double ff_c1a = 4.0 * e6c / (3.0 * pc_h * pc_me * c4c);              // physical_opacity.f:32
 constexpr double ff_c1b = pc_pi2 / (3.0 * pc_me * pc_h * pc_c);                 // argument of its sqrt

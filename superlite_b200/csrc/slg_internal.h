@@ -113,6 +113,7 @@ struct slg_ctx {
   // population rows (slot = (iz-1) nstage + ii-1) that the lines reference:
   // d_lrow_of_slot[slot] = compact row or -1, d_slot_of_lrow[row] = slot
   int nlrow = 0;
+  double line_chimax = 0.0;  // largest chilw of the lines (infinite if any is negative or NaN)
   int16_t* d_lrow_of_slot = nullptr;
   int16_t* d_slot_of_lrow = nullptr;
   float* d_ph1 = nullptr;
