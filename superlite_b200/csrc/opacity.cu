@@ -468,8 +468,10 @@ struct OpacArgs {
 
 // Sum over n lines of pg * og * exp(-chi h), og the staged population of the
 // line's row for this lane's shell; four lines per round: their loads and exps
-// are independent, and the terms are added one after another in line order.
-// INRANGE: the caller has shown -chi h in [-700, 0] for every line.
+// are independent, and the terms are added one after another in line order,
+// each by one fused multiply-add (one rounding where the reference rounds the
+// product and the sum).  INRANGE: the caller has shown -chi h in [-700, 0] for
+// every line.
 template <bool INRANGE>
 __device__ __forceinline__ double bb_sum_staged(const LineTerm* lt, int n, double h, const double* s_gl,
                                                 const double* etab) {
@@ -486,19 +488,19 @@ __device__ __forceinline__ double bb_sum_staged(const LineTerm* lt, int n, doubl
     for (int q = 0; q < 4; ++q)
       e[q] = INRANGE ? exp_tang_inrange(-(t[q].chi * h), etab) : exp_tang(-(t[q].chi * h), etab);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) sbb = sbb + t[q].pg * og[q] * e[q];
+    for (int q = 0; q < 4; ++q) sbb = fma(t[q].pg * og[q], e[q], sbb);
   }
   for (; k < n; ++k) {
     const LineVals t = load_line(lt + k);
     const double og = s_gl[line_row(t.idx) << 5];
     const double e = INRANGE ? exp_tang_inrange(-(t.chi * h), etab) : exp_tang(-(t.chi * h), etab);
-    sbb = sbb + t.pg * og * e;
+    sbb = fma(t.pg * og, e, sbb);
   }
   return sbb;
 }
 
 // One sub-group igs for shell i (lane `lane` of its block): bb, bf and ff in
-// the reference's order.  etab: the exp table (kExp2Tab64) in shared memory;
+// the reference's order.  etab: the exp table (kExp2Tab) in shared memory;
 // s_g: the block's population rows [line row][lane] in shared memory, or null
 // (read grndlev).
 __device__ inline double subgroup_opacity(const OpacArgs& A, int i, int lane, int igs, bool live, const double* etab,
@@ -533,7 +535,7 @@ __device__ inline double subgroup_opacity(const OpacArgs& A, int i, int lane, in
           const LineVals t = load_line(lt + k);
           const double ocg = A.grndlev[(size_t)line_slot(t.idx) * A.nc + i];
           if (ocg <= 0.0) continue;
-          sbb = sbb + t.pg * ocg * exp_tang(-(t.chi * h), etab);
+          sbb = fma(t.pg * ocg, exp_tang(-(t.chi * h), etab), sbb);
         }
       }
       cap = cap + sbb * expfac;
@@ -577,7 +579,7 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 5) opacity_fwd_kernel(const Opac
   __shared__ float tcap[OPAC_CT][OPAC_GT + 1];
   __shared__ float tem[OPAC_CT][OPAC_GT + 1];
   __shared__ double tcapd[OPAC_CT][OPAC_GT + 1];
-  __shared__ double etab[64];
+  __shared__ double etab[kExpTabN];
   extern __shared__ double s_rows[];  // [line row][lane] populations of this block's shells (A.stage_rows)
   exp_table_load(etab);
   if (A.stage_rows) {
@@ -813,16 +815,19 @@ struct OpacBwd {
 };
 
 // The bound-bound part of the adjoint for one (shell, group): adds
-// ue * d cap / d grndlev / expfac = ue * pg * exp(-chi h) of every line to its
-// row's shared accumulator (s_acc_l[row * 32]; ue = u * expfac), and returns
+// ue * d cap / d grndlev / expfac = ue * pg * exp(-chi h) of every line to
+// dL/d grndlev of its population slot in global memory (g_acc_l[slot * nc],
+// one reduction without return per term, coalesced over the warp's shells;
+// ue = u * expfac; shared-memory atomics here stalled the warps on their
+// returns), and returns
 // the sums over lines of pg exp(-chi h) og (capbb / expfac) and of the same
 // times chi (the T-derivative's weight).  Staged populations are clamped at
 // zero, so an unpopulated ion's term is +0 as the forward's skip.  Four lines
 // per round: independent loads and exps.
 template <bool INRANGE>
 __device__ __forceinline__ void bb_adjoint_staged(const LineTerm* lt, int n, double h, double ue,
-                                                  const double* s_gl, double* s_acc_l, const double* etab,
-                                                  double& sbb, double& schi) {
+                                                  const double* s_gl, double* g_acc_l, size_t nc,
+                                                  const double* etab, double& sbb, double& schi) {
   int k = 0;
   for (; k + 4 <= n; k += 4) {
     LineVals t[4];
@@ -839,37 +844,37 @@ __device__ __forceinline__ void bb_adjoint_staged(const LineTerm* lt, int n, dou
     for (int q = 0; q < 4; ++q)
       e[q] = t[q].pg * (INRANGE ? exp_tang_inrange(-(t[q].chi * h), etab) : exp_tang(-(t[q].chi * h), etab));
 #pragma unroll
-    for (int q = 0; q < 4; ++q) atomicAdd(s_acc_l + r[q], ue * e[q]);
+    for (int q = 0; q < 4; ++q) atomicAdd(g_acc_l + (size_t)line_slot(t[q].idx) * nc, ue * e[q]);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const double x = e[q] * o[q];
       sbb = sbb + x;
-      schi = schi + x * t[q].chi;
+      schi = fma(x, t[q].chi, schi);
     }
   }
   for (; k < n; ++k) {
     const LineVals t = load_line(lt + k);
     const int r = line_row(t.idx) << 5;
     const double e = t.pg * (INRANGE ? exp_tang_inrange(-(t.chi * h), etab) : exp_tang(-(t.chi * h), etab));
-    atomicAdd(s_acc_l + r, ue * e);
+    atomicAdd(g_acc_l + (size_t)line_slot(t.idx) * nc, ue * e);
     const double x = e * s_gl[r];
     sbb = sbb + x;
-    schi = schi + x * t.chi;
+    schi = fma(x, t.chi, schi);
   }
 }
 
-// Adjoint of subgroup_opacity (ngs = 1): bb, bf and ff in one pass over the
-// lines of each group, with per-(ion, shell) sums gathered in shared memory.
+// Adjoint of subgroup_opacity (ngs = 1): bb and ff in one pass over the lines
+// of each group (bf: bf_bwd_kernel); d/d(natomfr) sums gathered per (element,
+// shell) in shared memory, d/d(grndlev) reduced into global memory per term.
 __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const OpacArgs A, const OpacBwd B) {
   extern __shared__ double sm[];
   const int nrow = A.nlrow;                          // population rows the lines reference
-  double* s_grnd = sm;                               // [line row][32]
-  double* s_fr = sm + (size_t)nrow * 32;             // [nelem+1][32]
+  double* s_fr = sm;                                 // [nelem+1][32]
   double* s_t = s_fr + (size_t)(A.nelem + 1) * 32;   // [warp][32]
   double* s_h = s_t + OPAC_GT * 32;
   double* s_g = s_h + OPAC_GT * 32;                  // [line row][32] populations of this block's shells
-  const int ntot = (nrow + A.nelem + 1) * 32;
-  __shared__ double etab[64];
+  const int ntot = (A.nelem + 1) * 32;
+  __shared__ double etab[kExpTabN];
   exp_table_load(etab);
   for (int k = threadIdx.x; k < ntot; k += blockDim.x) sm[k] = 0.0;
   for (int k = threadIdx.x; k < nrow * 32; k += blockDim.x) {
@@ -898,9 +903,9 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const Opac
         const double ue = u * expfac;
         const bool inrange = h >= 0.0 && h * A.chimax <= 700.0;  // as in the forward
         if (inrange)
-          bb_adjoint_staged<true>(A.lt + l0, l1 - l0, h, ue, s_g + lane, s_grnd + lane, etab, sbb, schi);
+          bb_adjoint_staged<true>(A.lt + l0, l1 - l0, h, ue, s_g + lane, B.ggrnd + i, A.nc, etab, sbb, schi);
         else
-          bb_adjoint_staged<false>(A.lt + l0, l1 - l0, h, ue, s_g + lane, s_grnd + lane, etab, sbb, schi);
+          bb_adjoint_staged<false>(A.lt + l0, l1 - l0, h, ue, s_g + lane, B.ggrnd + i, A.nc, etab, sbb, schi);
         const double capbb = sbb * expfac;
         schi = schi * expfac;
         // h = hc/kT: d exp(-chi h)/dT = chi h/T exp(..), d expfac/dT = -(h/T) wlinv eh
@@ -962,11 +967,10 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const Opac
     if (b != 0.0) atomicAdd(&B.ghlp[i], b);
   }
   for (int k = threadIdx.x; k < ntot; k += blockDim.x) {
-    const double v = sm[k];
-    const int row = k >> 5, c = blockIdx.x * OPAC_CT + (k & 31);
+    const double v = s_fr[k];
+    const int iz = k >> 5, c = blockIdx.x * OPAC_CT + (k & 31);
     if (v == 0.0 || c >= A.nc) continue;
-    if (row < nrow) atomicAdd(&B.ggrnd[(size_t)A.slot_of_lrow[row] * A.nc + c], v);
-    else atomicAdd(&B.gfr[(size_t)c * (A.nelem + 1) + (row - nrow)], v);
+    atomicAdd(&B.gfr[(size_t)c * (A.nelem + 1) + iz], v);
   }
 }
 
@@ -1223,7 +1227,7 @@ int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, con
   cudaMemsetAsync(goc, 0, sizeof(double) * (size_t)nslot * nc, st);
   cudaMemsetAsync(gfr, 0, sizeof(double) * (size_t)nc * (A.nelem + 1), st);
   OpacBwd B{gcap, gT, ggrnd, goc, ghlp, gfr};
-  const size_t shm = sizeof(double) * ((size_t)(2 * A.nlrow + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
+  const size_t shm = sizeof(double) * ((size_t)(A.nlrow + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
   if (shm > 200 * 1024) return set_error(ctx, SLG_ERR_ARG, "opacity adjoint: too many ion slots (%d)", A.nlrow);
   static size_t shm_set = 0;  // raised only when needed
   if (shm > 48 * 1024 && shm > shm_set) {

@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(PK_BLOCK) imad_kernel(int iters, uint32_t a, u
 }
 
 __global__ void exp_eval_kernel(int64_t n, const double* __restrict__ x, double* __restrict__ y) {
-  __shared__ double tab[64];
+  __shared__ double tab[slg::kExpTabN];
   slg::exp_table_load(tab);
   __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)

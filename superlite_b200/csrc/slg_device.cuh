@@ -50,11 +50,15 @@ constexpr double cthomson = 8.0 * pc_pi * e4c / (3.0 * (pc_me * pc_me) * c4c);  
 // 2^17) and its remainder, e^r - 1 by its Taylor polynomial of degree 5
 // (truncation below 4e-17 relative), 2^(j/64) from a 64-entry table and 2^m
 // added to the exponent field.  Arguments outside [-700, 700] go to exp().
+// The constants and the table are the output of csrc/exp_table.py.  (A
+// 256-entry table with a degree-4 polynomial saves one FMA per exp but was
+// slower in the opacity kernels: its shared-memory lookups conflict more.)
+constexpr int kExpTabN = 64;
 constexpr double kExpInvL = 92.33248261689366;        // 64 / ln 2
 constexpr double kExpL1 = 0.010830424696223417;       // ln2/64, 36 significant bits
 constexpr double kExpL2 = 2.572804622327669e-14;      // ln2/64 - kExpL1
 // 2^(j/64), j = 0..63, correctly rounded
-static __constant__ double kExp2Tab64[64] = {
+static __constant__ double kExp2Tab[kExpTabN] = {
     1.0, 1.0108892860517005, 1.0218971486541166, 1.0330248790212284,
     1.0442737824274138, 1.0556451783605572, 1.0671404006768237, 1.0787607977571199,
     1.0905077326652577, 1.102382583307841, 1.1143867425958924, 1.1265216186082418,
@@ -73,13 +77,13 @@ static __constant__ double kExp2Tab64[64] = {
     1.9152065613971474, 1.9360617934922943, 1.9571441241754002, 1.978456026387951,
 };
 
-// Copies kExp2Tab64 into a block's shared array (call from every thread, then
-// __syncthreads()).
+// Copies kExp2Tab into a block's shared array of kExpTabN doubles (call from
+// every thread, then __syncthreads()).
 __device__ inline void exp_table_load(double* s_tab) {
-  for (int k = threadIdx.x; k < 64; k += blockDim.x) s_tab[k] = kExp2Tab64[k];
+  for (int k = threadIdx.x; k < kExpTabN; k += blockDim.x) s_tab[k] = kExp2Tab[k];
 }
 
-// tab: kExp2Tab64 in shared memory.  n = nearest integer of x 64/ln2 by the
+// tab: kExp2Tab in shared memory.  n = nearest integer of x 64/ln2 by the
 // add-and-subtract of 1.5 2^52 (|x 64/ln2| < 2^31, so the sum's low 32 bits
 // are n in two's complement and the difference is n exactly).  This form
 // requires x in [-700, 700] and does not check it: the result's exponent
@@ -96,8 +100,8 @@ __device__ __forceinline__ double exp_tang_inrange(double x, const double* tab) 
   p = fma(r, p, 0.5);
   p = fma(r, p, 1.0);
   p = p * r;  // e^r - 1
-  const double s = tab[ni & 63];
-  const double v = fma(s, p, s);  // in [0.99, 2): adding n/64's integer part to the exponent field stays normal
+  const double s = tab[ni & (kExpTabN - 1)];
+  const double v = fma(s, p, s);  // in [0.99, 2): adding m to the exponent field stays normal
   return __hiloint2double(__double2hiint(v) + (ni >> 6) * (1 << 20), __double2loint(v));
 }
 // Any x: outside [-700, 700], and for NaN, CUDA's exp.
