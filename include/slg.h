@@ -321,7 +321,9 @@ int slg_autotune_transport(slg_ctx* ctx, const slg_transport_in* in, const slg_p
                            int64_t nsample, int32_t* best, float* ms);
 /* Select the transport kernel variant (0..3, register budget / resident
  * blocks, as slg_autotune_transport times them) of both precisions explicitly,
- * e.g. after timing each on full launches of the caller's own workload. */
+ * e.g. after timing each on full launches of the caller's own workload.  A new
+ * context starts with FP64 variant 2 and mixed variant 3, the fastest on whole
+ * steps of a large batched workload. */
 int slg_set_transport_variant(slg_ctx* ctx, int32_t variant);
 /* radtemp, prt and isvacant on the device; emit and nvol are host arrays. */
 int slg_dev_interior_source(slg_ctx* ctx, const double* radtemp, const double* emit,

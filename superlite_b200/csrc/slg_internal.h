@@ -137,9 +137,11 @@ struct slg_ctx {
   // optional trace (host arrays) for the next particle_advance call
   uint64_t* trace_hash = nullptr;
   int32_t* trace_nstep = nullptr;
-  // launch configuration chosen by the autotuner (0 = defaults)
-  int trn_variant = 0;  // FP64 transport kernel variant (see launch_transport_variant)
-  int mix_variant = 0;  // mixed-precision variant (see launch_transport_mixed)
+  // transport kernel variants until slg_autotune_transport or
+  // slg_set_transport_variant choose: the ones measured fastest on whole
+  // steps of the batched 128-model workload at full particle budgets
+  int trn_variant = 2;  // FP64 transport kernel variant (see launch_transport_variant)
+  int mix_variant = 3;  // mixed-precision variant (see launch_transport_mixed)
   // transport_out of a queued slg_dev_particle_advance, completed by slg_sync
   slg_transport_out* pending_out = nullptr;
   // models (one for slg_set_grid): host descriptors, device copies, and the
