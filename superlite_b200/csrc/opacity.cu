@@ -815,18 +815,21 @@ struct OpacBwd {
 };
 
 // The bound-bound part of the adjoint for one (shell, group): adds
-// ue * d cap / d grndlev / expfac = ue * pg * exp(-chi h) of every line to
-// dL/d grndlev of its population slot in global memory (g_acc_l[slot * nc],
-// one reduction without return per term, coalesced over the warp's shells;
-// ue = u * expfac; shared-memory atomics here stalled the warps on their
-// returns), and returns
+// ue * d cap / d grndlev / expfac = ue * pg * exp(-chi h) of every line
+// (ue = u * expfac) to dL/d grndlev of its population row: GRED, in global
+// memory (acc_l = ggrnd + shell, entry slot * nc: one reduction without
+// return per term, coalesced over the warp's shells), else in the block's
+// shared accumulator (acc_l = s_grnd + lane, entry row * 32, atomics with
+// return).  Global reductions pay when the accumulated array is large (many
+// shells x rows: the updates spread over many addresses); on a small one they
+// queue on the same addresses, where the shared accumulator wins.  Returns
 // the sums over lines of pg exp(-chi h) og (capbb / expfac) and of the same
 // times chi (the T-derivative's weight).  Staged populations are clamped at
 // zero, so an unpopulated ion's term is +0 as the forward's skip.  Four lines
 // per round: independent loads and exps.
-template <bool INRANGE>
+template <bool INRANGE, bool GRED>
 __device__ __forceinline__ void bb_adjoint_staged(const LineTerm* lt, int n, double h, double ue,
-                                                  const double* s_gl, double* g_acc_l, size_t nc,
+                                                  const double* s_gl, double* acc_l, size_t nc,
                                                   const double* etab, double& sbb, double& schi) {
   int k = 0;
   for (; k + 4 <= n; k += 4) {
@@ -844,7 +847,8 @@ __device__ __forceinline__ void bb_adjoint_staged(const LineTerm* lt, int n, dou
     for (int q = 0; q < 4; ++q)
       e[q] = t[q].pg * (INRANGE ? exp_tang_inrange(-(t[q].chi * h), etab) : exp_tang(-(t[q].chi * h), etab));
 #pragma unroll
-    for (int q = 0; q < 4; ++q) atomicAdd(g_acc_l + (size_t)line_slot(t[q].idx) * nc, ue * e[q]);
+    for (int q = 0; q < 4; ++q)
+      atomicAdd(acc_l + (GRED ? (size_t)line_slot(t[q].idx) * nc : (size_t)r[q]), ue * e[q]);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const double x = e[q] * o[q];
@@ -856,7 +860,7 @@ __device__ __forceinline__ void bb_adjoint_staged(const LineTerm* lt, int n, dou
     const LineVals t = load_line(lt + k);
     const int r = line_row(t.idx) << 5;
     const double e = t.pg * (INRANGE ? exp_tang_inrange(-(t.chi * h), etab) : exp_tang(-(t.chi * h), etab));
-    atomicAdd(g_acc_l + (size_t)line_slot(t.idx) * nc, ue * e);
+    atomicAdd(acc_l + (GRED ? (size_t)line_slot(t.idx) * nc : (size_t)r), ue * e);
     const double x = e * s_gl[r];
     sbb = sbb + x;
     schi = fma(x, t.chi, schi);
@@ -865,15 +869,18 @@ __device__ __forceinline__ void bb_adjoint_staged(const LineTerm* lt, int n, dou
 
 // Adjoint of subgroup_opacity (ngs = 1): bb and ff in one pass over the lines
 // of each group (bf: bf_bwd_kernel); d/d(natomfr) sums gathered per (element,
-// shell) in shared memory, d/d(grndlev) reduced into global memory per term.
+// shell) in shared memory, d/d(grndlev) as bb_adjoint_staged's GRED says.
+template <bool GRED>
 __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const OpacArgs A, const OpacBwd B) {
   extern __shared__ double sm[];
   const int nrow = A.nlrow;                          // population rows the lines reference
-  double* s_fr = sm;                                 // [nelem+1][32]
+  const int nacc = GRED ? 0 : nrow;                  // shared accumulator rows
+  double* s_grnd = sm;                               // [line row][32] (not GRED)
+  double* s_fr = sm + (size_t)nacc * 32;             // [nelem+1][32]
   double* s_t = s_fr + (size_t)(A.nelem + 1) * 32;   // [warp][32]
   double* s_h = s_t + OPAC_GT * 32;
   double* s_g = s_h + OPAC_GT * 32;                  // [line row][32] populations of this block's shells
-  const int ntot = (A.nelem + 1) * 32;
+  const int ntot = (nacc + A.nelem + 1) * 32;
   __shared__ double etab[kExpTabN];
   exp_table_load(etab);
   for (int k = threadIdx.x; k < ntot; k += blockDim.x) sm[k] = 0.0;
@@ -902,10 +909,11 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const Opac
         double sbb = 0.0, schi = 0.0;
         const double ue = u * expfac;
         const bool inrange = h >= 0.0 && h * A.chimax <= 700.0;  // as in the forward
+        double* acc_l = GRED ? B.ggrnd + i : s_grnd + lane;
         if (inrange)
-          bb_adjoint_staged<true>(A.lt + l0, l1 - l0, h, ue, s_g + lane, B.ggrnd + i, A.nc, etab, sbb, schi);
+          bb_adjoint_staged<true, GRED>(A.lt + l0, l1 - l0, h, ue, s_g + lane, acc_l, A.nc, etab, sbb, schi);
         else
-          bb_adjoint_staged<false>(A.lt + l0, l1 - l0, h, ue, s_g + lane, B.ggrnd + i, A.nc, etab, sbb, schi);
+          bb_adjoint_staged<false, GRED>(A.lt + l0, l1 - l0, h, ue, s_g + lane, acc_l, A.nc, etab, sbb, schi);
         const double capbb = sbb * expfac;
         schi = schi * expfac;
         // h = hc/kT: d exp(-chi h)/dT = chi h/T exp(..), d expfac/dT = -(h/T) wlinv eh
@@ -967,10 +975,11 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const Opac
     if (b != 0.0) atomicAdd(&B.ghlp[i], b);
   }
   for (int k = threadIdx.x; k < ntot; k += blockDim.x) {
-    const double v = s_fr[k];
-    const int iz = k >> 5, c = blockIdx.x * OPAC_CT + (k & 31);
+    const double v = sm[k];
+    const int row = k >> 5, c = blockIdx.x * OPAC_CT + (k & 31);
     if (v == 0.0 || c >= A.nc) continue;
-    atomicAdd(&B.gfr[(size_t)c * (A.nelem + 1) + iz], v);
+    if (row < nacc) atomicAdd(&B.ggrnd[(size_t)A.slot_of_lrow[row] * A.nc + c], v);
+    else atomicAdd(&B.gfr[(size_t)c * (A.nelem + 1) + (row - nacc)], v);
   }
 }
 
@@ -983,6 +992,10 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const Opac
 // holds shell tx and slots ty, ty + 8, ty + 16, ty + 24.  Runs after
 // opacity_bwd_kernel and before opac_cell_bwd_kernel (one writer per entry).
 constexpr int BFB_T = 32;
+// population rows x shells from which the adjoint accumulates d/d(population)
+// in global memory: measured on B200, shared accumulators won at 40 rows x 256
+// shells and global reductions at 40 rows x 4096 shells
+constexpr size_t kBwdGlobalAccMin = 32768;
 __global__ void __launch_bounds__(BFB_T * 8) bf_bwd_kernel(const OpacArgs A, const OpacBwd B) {
   __shared__ double su[BFB_T][BFB_T + 1];  // [shell][group]
   __shared__ double sx[BFB_T][BFB_T + 1];  // [group][slot]
@@ -1227,15 +1240,23 @@ int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, con
   cudaMemsetAsync(goc, 0, sizeof(double) * (size_t)nslot * nc, st);
   cudaMemsetAsync(gfr, 0, sizeof(double) * (size_t)nc * (A.nelem + 1), st);
   OpacBwd B{gcap, gT, ggrnd, goc, ghlp, gfr};
-  const size_t shm = sizeof(double) * ((size_t)(A.nlrow + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
+  // d/d(population) accumulated in global memory when that array (rows x
+  // shells) is large, in shared memory otherwise (bb_adjoint_staged)
+  const bool gred = (size_t)A.nlrow * nc >= kBwdGlobalAccMin;
+  const size_t shm =
+      sizeof(double) * ((size_t)((gred ? 1 : 2) * A.nlrow + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
   if (shm > 200 * 1024) return set_error(ctx, SLG_ERR_ARG, "opacity adjoint: too many ion slots (%d)", A.nlrow);
-  static size_t shm_set = 0;  // raised only when needed
-  if (shm > 48 * 1024 && shm > shm_set) {
-    cudaFuncSetAttribute(opacity_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    shm_set = 200 * 1024;
+  static size_t shm_set[2] = {0, 0};  // raised only when needed
+  if (shm > 48 * 1024 && shm > shm_set[gred]) {
+    cudaFuncSetAttribute(gred ? opacity_bwd_kernel<true> : opacity_bwd_kernel<false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    shm_set[gred] = 200 * 1024;
   }
   dim3 grid((nc + OPAC_CT - 1) / OPAC_CT, (A.ng + OPAC_GT - 1) / OPAC_GT);
-  opacity_bwd_kernel<<<grid, OPAC_GT * 32, shm, st>>>(A, B);
+  if (gred)
+    opacity_bwd_kernel<true><<<grid, OPAC_GT * 32, shm, st>>>(A, B);
+  else
+    opacity_bwd_kernel<false><<<grid, OPAC_GT * 32, shm, st>>>(A, B);
   if (!A.nobf) {
     const dim3 bgrid((nc + BFB_T - 1) / BFB_T, (A.maxact + BFB_T - 1) / BFB_T);
     bf_bwd_kernel<<<bgrid, BFB_T * 8, 0, st>>>(A, B);

@@ -62,11 +62,7 @@ def _L(D, ws, T, R, X):
     return sum((w * o).sum() for w, o in zip(ws, outs))
 
 
-@pytest.mark.parametrize("tables", ["synthetic", "reference"])
-@pytest.mark.parametrize("which", ["temp", "rho", "massfr"])
-def test_adjoint_matches_central_differences(which, tables):
-    import cases
-    hot, D, case, T, R, X = _setup(atomic=cases.atomic_data() if tables == "reference" else None)
+def _check_central_differences(hot, D, T, R, X, which, ntrial=3):
     with torch.no_grad():
         outs = D.opacity(T, R, X)
     ws = _loss_weights(outs, seed=7)
@@ -77,7 +73,7 @@ def test_adjoint_matches_central_differences(which, tables):
     gen = torch.Generator(device=T.device).manual_seed(11)
     base = {"temp": T, "rho": R, "massfr": X}[which]
     h = 1e-6
-    for trial in range(3):
+    for trial in range(ntrial):
         v = torch.randn(base.shape, generator=gen, device=T.device, dtype=torch.float64) * base
         if which == "massfr":
             v = v * (X > 0)
@@ -91,6 +87,26 @@ def test_adjoint_matches_central_differences(which, tables):
 
         fd = (at(1.0) - at(-1.0)) / (2.0 * h)
         assert ad == pytest.approx(fd, rel=RTOL), (which, trial, ad, fd)
+
+
+@pytest.mark.parametrize("tables", ["synthetic", "reference"])
+@pytest.mark.parametrize("which", ["temp", "rho", "massfr"])
+def test_adjoint_matches_central_differences(which, tables):
+    import cases
+    hot, D, case, T, R, X = _setup(atomic=cases.atomic_data() if tables == "reference" else None)
+    _check_central_differences(hot, D, T, R, X, which)
+    hot.close()
+
+
+@pytest.mark.parametrize("which", ["temp", "massfr"])
+def test_adjoint_large_grid_matches_central_differences(which):
+    """A grid large enough (population rows referenced by lines x shells >=
+    32768, kBwdGlobalAccMin in csrc/opacity.cu) that the adjoint accumulates
+    d/d(population) by global reductions instead of shared-memory atomics."""
+    hot, D, case, T, R, X = _setup(nc=1024, ng=60, nline=20000, seed=9)
+    rows = len(set(zip(case.lines["iz"].tolist(), case.lines["ii"].tolist())))
+    assert rows * 1024 >= 32768, rows
+    _check_central_differences(hot, D, T, R, X, which, ntrial=2)
     hot.close()
 
 
