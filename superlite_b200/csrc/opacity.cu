@@ -32,6 +32,8 @@ namespace {
 
 constexpr int OPAC_GT = 8;   // groups per block (one warp each)
 constexpr int OPAC_CT = 32;  // shells per block (one per lane)
+constexpr int OPAC_FS = 2;   // forward: shells per lane (a block covers OPAC_FS * OPAC_CT shells)
+constexpr int OPAC_FC = OPAC_FS * OPAC_CT;
 
 // ------------------------------------------------------------ TMA bulk helpers
 __device__ inline uint32_t smem_u32(const void* p) {
@@ -467,9 +469,10 @@ struct OpacArgs {
 };
 
 // Sum over n lines of pg * og * exp(-chi h), og the staged population of the
-// line's row for this lane's shell; four lines per round: their loads and exps
-// are independent, and the terms are added one after another in line order,
-// each by one fused multiply-add (one rounding where the reference rounds the
+// line's row for this shell (s_gl: the shell's column of the block's staged
+// rows, OPAC_FC apart); four lines per round: their loads and exps are
+// independent, and the terms are added one after another in line order, each
+// by one fused multiply-add (one rounding where the reference rounds the
 // product and the sum).  INRANGE: the caller has shown -chi h in [-700, 0] for
 // every line.
 template <bool INRANGE>
@@ -483,7 +486,7 @@ __device__ __forceinline__ double bb_sum_staged(const LineTerm* lt, int n, doubl
 #pragma unroll
     for (int q = 0; q < 4; ++q) t[q] = load_line(lt + k + q);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) og[q] = s_gl[line_row(t[q].idx) << 5];
+    for (int q = 0; q < 4; ++q) og[q] = s_gl[line_row(t[q].idx) * OPAC_FC];
 #pragma unroll
     for (int q = 0; q < 4; ++q)
       e[q] = INRANGE ? exp_tang_inrange(-(t[q].chi * h), etab) : exp_tang(-(t[q].chi * h), etab);
@@ -492,55 +495,57 @@ __device__ __forceinline__ double bb_sum_staged(const LineTerm* lt, int n, doubl
   }
   for (; k < n; ++k) {
     const LineVals t = load_line(lt + k);
-    const double og = s_gl[line_row(t.idx) << 5];
+    const double og = s_gl[line_row(t.idx) * OPAC_FC];
     const double e = INRANGE ? exp_tang_inrange(-(t.chi * h), etab) : exp_tang(-(t.chi * h), etab);
     sbb = fma(t.pg * og, e, sbb);
   }
   return sbb;
 }
 
-// One sub-group igs for shell i (lane `lane` of its block): bb, bf and ff in
-// the reference's order.  etab: the exp table (kExp2Tab) in shared memory;
-// s_g: the block's population rows [line row][lane] in shared memory, or null
-// (read grndlev).
-__device__ inline double subgroup_opacity(const OpacArgs& A, int i, int lane, int igs, bool live, const double* etab,
-                                          const double* s_g) {
-  double cap = 0.0;
-  if (!live) return cap;
-  const double h = A.hckt[i];
-  if (!A.nobb) {
-    const int l0 = A.lstart[igs], l1 = A.lstart[igs + 1];
-    if (l1 > l0) {
-      const double wa = A.wlsub[igs - 1], wb = A.wlsub[igs];
-      const double wl = 0.5 * (wa + wb);
-      const double wlinv = 1.0 / wl;
-      const double expfac = 1.0 - exp(-(h * wlinv));
-      // sum over the sub-group's lines of phi gxs ocg exp(-chilw h), times the
-      // stimulated-emission factor once (the reference multiplies each term by
-      // it; the sum of positive terms differs by rounding only)
-      const LineTerm* lt = A.lt + l0;
-      const int n = l1 - l0;
-      double sbb;
-      // h * chimax <= 700: every exp argument -chi h lies in [-700, 0], where
-      // exp_tang needs no range check
-      const bool inrange = h >= 0.0 && h * A.chimax <= 700.0;
-      if (s_g) {
-        // staged populations are clamped at zero, so a term of an unpopulated
-        // ion adds +0 (the reference skips it: the same sum)
-        const double* s_gl = s_g + lane;
-        sbb = inrange ? bb_sum_staged<true>(lt, n, h, s_gl, etab) : bb_sum_staged<false>(lt, n, h, s_gl, etab);
-      } else {
-        sbb = 0.0;
-        for (int k = 0; k < n; ++k) {
-          const LineVals t = load_line(lt + k);
-          const double ocg = A.grndlev[(size_t)line_slot(t.idx) * A.nc + i];
-          if (ocg <= 0.0) continue;
-          sbb = fma(t.pg * ocg, exp_tang(-(t.chi * h), etab), sbb);
-        }
-      }
-      cap = cap + sbb * expfac;
+// bb_sum_staged for the two shells of a lane at once (s_gl: the first shell's
+// column; the second's is OPAC_CT further): each line record's load and index
+// work serves both terms.  Four lines per round: eight independent exps.
+template <bool INRANGE>
+__device__ __forceinline__ void bb_sum_staged2(const LineTerm* lt, int n, double h0, double h1, const double* s_gl,
+                                               const double* etab, double& sbb0, double& sbb1) {
+  double a0 = 0.0, a1 = 0.0;
+  int k = 0;
+  for (; k + 4 <= n; k += 4) {
+    LineVals t[4];
+    double o0[4], o1[4], e0[4], e1[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) t[q] = load_line(lt + k + q);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double* r = s_gl + line_row(t[q].idx) * OPAC_FC;
+      o0[q] = r[0];
+      o1[q] = r[OPAC_CT];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      e0[q] = INRANGE ? exp_tang_inrange(-(t[q].chi * h0), etab) : exp_tang(-(t[q].chi * h0), etab);
+      e1[q] = INRANGE ? exp_tang_inrange(-(t[q].chi * h1), etab) : exp_tang(-(t[q].chi * h1), etab);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      a0 = fma(t[q].pg * o0[q], e0[q], a0);
+      a1 = fma(t[q].pg * o1[q], e1[q], a1);
     }
   }
+  for (; k < n; ++k) {
+    const LineVals t = load_line(lt + k);
+    const double* r = s_gl + line_row(t.idx) * OPAC_FC;
+    a0 = fma(t.pg * r[0], INRANGE ? exp_tang_inrange(-(t.chi * h0), etab) : exp_tang(-(t.chi * h0), etab), a0);
+    a1 = fma(t.pg * r[OPAC_CT], INRANGE ? exp_tang_inrange(-(t.chi * h1), etab) : exp_tang(-(t.chi * h1), etab),
+             a1);
+  }
+  sbb0 = a0;
+  sbb1 = a1;
+}
+
+// Bound-free and free-free of sub-group igs for shell i (h = hc/kT), added to
+// cap in the reference's order (after the bound-bound term).
+__device__ inline double bf_ff_add(const OpacArgs& A, int i, int igs, double h, double cap) {
   if (!A.nobf) {
     const size_t base = (size_t)(igs - 1) * A.maxact;
     const int n = A.bnnz[igs - 1];
@@ -575,69 +580,160 @@ __device__ inline double subgroup_opacity(const OpacArgs& A, int i, int lane, in
   return cap;
 }
 
-__global__ void __launch_bounds__(OPAC_GT * 32, 5) opacity_fwd_kernel(const OpacArgs A) {
-  __shared__ float tcap[OPAC_CT][OPAC_GT + 1];
-  __shared__ float tem[OPAC_CT][OPAC_GT + 1];
-  __shared__ double tcapd[OPAC_CT][OPAC_GT + 1];
+// 1 - exp(-h / wl(igs)), wl the sub-group's centre: the stimulated-emission
+// factor of the bound-bound term (physical_opacity.f:148-149).
+__device__ __forceinline__ double bb_expfac(const OpacArgs& A, int igs, double h) {
+  const double wa = A.wlsub[igs - 1], wb = A.wlsub[igs];
+  const double wl = 0.5 * (wa + wb);
+  const double wlinv = 1.0 / wl;
+  return 1.0 - exp(-(h * wlinv));
+}
+
+// One sub-group igs for shell i: bb, bf and ff in the reference's order.
+// etab: the exp table (kExp2Tab) in shared memory; s_gl: the shell's column of
+// the block's staged population rows ([line row][OPAC_FC] in shared memory), or
+// null (read grndlev).
+__device__ inline double subgroup_opacity(const OpacArgs& A, int i, const double* s_gl, int igs, bool live,
+                                          const double* etab) {
+  double cap = 0.0;
+  if (!live) return cap;
+  const double h = A.hckt[i];
+  if (!A.nobb) {
+    const int l0 = A.lstart[igs], l1 = A.lstart[igs + 1];
+    if (l1 > l0) {
+      const double expfac = bb_expfac(A, igs, h);
+      // sum over the sub-group's lines of phi gxs ocg exp(-chilw h), times the
+      // stimulated-emission factor once (the reference multiplies each term by
+      // it; the sum of positive terms differs by rounding only)
+      const LineTerm* lt = A.lt + l0;
+      const int n = l1 - l0;
+      double sbb;
+      // h * chimax <= 700: every exp argument -chi h lies in [-700, 0], where
+      // exp_tang needs no range check
+      const bool inrange = h >= 0.0 && h * A.chimax <= 700.0;
+      if (s_gl) {
+        // staged populations are clamped at zero, so a term of an unpopulated
+        // ion adds +0 (the reference skips it: the same sum)
+        sbb = inrange ? bb_sum_staged<true>(lt, n, h, s_gl, etab) : bb_sum_staged<false>(lt, n, h, s_gl, etab);
+      } else {
+        sbb = 0.0;
+        for (int k = 0; k < n; ++k) {
+          const LineVals t = load_line(lt + k);
+          const double ocg = A.grndlev[(size_t)line_slot(t.idx) * A.nc + i];
+          if (ocg <= 0.0) continue;
+          sbb = fma(t.pg * ocg, exp_tang(-(t.chi * h), etab), sbb);
+        }
+      }
+      cap = cap + sbb * expfac;
+    }
+  }
+  return bf_ff_add(A, i, igs, h, cap);
+}
+
+// Block: OPAC_FC shells x OPAC_GT groups; warp w takes group
+// blockIdx.y * OPAC_GT + w + 1, lane l shells base + l and base + OPAC_CT + l.
+__global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_fwd_kernel(const OpacArgs A) {
+  __shared__ float tcap[OPAC_FC][OPAC_GT + 1];
+  __shared__ float tem[OPAC_FC][OPAC_GT + 1];
+  __shared__ double tcapd[OPAC_FC][OPAC_GT + 1];
   __shared__ double etab[kExpTabN];
-  extern __shared__ double s_rows[];  // [line row][lane] populations of this block's shells (A.stage_rows)
+  extern __shared__ double s_rows[];  // [line row][OPAC_FC] populations of this block's shells (A.stage_rows)
   exp_table_load(etab);
+  const int base = blockIdx.x * OPAC_FC;
   if (A.stage_rows) {
-    for (int k = threadIdx.x; k < A.nlrow * 32; k += blockDim.x) {
-      const int ii = blockIdx.x * OPAC_CT + (k & 31);
-      const double v = ii < A.nc ? A.grndlev[(size_t)A.slot_of_lrow[k >> 5] * A.nc + ii] : 0.0;
+    for (int k = threadIdx.x; k < A.nlrow * OPAC_FC; k += blockDim.x) {
+      const int ii = base + (k % OPAC_FC);
+      const double v = ii < A.nc ? A.grndlev[(size_t)A.slot_of_lrow[k / OPAC_FC] * A.nc + ii] : 0.0;
       s_rows[k] = v < 0.0 ? 0.0 : v;  // the reference skips lines with ocg <= 0
     }
   }
   __syncthreads();
-  const double* s_g = A.stage_rows ? s_rows : nullptr;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ig = blockIdx.y * OPAC_GT + warp + 1;  // 1-based group
-  const int i = blockIdx.x * OPAC_CT + lane;       // 0-based shell
-  const bool valid = ig <= A.ng && i < A.nc;
-  const bool live = valid && A.mass[i] > 0.0;
-  double cap = 0.0;
-  if (valid) {
-    if (A.ngs == 1) {
-      cap = subgroup_opacity(A, i, lane, ig, live, etab, s_g);
-    } else {
-      // collapse subgridding, physical_opacity.f:252-264
-      double sp = 0.0, sr = 0.0;
-      for (int s = 1; s <= A.ngs; ++s) {
-        const double v = subgroup_opacity(A, i, lane, (ig - 1) * A.ngs + s, live, etab, s_g);
-        if (v > 0.0) { sp = sp + v; sr = sr + 1.0 / v; }
+  int ii[OPAC_FS];
+  bool valid[OPAC_FS], live[OPAC_FS];
+  double cap[OPAC_FS];
+#pragma unroll
+  for (int s = 0; s < OPAC_FS; ++s) {
+    ii[s] = base + s * OPAC_CT + lane;  // 0-based shell
+    valid[s] = ig <= A.ng && ii[s] < A.nc;
+    live[s] = valid[s] && A.mass[ii[s]] > 0.0;
+    cap[s] = 0.0;
+  }
+  if (A.ngs == 1 && A.stage_rows) {
+    // both shells' bound-bound sums in one pass over the group's lines
+    // (a shell that is not live runs the loop with h = 0 and is discarded)
+    double h[OPAC_FS];
+#pragma unroll
+    for (int s = 0; s < OPAC_FS; ++s) h[s] = live[s] ? A.hckt[ii[s]] : 0.0;
+    const int l0 = ig <= A.ng ? A.lstart[ig] : 0, l1 = ig <= A.ng ? A.lstart[ig + 1] : 0;
+    double sbb[OPAC_FS] = {0.0, 0.0};
+    if (!A.nobb && l1 > l0) {
+      const bool inrange = h[0] >= 0.0 && h[0] * A.chimax <= 700.0 && h[1] >= 0.0 && h[1] * A.chimax <= 700.0;
+      if (inrange)
+        bb_sum_staged2<true>(A.lt + l0, l1 - l0, h[0], h[1], s_rows + lane, etab, sbb[0], sbb[1]);
+      else
+        bb_sum_staged2<false>(A.lt + l0, l1 - l0, h[0], h[1], s_rows + lane, etab, sbb[0], sbb[1]);
+    }
+#pragma unroll
+    for (int s = 0; s < OPAC_FS; ++s) {
+      if (!live[s]) continue;
+      double c = 0.0;
+      if (!A.nobb && l1 > l0) c = c + sbb[s] * bb_expfac(A, ig, h[s]);
+      cap[s] = bf_ff_add(A, ii[s], ig, h[s], c);
+    }
+  } else {
+#pragma unroll 1
+    for (int s = 0; s < OPAC_FS; ++s) {
+      if (!valid[s]) continue;
+      const double* s_gl = A.stage_rows ? s_rows + s * OPAC_CT + lane : nullptr;
+      if (A.ngs == 1) {
+        cap[s] = subgroup_opacity(A, ii[s], s_gl, ig, live[s], etab);
+      } else {
+        // collapse subgridding, physical_opacity.f:252-264
+        double sp = 0.0, sr = 0.0;
+        for (int g = 1; g <= A.ngs; ++g) {
+          const double v = subgroup_opacity(A, ii[s], s_gl, (ig - 1) * A.ngs + g, live[s], etab);
+          if (v > 0.0) { sp = sp + v; sr = sr + 1.0 / v; }
+        }
+        const double help = 1.0 / A.ngs;
+        const double capp = sp * help;
+        double capr = sr * help;
+        if (capr > 0.0) capr = 1.0 / capr;
+        cap[s] = (1.0 - A.mix) * capp + A.mix * capr;
       }
-      const double help = 1.0 / A.ngs;
-      const double capp = sp * help;
-      double capr = sr * help;
-      if (capr > 0.0) capr = 1.0 / capr;
-      cap = (1.0 - A.mix) * capp + A.mix * capr;
     }
   }
-  float c32 = (float)cap, e32 = 0.f;
-  if (live) {
-    const double wl = 0.5 * (A.grp_wl[ig] + A.grp_wl[ig - 1]);
-    const double B_nu = (wl * wl / pc_c) * planck(wl, A.temp[i]);
-    e32 = (float)(0.0 + cap * B_nu);
-    int f = 0;
-    if (c32 == 0.f) f |= 1;
-    if (c32 < 0.f) f |= 2;
-    if (c32 != c32) f |= 4;
-    if (c32 > FLT_MAX) f |= 8;
-    if (f) atomicOr(A.flags, f);
+#pragma unroll
+  for (int s = 0; s < OPAC_FS; ++s) {
+    const int i = ii[s];
+    float c32 = (float)cap[s], e32 = 0.f;
+    if (live[s]) {
+      const double wl = 0.5 * (A.grp_wl[ig] + A.grp_wl[ig - 1]);
+      const double B_nu = (wl * wl / pc_c) * planck(wl, A.temp[i]);
+      e32 = (float)(0.0 + cap[s] * B_nu);
+      int f = 0;
+      if (c32 == 0.f) f |= 1;
+      if (c32 < 0.f) f |= 2;
+      if (c32 != c32) f |= 4;
+      if (c32 > FLT_MAX) f |= 8;
+      if (f) atomicOr(A.flags, f);
+    }
+    if (valid[s] && A.cap64) A.cap64[(size_t)(ig - 1) * A.nc + i] = cap[s];
+    tcap[s * OPAC_CT + lane][warp] = c32;
+    tem[s * OPAC_CT + lane][warp] = e32;
+    if (A.capg64) tcapd[s * OPAC_CT + lane][warp] = cap[s];
   }
-  if (valid && A.cap64) A.cap64[(size_t)(ig - 1) * A.nc + i] = cap;
-  tcap[lane][warp] = c32;
-  tem[lane][warp] = e32;
-  if (A.capg64) tcapd[lane][warp] = cap;
   __syncthreads();
   // write (ng, ncell): each shell's OPAC_GT consecutive groups together
-  const int ci = threadIdx.x / OPAC_GT, gj = threadIdx.x % OPAC_GT;
-  const int i2 = blockIdx.x * OPAC_CT + ci, g2 = blockIdx.y * OPAC_GT + gj;
-  if (i2 < A.nc && g2 < A.ng) {
-    A.cap32[(size_t)i2 * A.ng + g2] = tcap[ci][gj];
-    A.emiss32[(size_t)i2 * A.ng + g2] = tem[ci][gj];
-    if (A.capg64) A.capg64[(size_t)i2 * A.ng + g2] = tcapd[ci][gj];
+  for (int t = threadIdx.x; t < OPAC_FC * OPAC_GT; t += blockDim.x) {
+    const int ci = t / OPAC_GT, gj = t % OPAC_GT;
+    const int i2 = base + ci, g2 = blockIdx.y * OPAC_GT + gj;
+    if (i2 < A.nc && g2 < A.ng) {
+      A.cap32[(size_t)i2 * A.ng + g2] = tcap[ci][gj];
+      A.emiss32[(size_t)i2 * A.ng + g2] = tem[ci][gj];
+      if (A.capg64) A.capg64[(size_t)i2 * A.ng + g2] = tcapd[ci][gj];
+    }
   }
 }
 
@@ -1075,9 +1171,17 @@ __global__ void opac_cell_bwd_kernel(int nc, int nelem, int nst, const int32_t* 
 // ============================================================ launchers
 // Shared memory of opacity_fwd_kernel's staged population rows (sets
 // A.stage_rows); rows beyond 40 KB are read from grndlev instead.
+// Dynamic shared memory of opacity_fwd_kernel: the block's staged population
+// rows (up to 160 rows; beyond, the kernel reads grndlev).  Above 48 KB the
+// kernel's limit is raised once.
 static size_t fwd_rows_smem(OpacArgs& A) {
-  const size_t b = sizeof(double) * 32 * (size_t)A.nlrow;
-  A.stage_rows = (!A.nobb && A.nlrow > 0 && b <= 40 * 1024) ? 1 : 0;
+  const size_t b = sizeof(double) * OPAC_FC * (size_t)A.nlrow;
+  A.stage_rows = (!A.nobb && A.nlrow > 0 && b <= 80 * 1024) ? 1 : 0;
+  static bool raised = false;
+  if (A.stage_rows && b > 48 * 1024 && !raised) {
+    cudaFuncSetAttribute(opacity_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024);
+    raised = true;
+  }
   return A.stage_rows ? b : 0;
 }
 
@@ -1188,7 +1292,7 @@ int launch_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_
   const int rc = opacity_prepare(ctx, gas, flags, gas_sig, A);
   if (rc) return rc;
   A.cap32 = gas_cap; A.emiss32 = gas_emiss; A.cap64 = cap64;
-  dim3 grid((A.nc + OPAC_CT - 1) / OPAC_CT, (A.ng + OPAC_GT - 1) / OPAC_GT);
+  dim3 grid((A.nc + OPAC_FC - 1) / OPAC_FC, (A.ng + OPAC_GT - 1) / OPAC_GT);
   const size_t shm = fwd_rows_smem(A);
   opacity_fwd_kernel<<<grid, OPAC_GT * 32, shm, ctx->stream>>>(A);
   return cuda_check(ctx, cudaGetLastError(), "opacity_fwd launch");
@@ -1203,7 +1307,7 @@ int launch_physical_opacity64(slg_ctx* ctx, const slg_gas* gas, double* gas_sig,
   const int rc = opacity_prepare(ctx, gas, &fl, gas_sig, A);
   if (rc) return rc;
   A.cap32 = gas_cap; A.emiss32 = gas_emiss; A.capg64 = capg64;
-  dim3 grid((A.nc + OPAC_CT - 1) / OPAC_CT, (A.ng + OPAC_GT - 1) / OPAC_GT);
+  dim3 grid((A.nc + OPAC_FC - 1) / OPAC_FC, (A.ng + OPAC_GT - 1) / OPAC_GT);
   const size_t shm = fwd_rows_smem(A);
   opacity_fwd_kernel<<<grid, OPAC_GT * 32, shm, ctx->stream>>>(A);
   return cuda_check(ctx, cudaGetLastError(), "opacity_fwd launch");

@@ -69,6 +69,26 @@ def test_physical_opacity_on_reference_atomic_data(hot, oracle, flags):
     _assert_opacity_parity(got, ref)
 
 
+@pytest.mark.parametrize("nrow", [100, 170])
+def test_physical_opacity_many_population_rows(hot, oracle, nrow):
+    """Lines spread over many ion stages: the forward kernel stages the
+    population rows that lines reference in shared memory for up to 160 rows
+    (above 80 rows beyond the default 48 KB) and reads them from global memory
+    beyond; both against the oracle."""
+    import dataclasses
+    case = cases.reference_opacity_case(oracle, ncell=40, ng=100, nline=20000, seed=13, lines="synthetic")
+    ni = case.gas.ion_ni
+    slots = [(iz, ii) for iz in range(1, len(ni) + 1) for ii in range(1, min(iz, int(ni[iz - 1]) - 1) + 1)]
+    assert len(slots) >= nrow
+    lines = case.lines.copy()
+    pick = np.arange(len(lines)) % nrow
+    lines["iz"] = np.array([slots[k][0] for k in pick], dtype=np.int16)
+    lines["ii"] = np.array([slots[k][1] for k in pick], dtype=np.int16)
+    case = dataclasses.replace(case, lines=lines)
+    _setup(hot, case)
+    _assert_opacity_parity(_gpu_opacity(hot, case), oracle.physical_opacity(case))
+
+
 def test_physical_opacity_config2_matches_oracle(hot, oracle):
     """Opacity at the physical-opacity workload's full size (256 shells x 2000
     groups x 5e5 synthetic lines) on the reference's Verner, Sutherland and
