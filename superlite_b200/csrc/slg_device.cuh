@@ -211,8 +211,10 @@ struct u32x4 { uint32_t a, b, c, d; };
 __device__ inline u32x4 philox4x32_10(u32x4 ctr, uint32_t k0, uint32_t k1) {
 #pragma unroll
   for (int r = 0; r < 10; ++r) {
-    const uint32_t hi0 = __umulhi(0xD2511F53u, ctr.a), lo0 = 0xD2511F53u * ctr.a;
-    const uint32_t hi1 = __umulhi(0xCD9E8D57u, ctr.c), lo1 = 0xCD9E8D57u * ctr.c;
+    // one 32 x 32 -> 64-bit multiply gives both halves
+    const uint64_t p0 = (uint64_t)0xD2511F53u * ctr.a, p1 = (uint64_t)0xCD9E8D57u * ctr.c;
+    const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
     ctr = u32x4{hi1 ^ ctr.b ^ k0, lo1, hi0 ^ ctr.d ^ k1, lo0};
     k0 += 0x9E3779B9u;
     k1 += 0xBB67AE85u;

@@ -76,7 +76,9 @@ struct PhiloxStream32 {
     }
     ++j;
     const uint32_t u = i == 0u ? w[0] : (i == 1u ? w[1] : (i == 2u ? w[2] : w[3]));
-    return ((float)(u >> 9) + 0.5f) * 0x1p-23f;
+    // (m + 1/2) 2^-23 for the top 23 bits m: 1 + m 2^-23 (the bits under the
+    // exponent of 1) minus 1 - 2^-24, exact (both operands in [1/2, 2])
+    return __uint_as_float(0x3F800000u | (u >> 9)) - 0.99999994f;
   }
 };
 
