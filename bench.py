@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=None,
                     help="timed steps (default 1 for the batched workload, whose step runs about a minute; 3 otherwise)")
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--transport-variant", type=int, choices=(0, 1, 2, 3), default=None,
+                    help="batched workload: run this particle-loop variant (no autotuner, no tuning steps)")
     ap.add_argument("--no-tune-steps", dest="tune_steps", action="store_false",
                     help="batched workload: keep the sample autotuner's variant instead of timing each variant on "
                          "one whole untimed step")
@@ -537,7 +539,11 @@ def run_batched(a):
     # step's particles (the first 1e6 slots), then the particle loop with the
     # chosen variant
     ts.prepare(seed0 - 1)
-    variant, tune_ms = ts.autotune(seed=seed0 - 1, nsample=1_000_000)
+    if a.transport_variant is None:
+        variant, tune_ms = ts.autotune(seed=seed0 - 1, nsample=1_000_000)
+    else:
+        variant, tune_ms = a.transport_variant, None
+        hot._check(hot.lib.slg_set_transport_variant(hot.h, variant))
     ts.finish(seed0 - 1)
     ts.sync()
     # the kernel variants on whole steps (untimed, beside the warm-ups): the
@@ -546,7 +552,7 @@ def run_batched(a):
     # kept for the warm-ups and the timed steps
     ev_p = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     full_ms = {}
-    if a.tune_steps:
+    if a.tune_steps and a.transport_variant is None:
         for v in range(4):
             hot._check(hot.lib.slg_set_transport_variant(hot.h, v))
             ts.prepare(seed0 - 10 - v)
