@@ -51,13 +51,14 @@ SEED_CASE = 2
 L_BOL = 1e42
 # algorithmic bytes of one particle-step: event-based SoA traffic, 2 x (5 x 8 + 4 x 4 + 8) B
 BYTES_PER_STEP = 128.0
-# Warp instructions issued per particle-step by particle_advance_mixed_kernel and
-# the active lanes per warp instruction, from one ncu capture of that kernel on
-# the batched workload at 0.1x particle budgets (smsp__inst_executed.sum /
-# particle-steps of the launch; smsp__thread_inst_executed.sum /
-# smsp__inst_executed.sum): profiles/particle_advance_mixed_batched_128models_npart0.1.md
-MIXED_WARP_INST_PER_STEP = 51.1
-MIXED_LANES_PER_INST = 9.95
+# Per particle-loop variant (0..3: particle_advance_mixed_kernel<4..7>): warp
+# instructions issued per particle-step and active lanes per warp instruction,
+# from one ncu capture of each variant on the batched workload at 0.1x particle
+# budgets (--transport-variant V; smsp__inst_executed.sum / particle-steps of
+# the launch; smsp__thread_inst_executed.sum / smsp__inst_executed.sum):
+# profiles/particle_advance_mixed_batched_128models_npart0.1.md
+MIXED_WARP_INST_PER_STEP = {0: 50.2, 1: 52.6, 2: 55.1, 3: 59.6}
+MIXED_LANES_PER_INST = {0: 9.99, 1: 9.61, 2: 9.33, 3: 9.03}
 
 
 def parse():
@@ -611,7 +612,7 @@ def run_batched(a):
     from superlite_b200 import peaks as PK
     pipes = PK.measure(local)
     issue_peak = pipes["warp_inst_issue_per_s"]["value"]
-    issue = MIXED_WARP_INST_PER_STEP * tr_rate if tr_rate else None
+    issue = MIXED_WARP_INST_PER_STEP[variant] * tr_rate if tr_rate else None
     res = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -629,18 +630,18 @@ def run_batched(a):
         "roofline": {"bound": "issue", "achieved": issue, "peak": issue_peak, "unit": "warp-instructions/s",
                      "frac": issue / issue_peak if issue else None,
                      # DRAM bytes of one launch: ncu dram__bytes_read.sum + dram__bytes_write.sum of this
-                     # kernel on the same batch with particle budgets x 0.1 (4.157e9 B for 2.944e7
-                     # particles: the packets read and written once, plus table and tally traffic),
-                     # scaled by the particles of this launch
-                     "traffic": 4.157e9 * float(b.npart.sum()) / 2.944e7,
-                     "traffic_basis": "ncu capture of particle_advance_mixed_kernel at 0.1x particle budgets "
-                                      "(4.16 GB), scaled by particles",
-                     "kernel": "particle_advance_mixed_kernel",
-                     "basis": f"{MIXED_WARP_INST_PER_STEP} warp instructions per particle-step (ncu) x particle-"
-                              "steps/s of the last warm-up step's particle loop; peak = measured FP32-FMA issue "
-                              "rate of this GPU (slg_pipe_throughput, one warp instruction per cycle per "
-                              "scheduler)",
-                     "simt_lanes_per_warp_instruction": MIXED_LANES_PER_INST,
+                     # kernel on the same batch with particle budgets x 0.1 (4.11e9-4.20e9 B for 2.944e7
+                     # particles over the four variants: the packets read and written once, plus table
+                     # and tally traffic), scaled by the particles of this launch
+                     "traffic": 4.19e9 * float(b.npart.sum()) / 2.944e7,
+                     "traffic_basis": "ncu capture of particle_advance_mixed_kernel<7> at 0.1x particle budgets "
+                                      "(4.19 GB), scaled by particles",
+                     "kernel": f"particle_advance_mixed_kernel<{variant + 4}>",
+                     "basis": f"{MIXED_WARP_INST_PER_STEP[variant]} warp instructions per particle-step of this "
+                              "variant (ncu) x particle-steps/s of the last warm-up step's particle loop; peak = "
+                              "measured FP32-FMA issue rate of this GPU (slg_pipe_throughput, one warp instruction "
+                              "per cycle per scheduler)",
+                     "simt_lanes_per_warp_instruction": MIXED_LANES_PER_INST[variant],
                      "hbm": {"achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak if achieved else None, "binding": False,
                              "basis": f"{BYTES_PER_STEP:.0f} B per particle-step (event-based SoA traffic); "
