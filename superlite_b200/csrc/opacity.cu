@@ -1169,19 +1169,14 @@ __global__ void opac_cell_bwd_kernel(int nc, int nelem, int nst, const int32_t* 
 }  // namespace
 
 // ============================================================ launchers
-// Shared memory of opacity_fwd_kernel's staged population rows (sets
-// A.stage_rows); rows beyond 40 KB are read from grndlev instead.
-// Dynamic shared memory of opacity_fwd_kernel: the block's staged population
-// rows (up to 160 rows; beyond, the kernel reads grndlev).  Above 48 KB the
-// kernel's limit is raised once.
-static size_t fwd_rows_smem(OpacArgs& A) {
+// Dynamic shared memory of opacity_fwd_kernel (sets A.stage_rows): the block's
+// staged population rows, up to 160 rows (beyond, the kernel reads grndlev);
+// above 48 KB the kernel's limit is raised on the device once.
+static size_t fwd_rows_smem(const slg_ctx* ctx, OpacArgs& A) {
   const size_t b = sizeof(double) * OPAC_FC * (size_t)A.nlrow;
   A.stage_rows = (!A.nobb && A.nlrow > 0 && b <= 80 * 1024) ? 1 : 0;
-  static bool raised = false;
-  if (A.stage_rows && b > 48 * 1024 && !raised) {
-    cudaFuncSetAttribute(opacity_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024);
-    raised = true;
-  }
+  static unsigned raised = 0;
+  if (A.stage_rows && b > 48 * 1024) raise_smem_limit(raised, ctx->device, opacity_fwd_kernel, 80 * 1024);
   return A.stage_rows ? b : 0;
 }
 
@@ -1223,11 +1218,8 @@ static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_f
     const size_t shm = 16 + sizeof(double) * nedge_pad + sizeof(unsigned int) * (nedge + 1);
     if (shm > 220 * 1024)
       return set_error(ctx, SLG_ERR_ARG, "too many sub-groups for line binning (%d)", ngsub);
-    static size_t shm_set = 0;  // raised only when needed (no attribute calls on repeated launches)
-    if (shm > shm_set) {
-      cudaFuncSetAttribute(bin_lines_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-      shm_set = 220 * 1024;
-    }
+    static unsigned raised = 0;  // per device; no attribute calls on repeated launches
+    if (shm > 48 * 1024) raise_smem_limit(raised, ctx->device, bin_lines_kernel, 220 * 1024);
     const int64_t per_block = 256 * 8;
     const int nb = (int)((ctx->nline + per_block - 1) / per_block);
     bin_lines_kernel<<<nb, 256, shm, st>>>(ctx->d_bb, ctx->nline, d_wlsub, nedge, nedge_pad, d_counts,
@@ -1293,7 +1285,7 @@ int launch_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_
   if (rc) return rc;
   A.cap32 = gas_cap; A.emiss32 = gas_emiss; A.cap64 = cap64;
   dim3 grid((A.nc + OPAC_FC - 1) / OPAC_FC, (A.ng + OPAC_GT - 1) / OPAC_GT);
-  const size_t shm = fwd_rows_smem(A);
+  const size_t shm = fwd_rows_smem(ctx, A);
   opacity_fwd_kernel<<<grid, OPAC_GT * 32, shm, ctx->stream>>>(A);
   return cuda_check(ctx, cudaGetLastError(), "opacity_fwd launch");
 }
@@ -1308,7 +1300,7 @@ int launch_physical_opacity64(slg_ctx* ctx, const slg_gas* gas, double* gas_sig,
   if (rc) return rc;
   A.cap32 = gas_cap; A.emiss32 = gas_emiss; A.capg64 = capg64;
   dim3 grid((A.nc + OPAC_FC - 1) / OPAC_FC, (A.ng + OPAC_GT - 1) / OPAC_GT);
-  const size_t shm = fwd_rows_smem(A);
+  const size_t shm = fwd_rows_smem(ctx, A);
   opacity_fwd_kernel<<<grid, OPAC_GT * 32, shm, ctx->stream>>>(A);
   return cuda_check(ctx, cudaGetLastError(), "opacity_fwd launch");
 }
@@ -1350,11 +1342,10 @@ int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, con
   const size_t shm =
       sizeof(double) * ((size_t)((gred ? 1 : 2) * A.nlrow + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
   if (shm > 200 * 1024) return set_error(ctx, SLG_ERR_ARG, "opacity adjoint: too many ion slots (%d)", A.nlrow);
-  static size_t shm_set[2] = {0, 0};  // raised only when needed
-  if (shm > 48 * 1024 && shm > shm_set[gred]) {
-    cudaFuncSetAttribute(gred ? opacity_bwd_kernel<true> : opacity_bwd_kernel<false>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    shm_set[gred] = 200 * 1024;
+  static unsigned raised[2] = {0, 0};  // per device and form
+  if (shm > 48 * 1024) {
+    if (gred) raise_smem_limit(raised[1], ctx->device, opacity_bwd_kernel<true>, 200 * 1024);
+    else raise_smem_limit(raised[0], ctx->device, opacity_bwd_kernel<false>, 200 * 1024);
   }
   dim3 grid((nc + OPAC_CT - 1) / OPAC_CT, (A.ng + OPAC_GT - 1) / OPAC_GT);
   if (gred)

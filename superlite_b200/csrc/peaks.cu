@@ -89,10 +89,25 @@ __global__ void exp_eval_kernel(int64_t n, const double* __restrict__ x, double*
 
 }  // namespace
 
+namespace {
+// The calling thread's current device, selected for the call and put back.
+struct DeviceScope {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceScope(int device) {
+    ok = cudaGetDevice(&prev) == cudaSuccess && cudaSetDevice(device) == cudaSuccess;
+  }
+  ~DeviceScope() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+}  // namespace
+
 extern "C" int slg_exp_eval(int device, int64_t n, const double* x, double* y) {
   if (n < 0 || (n > 0 && (!x || !y))) return SLG_ERR_ARG;
   if (n == 0) return SLG_OK;
-  if (cudaSetDevice(device) != cudaSuccess) return SLG_ERR_CUDA;
+  DeviceScope dev(device);
+  if (!dev.ok) return SLG_ERR_CUDA;
   double* d = nullptr;
   if (cudaMalloc(&d, sizeof(double) * 2 * (size_t)n) != cudaSuccess) return SLG_ERR_OOM;
   int rc = SLG_OK;
@@ -110,7 +125,8 @@ extern "C" int slg_exp_eval(int device, int64_t n, const double* x, double* y) {
 
 extern "C" int slg_pipe_throughput(int device, int which, int iters, double* ops_per_s, float* ms) {
   if (!ops_per_s || iters < 1 || which < 0 || which > 3) return SLG_ERR_ARG;
-  if (cudaSetDevice(device) != cudaSuccess) return SLG_ERR_CUDA;
+  DeviceScope dev(device);
+  if (!dev.ok) return SLG_ERR_CUDA;
   int nsm = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return SLG_ERR_CUDA;
   const int nblk = nsm * PK_BLOCKS_PER_SM;

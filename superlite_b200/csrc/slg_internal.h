@@ -167,6 +167,18 @@ struct slg_ctx {
 };
 
 namespace slg {
+// Raises kernel `fn`'s dynamic shared-memory limit to `bytes` on the current
+// device (the context's: every entry point selects it) the first time a
+// launch there needs it; the attribute holds per device, so `mask` keeps one
+// bit per device id.
+template <class F>
+inline void raise_smem_limit(unsigned& mask, int device, F* fn, int bytes) {
+  const unsigned bit = device >= 0 && device < 32 ? 1u << device : 0u;
+  if (bit && (mask & bit)) return;
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  mask |= bit;
+}
+
 int set_error(slg_ctx* ctx, int code, const char* fmt, ...);
 int cuda_check(slg_ctx* ctx, cudaError_t e, const char* what);
 void* scratch(slg_ctx* ctx, int slot, size_t bytes);  // nullptr on failure (error set)
