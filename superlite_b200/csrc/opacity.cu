@@ -196,31 +196,43 @@ __global__ void opac_cell_prep_kernel(int nc, int nelem, int nst, const int32_t*
 // (:238, nonlinear); those are flagged in ffclamp (bit iz - 1) and added per
 // group.  Elements with fr = 0 add +0 in the reference (:240-241) and are left
 // out.  The sum is re-associated (one product by help per group instead of one
-// per element): a rounding-level difference.
+// per element): a rounding-level difference.  For the adjoint: D[j] = sum_z
+// z^2 fr_z (G[j, igg] - G[j, igg - 1]) over the same elements (d gff / d dgg
+// is linear in the row weights too), and ffclamp_all flags every clamped
+// element whatever its fr (d cap / d fr needs them all).
 // One thread per (shell, table row j).
 __global__ void ff_sum_kernel(int nc, int nelem, const double* __restrict__ natomfr, const int* __restrict__ ffigg,
                               const double* __restrict__ ffdgg, const double* __restrict__ G,
-                              double* __restrict__ ffsum, unsigned* __restrict__ ffclamp) {
+                              double* __restrict__ ffsum, double* __restrict__ ffdsum, unsigned* __restrict__ ffclamp,
+                              unsigned* __restrict__ ffclamp_all) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (int64_t)nc * FF_NU) return;
   const int i = (int)(t / FF_NU), j = (int)(t % FF_NU);
   const double* nfr = natomfr + (size_t)(nelem + 1) * i;
-  double S = 0.0;
-  unsigned clamp = 0;
+  double S = 0.0, D = 0.0;
+  unsigned clamp = 0, clamp_all = 0;
   for (int iz = 1; iz <= nelem; ++iz) {
     const double fr = nfr[iz];
-    if (fr == 0.0) continue;
     const int igg = ffigg[(size_t)(iz - 1) * nc + i];
     if (igg < 0) {
-      clamp |= 1u << (iz - 1);
+      clamp_all |= 1u << (iz - 1);
+      if (fr != 0.0) clamp |= 1u << (iz - 1);
       continue;
     }
+    if (fr == 0.0) continue;
     const double dgg = ffdgg[(size_t)(iz - 1) * nc + i];
-    const double gz = (1.0 - dgg) * G[j + FF_NU * (igg - 1)] + dgg * G[j + FF_NU * igg];
-    S = S + (double)(iz * iz) * fr * gz;
+    const double g0 = G[j + FF_NU * (igg - 1)], g1 = G[j + FF_NU * igg];
+    const double gz = (1.0 - dgg) * g0 + dgg * g1;
+    const double w = (double)(iz * iz) * fr;
+    S = S + w * gz;
+    D = D + w * (g1 - g0);
   }
   ffsum[(size_t)i * FF_NU + j] = S;
-  if (j == 0) ffclamp[i] = clamp;
+  ffdsum[(size_t)i * FF_NU + j] = D;
+  if (j == 0) {
+    ffclamp[i] = clamp;
+    ffclamp_all[i] = clamp_all;
+  }
 }
 
 // Which ion slots (iz,ii) carry any population: 1 if any cell has oc != 0.
@@ -458,7 +470,9 @@ struct OpacArgs {
   const int* ffigg;         // [iz-1][cell], negative: apply gff >= 1
   const double* ffdgg;
   const double* ffsum;      // [cell][81]: sum over unclamped elements of z^2 fr gff at each table row
+  const double* ffdsum;     // [cell][81]: the same of z^2 fr d gff / d dgg
   const unsigned* ffclamp;  // [cell]: elements (bit iz-1) with fr != 0 under the gff >= 1 clamp
+  const unsigned* ffclamp_all;  // [cell]: every element under the clamp
   const double* gff;        // (81,41)
   double ffc1;
   float* cap32;             // (ng, ncell)
@@ -1030,20 +1044,27 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const Opac
       const double dlnhelp = -0.5 / T - eu * uu / (T * (1.0 - eu));
       const double ln10 = 2.302585092994045684;
       const double dru = -10.0 / (ln10 * T), drgg = -5.0 / (ln10 * T);  // table coordinates vs T
+      // unclamped elements from the shell's sums over elements (ff_sum_kernel):
+      // S = sum z^2 fr gff, dS/dT through the table row (du) and column (dgg);
+      // their d cap / d fr by ff_weight_kernel and ff_fr_bwd_kernel
+      const double* Sv = A.ffsum + (size_t)i * FF_NU;
+      const double* Dv = A.ffdsum + (size_t)i * FF_NU;
+      const double s0 = Sv[iu - 1], s1 = Sv[iu];
+      double S = (1.0 - du) * s0 + du * s1;
+      double dS = (s1 - s0) * dru + ((1.0 - du) * Dv[iu - 1] + du * Dv[iu]) * drgg;
+      // elements under the gff >= 1 clamp, one by one
       const double* nfr = A.natomfr + (size_t)(A.nelem + 1) * i;
-      double S = 0.0, dS = 0.0;
-      for (int iz = 1; iz <= A.nelem; ++iz) {
+      for (unsigned m = A.ffclamp_all[i]; m; m &= m - 1) {
+        const int iz = __ffs(m);
         const double fr = nfr[iz];
-        int igg = A.ffigg[(size_t)(iz - 1) * A.nc + i];
-        const bool clamp1 = igg < 0;
-        igg = clamp1 ? -igg : igg;
+        const int igg = -A.ffigg[(size_t)(iz - 1) * A.nc + i];
         const double dgg = A.ffdgg[(size_t)(iz - 1) * A.nc + i];
         const double* G = A.gff;
         const double g00 = G[(iu - 1) + FF_NU * (igg - 1)], g10 = G[iu + FF_NU * (igg - 1)];
         const double g01 = G[(iu - 1) + FF_NU * igg], g11 = G[iu + FF_NU * igg];
         const double graw = (1.0 - du) * (1.0 - dgg) * g00 + du * (1.0 - dgg) * g10 + (1.0 - du) * dgg * g01 +
                             du * dgg * g11;
-        const bool flat = clamp1 && graw < 1.0;
+        const bool flat = graw < 1.0;
         const double g = flat ? 1.0 : graw;
         const double dg = flat ? 0.0
                                : ((1.0 - dgg) * (g10 - g00) + dgg * (g11 - g01)) * dru +
@@ -1088,6 +1109,65 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const Opac
 // holds shell tx and slots ty, ty + 8, ty + 16, ty + 24.  Runs after
 // opacity_bwd_kernel and before opac_cell_bwd_kernel (one writer per entry).
 constexpr int BFB_T = 32;
+// d cap(g, i) / d fr(z, i) = help(g, i) z^2 gff_z(g, i) for the elements
+// without the gff >= 1 clamp, where gff_z = (1 - du_g) Gz[iu_g - 1] + du_g
+// Gz[iu_g] is linear in the table-row weights: sum_g u_g help_g gff_z =
+// sum_j W[j] Gz[j] with W[j] the row weights of all groups, weighted by
+// u_g help_g (u = dL/dcap).  ff_weight_kernel forms W per shell (one thread
+// per (shell, group), the warp's contributions to one row summed first),
+// ff_fr_bwd_kernel adds
+// z^2 sum_j W[j] Gz[j] to gfr (after opacity_bwd_kernel, which adds the
+// clamped elements).
+__global__ void ff_weight_kernel(const OpacArgs A, const double* __restrict__ gcap, double* __restrict__ W) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  int key = -1;
+  double wlo = 0.0, whi = 0.0;
+  if (t < (int64_t)A.nc * A.ng) {
+    const int i = (int)(t / A.ng), g = (int)(t % A.ng);
+    const double u = A.mass[i] > 0.0 ? gcap[t] : 0.0;
+    if (u != 0.0) {
+      const double h = A.hckt[i];
+      const double wl = A.wlsub[g];
+      const double uu = h / wl;
+      const double ru = 10.0 * (log10(uu) + 4.0) + 1.0;
+      const int iu = ru < 1.0 ? 1 : (ru >= (double)(FF_NU - 1) ? FF_NU - 1 : (int)floor(ru));
+      const double du = ru - iu;
+      const double help = A.ffc1 * sqrt(h) * (1.0 - exp(-uu)) * cube(wl) * A.hlparr[i];
+      key = i * FF_NU + (iu - 1);
+      wlo = u * help * (1.0 - du);
+      whi = u * help * du;
+    }
+  }
+  // one atomic pair per distinct (shell, row) of the warp: a shell's
+  // consecutive groups fall on the same few rows
+  const unsigned grp = __match_any_sync(0xffffffffu, key);
+  double slo = 0.0, shi = 0.0;
+  for (unsigned m = grp; m; m &= m - 1) {
+    const int src = __ffs(m) - 1;
+    slo += __shfl_sync(grp, wlo, src);
+    shi += __shfl_sync(grp, whi, src);
+  }
+  if (key >= 0 && lane == __ffs(grp) - 1) {
+    atomicAdd(W + key, slo);
+    atomicAdd(W + key + 1, shi);
+  }
+}
+
+__global__ void ff_fr_bwd_kernel(const OpacArgs A, const double* __restrict__ W, double* __restrict__ gfr) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)A.nc * A.nelem) return;
+  const int i = (int)(t / A.nelem), iz = (int)(t % A.nelem) + 1;
+  const int igg = A.ffigg[(size_t)(iz - 1) * A.nc + i];
+  if (igg < 0) return;  // clamped: opacity_bwd_kernel
+  const double dgg = A.ffdgg[(size_t)(iz - 1) * A.nc + i];
+  const double* G = A.gff;
+  const double* w = W + (size_t)i * FF_NU;
+  double acc = 0.0;
+  for (int j = 0; j < FF_NU; ++j) acc = acc + w[j] * ((1.0 - dgg) * G[j + FF_NU * (igg - 1)] + dgg * G[j + FF_NU * igg]);
+  gfr[(size_t)i * (A.nelem + 1) + iz] += (double)(iz * iz) * acc;
+}
+
 // population rows x shells from which the adjoint accumulates d/d(population)
 // in global memory: measured on B200, shared accumulators won at 40 rows x 256
 // shells and global reductions at 40 rows x 4096 shells
@@ -1235,15 +1315,17 @@ static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_f
   opac_cell_prep_kernel<<<dim3((nc + 127) / 128, nelem), 128, 0, st>>>(
       nc, nelem, nst, ctx->d_ion_ni, gas->temp, gas->natom, gas->nelec, gas->vol, gas->mass, gas->oc,
       gas->ginv, flags->nothmson, d_hckt, gas_sig, d_hlp, d_grnd, d_ffigg, d_ffdgg);
-  double* d_ffsum = nullptr;
+  double *d_ffsum = nullptr, *d_ffdsum = nullptr;
   unsigned* d_ffclamp = nullptr;
   if (!flags->noff && ctx->d_gff) {
-    d_ffsum = (double*)scratch(ctx, 88, sizeof(double) * (size_t)nc * FF_NU);
-    d_ffclamp = (unsigned*)scratch(ctx, 89, sizeof(unsigned) * (size_t)nc);
+    d_ffsum = (double*)scratch(ctx, 88, sizeof(double) * 2 * (size_t)nc * FF_NU);
+    d_ffclamp = (unsigned*)scratch(ctx, 89, sizeof(unsigned) * 2 * (size_t)nc);
     if (!d_ffsum || !d_ffclamp) return SLG_ERR_OOM;
+    d_ffdsum = d_ffsum + (size_t)nc * FF_NU;
     const int64_t nt = (int64_t)nc * FF_NU;
     ff_sum_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(nc, nelem, gas->natomfr, d_ffigg, d_ffdgg,
-                                                                ctx->d_gff, d_ffsum, d_ffclamp);
+                                                                ctx->d_gff, d_ffsum, d_ffdsum, d_ffclamp,
+                                                                d_ffclamp + nc);
   }
   const bool do_bf = !flags->nobf;
   double* d_xsc = nullptr;
@@ -1271,7 +1353,8 @@ static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_f
   A.xsc = d_xsc; A.bslot = d_bslot; A.bnnz = d_bnnz;
   A.hckt = d_hckt; A.hlparr = d_hlp; A.mass = gas->mass; A.natomfr = gas->natomfr; A.temp = gas->temp;
   A.ffigg = d_ffigg; A.ffdgg = d_ffdgg; A.gff = ctx->d_gff;
-  A.ffsum = d_ffsum; A.ffclamp = d_ffclamp;
+  A.ffsum = d_ffsum; A.ffdsum = d_ffdsum; A.ffclamp = d_ffclamp;
+  A.ffclamp_all = d_ffclamp ? d_ffclamp + nc : nullptr;
   A.ffc1 = ff_c1a * sqrt(ff_c1b);
   A.cap32 = nullptr; A.emiss32 = nullptr; A.cap64 = nullptr; A.capg64 = nullptr; A.flags = d_flags;
   if (!ctx->d_gff && !A.noff) return set_error(ctx, SLG_ERR_STATE, "free-free table not set");
@@ -1352,6 +1435,15 @@ int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, con
     opacity_bwd_kernel<true><<<grid, OPAC_GT * 32, shm, st>>>(A, B);
   else
     opacity_bwd_kernel<false><<<grid, OPAC_GT * 32, shm, st>>>(A, B);
+  if (!A.noff) {
+    double* W = (double*)scratch(ctx, 90, sizeof(double) * ((size_t)nc * FF_NU + 1));
+    if (!W) return SLG_ERR_OOM;
+    cudaMemsetAsync(W, 0, sizeof(double) * ((size_t)nc * FF_NU + 1), st);
+    const int64_t nw = (int64_t)nc * A.ng;
+    ff_weight_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(A, gcap, W);
+    const int64_t nf = (int64_t)nc * A.nelem;
+    ff_fr_bwd_kernel<<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(A, W, gfr);
+  }
   if (!A.nobf) {
     const dim3 bgrid((nc + BFB_T - 1) / BFB_T, (A.maxact + BFB_T - 1) / BFB_T);
     bf_bwd_kernel<<<bgrid, BFB_T * 8, 0, st>>>(A, B);
