@@ -527,6 +527,10 @@ def run_batched(a):
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        # the single-GPU comparisons (FP64 forms, configs[0]/[2], opacity) would
+        # only repeat per rank what the N = 1 line reports; the N-GPU line keeps
+        # the timed step, e2e and the clocks, so the GPUs are held briefly
+        a.no_fp64 = a.no_configs = a.no_opacity = True
     b = W.analytic_batch(nmodel=a.nmodel, seed=SEED_BATCH + 1000 * rank)
     if a.npart_scale != 1.0:
         b = W.analytic_batch(nmodel=a.nmodel, seed=SEED_BATCH + 1000 * rank,
