@@ -181,7 +181,9 @@ __global__ void opac_cell_prep_kernel(int nc, int nelem, int nst, const int32_t*
     }
     const double gg = (double)(iz * iz) * pc_rydberg * h;
     const double rgg = 5.0 * (log10(gg) + 4.0) + 1.0;
-    int igg = rgg < 1.0 ? 1 : (rgg >= (double)(FF_NGG - 1) ? FF_NGG - 1 : (int)floor(rgg));
+    // max(floor(rgg), 1) and min(., ff_ngg - 1) as :228-230; a NaN (from a NaN
+    // temperature) takes the lower bound, so the table reads stay in bounds
+    int igg = !(rgg >= 1.0) ? 1 : (rgg >= (double)(FF_NGG - 1) ? FF_NGG - 1 : (int)floor(rgg));
     ffigg[(size_t)(iz - 1) * nc + i] = rgg > (double)FF_NGG ? -igg : igg;  // sign: gff >= 1 clamp (:238)
     ffdgg[(size_t)(iz - 1) * nc + i] = rgg - igg;
   }
@@ -572,7 +574,7 @@ __device__ inline double bf_ff_add(const OpacArgs& A, int i, int igs, double h, 
     const double wlinv = 1.0 / wl;
     const double u = h * wlinv;
     const double ru = 10.0 * (log10(u) + 4.0) + 1.0;
-    const int iu = ru < 1.0 ? 1 : (ru >= (double)(FF_NU - 1) ? FF_NU - 1 : (int)floor(ru));
+    const int iu = !(ru >= 1.0) ? 1 : (ru >= (double)(FF_NU - 1) ? FF_NU - 1 : (int)floor(ru));
     const double du = ru - iu;
     const double help = A.ffc1 * sqrt(h) * (1.0 - exp(-u)) * cube(wl) * A.hlparr[i];
     // sum over elements of z^2 fr gff (ff_sum_kernel), the clamped ones here
@@ -1036,7 +1038,7 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const Opac
       const double wlinv = 1.0 / wl;
       const double uu = h * wlinv;
       const double ru = 10.0 * (log10(uu) + 4.0) + 1.0;
-      const int iu = ru < 1.0 ? 1 : (ru >= (double)(FF_NU - 1) ? FF_NU - 1 : (int)floor(ru));
+      const int iu = !(ru >= 1.0) ? 1 : (ru >= (double)(FF_NU - 1) ? FF_NU - 1 : (int)floor(ru));
       const double du = ru - iu;
       const double eu = exp(-uu);
       const double hn = A.ffc1 * sqrt(h) * (1.0 - eu) * cube(wl);
@@ -1131,7 +1133,7 @@ __global__ void ff_weight_kernel(const OpacArgs A, const double* __restrict__ gc
       const double wl = A.wlsub[g];
       const double uu = h / wl;
       const double ru = 10.0 * (log10(uu) + 4.0) + 1.0;
-      const int iu = ru < 1.0 ? 1 : (ru >= (double)(FF_NU - 1) ? FF_NU - 1 : (int)floor(ru));
+      const int iu = !(ru >= 1.0) ? 1 : (ru >= (double)(FF_NU - 1) ? FF_NU - 1 : (int)floor(ru));
       const double du = ru - iu;
       const double help = A.ffc1 * sqrt(h) * (1.0 - exp(-uu)) * cube(wl) * A.hlparr[i];
       key = i * FF_NU + (iu - 1);
