@@ -1252,13 +1252,15 @@ __global__ void opac_cell_bwd_kernel(int nc, int nelem, int nst, const int32_t* 
 
 // ============================================================ launchers
 // Dynamic shared memory of opacity_fwd_kernel (sets A.stage_rows): the block's
-// staged population rows, up to 160 rows (beyond, the kernel reads grndlev);
-// above 48 KB the kernel's limit is raised on the device once.
+// staged population rows, up to 160 rows (beyond, the kernel reads grndlev).
+// The kernel's dynamic limit is raised on the device before its first staged
+// launch: with its static arrays, a block passes the default 48 KB from about
+// 77 rows on.
 static size_t fwd_rows_smem(const slg_ctx* ctx, OpacArgs& A) {
   const size_t b = sizeof(double) * OPAC_FC * (size_t)A.nlrow;
   A.stage_rows = (!A.nobb && A.nlrow > 0 && b <= 80 * 1024) ? 1 : 0;
   static unsigned raised = 0;
-  if (A.stage_rows && b > 48 * 1024) raise_smem_limit(raised, ctx->device, opacity_fwd_kernel, 80 * 1024);
+  if (A.stage_rows) raise_smem_limit(raised, ctx->device, opacity_fwd_kernel, 80 * 1024);
   return A.stage_rows ? b : 0;
 }
 
@@ -1301,7 +1303,7 @@ static int opacity_prepare(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_f
     if (shm > 220 * 1024)
       return set_error(ctx, SLG_ERR_ARG, "too many sub-groups for line binning (%d)", ngsub);
     static unsigned raised = 0;  // per device; no attribute calls on repeated launches
-    if (shm > 48 * 1024) raise_smem_limit(raised, ctx->device, bin_lines_kernel, 220 * 1024);
+    raise_smem_limit(raised, ctx->device, bin_lines_kernel, 220 * 1024);
     const int64_t per_block = 256 * 8;
     const int nb = (int)((ctx->nline + per_block - 1) / per_block);
     bin_lines_kernel<<<nb, 256, shm, st>>>(ctx->d_bb, ctx->nline, d_wlsub, nedge, nedge_pad, d_counts,
@@ -1427,11 +1429,9 @@ int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, con
   const size_t shm =
       sizeof(double) * ((size_t)((gred ? 1 : 2) * A.nlrow + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
   if (shm > 200 * 1024) return set_error(ctx, SLG_ERR_ARG, "opacity adjoint: too many ion slots (%d)", A.nlrow);
-  static unsigned raised[2] = {0, 0};  // per device and form
-  if (shm > 48 * 1024) {
-    if (gred) raise_smem_limit(raised[1], ctx->device, opacity_bwd_kernel<true>, 200 * 1024);
-    else raise_smem_limit(raised[0], ctx->device, opacity_bwd_kernel<false>, 200 * 1024);
-  }
+  static unsigned raised[2] = {0, 0};  // per device and form (with the static table, before 48 KB)
+  if (gred) raise_smem_limit(raised[1], ctx->device, opacity_bwd_kernel<true>, 200 * 1024);
+  else raise_smem_limit(raised[0], ctx->device, opacity_bwd_kernel<false>, 200 * 1024);
   dim3 grid((nc + OPAC_CT - 1) / OPAC_CT, (A.ng + OPAC_GT - 1) / OPAC_GT);
   if (gred)
     opacity_bwd_kernel<true><<<grid, OPAC_GT * 32, shm, st>>>(A, B);

@@ -577,7 +577,7 @@ int launch_fluxtally(slg_ctx* ctx, int64_t npart, const slg_packet* prt, int32_t
   const size_t shm = (size_t)flx_ng * (2 * sizeof(double) + sizeof(int));
   const int use_smem = shm <= 96 * 1024;
   static unsigned raised = 0;  // per device; no attribute calls on repeated launches
-  if (use_smem && shm > 48 * 1024) raise_smem_limit(raised, ctx->device, fluxtally_kernel, 96 * 1024);
+  if (use_smem) raise_smem_limit(raised, ctx->device, fluxtally_kernel, 96 * 1024);
   long long nb = (npart + 255) / 256;
   const long long cap = (long long)ctx->num_sms * 4;
   if (nb > cap) nb = cap;
