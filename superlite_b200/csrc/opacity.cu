@@ -32,8 +32,8 @@ namespace {
 
 constexpr int OPAC_GT = 8;   // groups per block (one warp each)
 constexpr int OPAC_CT = 32;  // shells per block (one per lane)
-constexpr int OPAC_FS = 2;   // forward: shells per lane (a block covers OPAC_FS * OPAC_CT shells)
-constexpr int OPAC_FC = OPAC_FS * OPAC_CT;
+// forward: FS shells per lane (a block covers FS * OPAC_CT shells), 2 or 4
+// (opacity_fwd_kernel<FS>; launch_fwd picks it)
 
 // ------------------------------------------------------------ TMA bulk helpers
 __device__ inline uint32_t smem_u32(const void* p) {
@@ -486,12 +486,12 @@ struct OpacArgs {
 
 // Sum over n lines of pg * og * exp(-chi h), og the staged population of the
 // line's row for this shell (s_gl: the shell's column of the block's staged
-// rows, OPAC_FC apart); four lines per round: their loads and exps are
+// rows, FC apart); four lines per round: their loads and exps are
 // independent, and the terms are added one after another in line order, each
 // by one fused multiply-add (one rounding where the reference rounds the
 // product and the sum).  INRANGE: the caller has shown -chi h in [-700, 0] for
 // every line.
-template <bool INRANGE>
+template <bool INRANGE, int FC>
 __device__ __forceinline__ double bb_sum_staged(const LineTerm* lt, int n, double h, const double* s_gl,
                                                 const double* etab) {
   double sbb = 0.0;
@@ -502,7 +502,7 @@ __device__ __forceinline__ double bb_sum_staged(const LineTerm* lt, int n, doubl
 #pragma unroll
     for (int q = 0; q < 4; ++q) t[q] = load_line(lt + k + q);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) og[q] = s_gl[line_row(t[q].idx) * OPAC_FC];
+    for (int q = 0; q < 4; ++q) og[q] = s_gl[line_row(t[q].idx) * FC];
 #pragma unroll
     for (int q = 0; q < 4; ++q)
       e[q] = INRANGE ? exp_tang_inrange(-(t[q].chi * h), etab) : exp_tang(-(t[q].chi * h), etab);
@@ -511,52 +511,50 @@ __device__ __forceinline__ double bb_sum_staged(const LineTerm* lt, int n, doubl
   }
   for (; k < n; ++k) {
     const LineVals t = load_line(lt + k);
-    const double og = s_gl[line_row(t.idx) * OPAC_FC];
+    const double og = s_gl[line_row(t.idx) * FC];
     const double e = INRANGE ? exp_tang_inrange(-(t.chi * h), etab) : exp_tang(-(t.chi * h), etab);
     sbb = fma(t.pg * og, e, sbb);
   }
   return sbb;
 }
 
-// bb_sum_staged for the two shells of a lane at once (s_gl: the first shell's
-// column; the second's is OPAC_CT further): each line record's load and index
-// work serves both terms.  Four lines per round: eight independent exps.
-template <bool INRANGE>
-__device__ __forceinline__ void bb_sum_staged2(const LineTerm* lt, int n, double h0, double h1, const double* s_gl,
-                                               const double* etab, double& sbb0, double& sbb1) {
-  double a0 = 0.0, a1 = 0.0;
+// bb_sum_staged for the FS shells of a lane at once (s_gl: the first shell's
+// column; the others' are OPAC_CT apart, rows FS * OPAC_CT apart): each line
+// record's load and index work serves FS terms.  NL lines per round: FS * NL
+// independent exps.
+template <bool INRANGE, int FS, int NL>
+__device__ __forceinline__ void bb_sum_staged_fs(const LineTerm* lt, int n, const double* h, const double* s_gl,
+                                                 const double* etab, double* sbb) {
+  constexpr int FC = FS * OPAC_CT;
+  double a[FS];
+#pragma unroll
+  for (int s = 0; s < FS; ++s) a[s] = 0.0;
   int k = 0;
-  for (; k + 4 <= n; k += 4) {
-    LineVals t[4];
-    double o0[4], o1[4], e0[4], e1[4];
+  for (; k + NL <= n; k += NL) {
+    LineVals t[NL];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) t[q] = load_line(lt + k + q);
+    for (int q = 0; q < NL; ++q) t[q] = load_line(lt + k + q);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const double* r = s_gl + line_row(t[q].idx) * OPAC_FC;
-      o0[q] = r[0];
-      o1[q] = r[OPAC_CT];
-    }
+    for (int q = 0; q < NL; ++q) {
+      const double* r = s_gl + line_row(t[q].idx) * FC;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      e0[q] = INRANGE ? exp_tang_inrange(-(t[q].chi * h0), etab) : exp_tang(-(t[q].chi * h0), etab);
-      e1[q] = INRANGE ? exp_tang_inrange(-(t[q].chi * h1), etab) : exp_tang(-(t[q].chi * h1), etab);
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      a0 = fma(t[q].pg * o0[q], e0[q], a0);
-      a1 = fma(t[q].pg * o1[q], e1[q], a1);
+      for (int s = 0; s < FS; ++s) {
+        const double e = INRANGE ? exp_tang_inrange(-(t[q].chi * h[s]), etab) : exp_tang(-(t[q].chi * h[s]), etab);
+        a[s] = fma(t[q].pg * r[s * OPAC_CT], e, a[s]);
+      }
     }
   }
   for (; k < n; ++k) {
     const LineVals t = load_line(lt + k);
-    const double* r = s_gl + line_row(t.idx) * OPAC_FC;
-    a0 = fma(t.pg * r[0], INRANGE ? exp_tang_inrange(-(t.chi * h0), etab) : exp_tang(-(t.chi * h0), etab), a0);
-    a1 = fma(t.pg * r[OPAC_CT], INRANGE ? exp_tang_inrange(-(t.chi * h1), etab) : exp_tang(-(t.chi * h1), etab),
-             a1);
+    const double* r = s_gl + line_row(t.idx) * FC;
+#pragma unroll
+    for (int s = 0; s < FS; ++s) {
+      const double e = INRANGE ? exp_tang_inrange(-(t.chi * h[s]), etab) : exp_tang(-(t.chi * h[s]), etab);
+      a[s] = fma(t.pg * r[s * OPAC_CT], e, a[s]);
+    }
   }
-  sbb0 = a0;
-  sbb1 = a1;
+#pragma unroll
+  for (int s = 0; s < FS; ++s) sbb[s] = a[s];
 }
 
 // Bound-free and free-free of sub-group igs for shell i (h = hc/kT), added to
@@ -607,8 +605,9 @@ __device__ __forceinline__ double bb_expfac(const OpacArgs& A, int igs, double h
 
 // One sub-group igs for shell i: bb, bf and ff in the reference's order.
 // etab: the exp table (kExp2Tab) in shared memory; s_gl: the shell's column of
-// the block's staged population rows ([line row][OPAC_FC] in shared memory), or
+// the block's staged population rows ([line row][FC] in shared memory), or
 // null (read grndlev).
+template <int FC>
 __device__ inline double subgroup_opacity(const OpacArgs& A, int i, const double* s_gl, int igs, bool live,
                                           const double* etab) {
   double cap = 0.0;
@@ -630,7 +629,7 @@ __device__ inline double subgroup_opacity(const OpacArgs& A, int i, const double
       if (s_gl) {
         // staged populations are clamped at zero, so a term of an unpopulated
         // ion adds +0 (the reference skips it: the same sum)
-        sbb = inrange ? bb_sum_staged<true>(lt, n, h, s_gl, etab) : bb_sum_staged<false>(lt, n, h, s_gl, etab);
+        sbb = inrange ? bb_sum_staged<true, FC>(lt, n, h, s_gl, etab) : bb_sum_staged<false, FC>(lt, n, h, s_gl, etab);
       } else {
         sbb = 0.0;
         for (int k = 0; k < n; ++k) {
@@ -646,31 +645,33 @@ __device__ inline double subgroup_opacity(const OpacArgs& A, int i, const double
   return bf_ff_add(A, i, igs, h, cap);
 }
 
-// Block: OPAC_FC shells x OPAC_GT groups; warp w takes group
-// blockIdx.y * OPAC_GT + w + 1, lane l shells base + l and base + OPAC_CT + l.
+// Block: FS * OPAC_CT shells x OPAC_GT groups; warp w takes group
+// blockIdx.y * OPAC_GT + w + 1, lane l shells base + s OPAC_CT + l, s < FS.
+template <int FS>
 __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_fwd_kernel(const OpacArgs A) {
-  __shared__ float tcap[OPAC_FC][OPAC_GT + 1];
-  __shared__ float tem[OPAC_FC][OPAC_GT + 1];
-  __shared__ double tcapd[OPAC_FC][OPAC_GT + 1];
+  constexpr int FC = FS * OPAC_CT;
+  __shared__ float tcap[FC][OPAC_GT + 1];
+  __shared__ float tem[FC][OPAC_GT + 1];
+  __shared__ double tcapd[FC][OPAC_GT + 1];
   __shared__ double etab[kExpTabN];
-  extern __shared__ double s_rows[];  // [line row][OPAC_FC] populations of this block's shells (A.stage_rows)
+  extern __shared__ double s_rows[];  // [line row][FC] populations of this block's shells (A.stage_rows)
   exp_table_load(etab);
-  const int base = blockIdx.x * OPAC_FC;
+  const int base = blockIdx.x * FC;
   if (A.stage_rows) {
-    for (int k = threadIdx.x; k < A.nlrow * OPAC_FC; k += blockDim.x) {
-      const int ii = base + (k % OPAC_FC);
-      const double v = ii < A.nc ? A.grndlev[(size_t)A.slot_of_lrow[k / OPAC_FC] * A.nc + ii] : 0.0;
+    for (int k = threadIdx.x; k < A.nlrow * FC; k += blockDim.x) {
+      const int ii = base + (k % FC);
+      const double v = ii < A.nc ? A.grndlev[(size_t)A.slot_of_lrow[k / FC] * A.nc + ii] : 0.0;
       s_rows[k] = v < 0.0 ? 0.0 : v;  // the reference skips lines with ocg <= 0
     }
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ig = blockIdx.y * OPAC_GT + warp + 1;  // 1-based group
-  int ii[OPAC_FS];
-  bool valid[OPAC_FS], live[OPAC_FS];
-  double cap[OPAC_FS];
+  int ii[FS];
+  bool valid[FS], live[FS];
+  double cap[FS];
 #pragma unroll
-  for (int s = 0; s < OPAC_FS; ++s) {
+  for (int s = 0; s < FS; ++s) {
     ii[s] = base + s * OPAC_CT + lane;  // 0-based shell
     valid[s] = ig <= A.ng && ii[s] < A.nc;
     live[s] = valid[s] && A.mass[ii[s]] > 0.0;
@@ -679,20 +680,25 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_fwd_kernel(const Opac
   if (A.ngs == 1 && A.stage_rows) {
     // both shells' bound-bound sums in one pass over the group's lines
     // (a shell that is not live runs the loop with h = 0 and is discarded)
-    double h[OPAC_FS];
+    double h[FS];
 #pragma unroll
-    for (int s = 0; s < OPAC_FS; ++s) h[s] = live[s] ? A.hckt[ii[s]] : 0.0;
+    for (int s = 0; s < FS; ++s) h[s] = live[s] ? A.hckt[ii[s]] : 0.0;
     const int l0 = ig <= A.ng ? A.lstart[ig] : 0, l1 = ig <= A.ng ? A.lstart[ig + 1] : 0;
-    double sbb[OPAC_FS] = {0.0, 0.0};
+    double sbb[FS];
+#pragma unroll
+    for (int s = 0; s < FS; ++s) sbb[s] = 0.0;
     if (!A.nobb && l1 > l0) {
-      const bool inrange = h[0] >= 0.0 && h[0] * A.chimax <= 700.0 && h[1] >= 0.0 && h[1] * A.chimax <= 700.0;
+      bool inrange = true;
+#pragma unroll
+      for (int s = 0; s < FS; ++s) inrange = inrange && h[s] >= 0.0 && h[s] * A.chimax <= 700.0;
+      constexpr int NL = FS == 2 ? 4 : 2;  // eight exps in flight
       if (inrange)
-        bb_sum_staged2<true>(A.lt + l0, l1 - l0, h[0], h[1], s_rows + lane, etab, sbb[0], sbb[1]);
+        bb_sum_staged_fs<true, FS, NL>(A.lt + l0, l1 - l0, h, s_rows + lane, etab, sbb);
       else
-        bb_sum_staged2<false>(A.lt + l0, l1 - l0, h[0], h[1], s_rows + lane, etab, sbb[0], sbb[1]);
+        bb_sum_staged_fs<false, FS, NL>(A.lt + l0, l1 - l0, h, s_rows + lane, etab, sbb);
     }
 #pragma unroll
-    for (int s = 0; s < OPAC_FS; ++s) {
+    for (int s = 0; s < FS; ++s) {
       if (!live[s]) continue;
       double c = 0.0;
       if (!A.nobb && l1 > l0) c = c + sbb[s] * bb_expfac(A, ig, h[s]);
@@ -700,16 +706,16 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_fwd_kernel(const Opac
     }
   } else {
 #pragma unroll 1
-    for (int s = 0; s < OPAC_FS; ++s) {
+    for (int s = 0; s < FS; ++s) {
       if (!valid[s]) continue;
       const double* s_gl = A.stage_rows ? s_rows + s * OPAC_CT + lane : nullptr;
       if (A.ngs == 1) {
-        cap[s] = subgroup_opacity(A, ii[s], s_gl, ig, live[s], etab);
+        cap[s] = subgroup_opacity<FC>(A, ii[s], s_gl, ig, live[s], etab);
       } else {
         // collapse subgridding, physical_opacity.f:252-264
         double sp = 0.0, sr = 0.0;
         for (int g = 1; g <= A.ngs; ++g) {
-          const double v = subgroup_opacity(A, ii[s], s_gl, (ig - 1) * A.ngs + g, live[s], etab);
+          const double v = subgroup_opacity<FC>(A, ii[s], s_gl, (ig - 1) * A.ngs + g, live[s], etab);
           if (v > 0.0) { sp = sp + v; sr = sr + 1.0 / v; }
         }
         const double help = 1.0 / A.ngs;
@@ -721,7 +727,7 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_fwd_kernel(const Opac
     }
   }
 #pragma unroll
-  for (int s = 0; s < OPAC_FS; ++s) {
+  for (int s = 0; s < FS; ++s) {
     const int i = ii[s];
     float c32 = (float)cap[s], e32 = 0.f;
     if (live[s]) {
@@ -742,7 +748,7 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_fwd_kernel(const Opac
   }
   __syncthreads();
   // write (ng, ncell): each shell's OPAC_GT consecutive groups together
-  for (int t = threadIdx.x; t < OPAC_FC * OPAC_GT; t += blockDim.x) {
+  for (int t = threadIdx.x; t < FC * OPAC_GT; t += blockDim.x) {
     const int ci = t / OPAC_GT, gj = t % OPAC_GT;
     const int i2 = base + ci, g2 = blockIdx.y * OPAC_GT + gj;
     if (i2 < A.nc && g2 < A.ng) {
@@ -1111,6 +1117,8 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const Opac
 // holds shell tx and slots ty, ty + 8, ty + 16, ty + 24.  Runs after
 // opacity_bwd_kernel and before opac_cell_bwd_kernel (one writer per entry).
 constexpr int BFB_T = 32;
+// shells from which the forward takes four shells per lane
+constexpr int kFwdFourShellsMin = 2048;
 // d cap(g, i) / d fr(z, i) = help(g, i) z^2 gff_z(g, i) for the elements
 // without the gff >= 1 clamp, where gff_z = (1 - du_g) Gz[iu_g - 1] + du_g
 // Gz[iu_g] is linear in the table-row weights: sum_g u_g help_g gff_z =
@@ -1251,17 +1259,31 @@ __global__ void opac_cell_bwd_kernel(int nc, int nelem, int nst, const int32_t* 
 }  // namespace
 
 // ============================================================ launchers
-// Dynamic shared memory of opacity_fwd_kernel (sets A.stage_rows): the block's
-// staged population rows, up to 160 rows (beyond, the kernel reads grndlev).
-// The kernel's dynamic limit is raised on the device before its first staged
-// launch: with its static arrays, a block passes the default 48 KB from about
-// 77 rows on.
-static size_t fwd_rows_smem(const slg_ctx* ctx, OpacArgs& A) {
-  const size_t b = sizeof(double) * OPAC_FC * (size_t)A.nlrow;
+// One launch of opacity_fwd_kernel on the stream.  Shells per lane: 4 on large
+// grids (each line record serves four terms; measured on B200 at 4096 shells:
+// 11.2 against 11.7 ms), 2 where four would leave too few blocks for the SMs
+// (256 shells: 0.39 against 0.41 ms) or too many staged rows.  The block's
+// population rows are staged in shared memory up to 80 KB of them (beyond,
+// the kernel reads grndlev); the kernel's dynamic limit is raised on the
+// device before its first staged launch (with its static arrays a block
+// passes the default 48 KB from about 77 rows at 2 shells per lane).
+static int launch_fwd(slg_ctx* ctx, OpacArgs& A) {
+  const size_t rows4 = sizeof(double) * 4 * OPAC_CT * (size_t)A.nlrow;
+  const bool four = A.nc >= kFwdFourShellsMin && (A.nobb || A.nlrow == 0 || rows4 <= 80 * 1024);
+  const int fs = four ? 4 : 2;
+  const size_t b = sizeof(double) * fs * OPAC_CT * (size_t)A.nlrow;
   A.stage_rows = (!A.nobb && A.nlrow > 0 && b <= 80 * 1024) ? 1 : 0;
-  static unsigned raised = 0;
-  if (A.stage_rows) raise_smem_limit(raised, ctx->device, opacity_fwd_kernel, 80 * 1024);
-  return A.stage_rows ? b : 0;
+  const size_t shm = A.stage_rows ? b : 0;
+  static unsigned raised[2] = {0, 0};  // per device and form
+  const dim3 grid((A.nc + fs * OPAC_CT - 1) / (fs * OPAC_CT), (A.ng + OPAC_GT - 1) / OPAC_GT);
+  if (four) {
+    raise_smem_limit(raised[1], ctx->device, opacity_fwd_kernel<4>, 80 * 1024);
+    opacity_fwd_kernel<4><<<grid, OPAC_GT * 32, shm, ctx->stream>>>(A);
+  } else {
+    raise_smem_limit(raised[0], ctx->device, opacity_fwd_kernel<2>, 80 * 1024);
+    opacity_fwd_kernel<2><<<grid, OPAC_GT * 32, shm, ctx->stream>>>(A);
+  }
+  return cuda_check(ctx, cudaGetLastError(), "opacity_fwd launch");
 }
 
 // Everything the opacity kernels read, queued on the stream: sub-group edges,
@@ -1371,10 +1393,7 @@ int launch_physical_opacity(slg_ctx* ctx, const slg_gas* gas, const slg_opacity_
   const int rc = opacity_prepare(ctx, gas, flags, gas_sig, A);
   if (rc) return rc;
   A.cap32 = gas_cap; A.emiss32 = gas_emiss; A.cap64 = cap64;
-  dim3 grid((A.nc + OPAC_FC - 1) / OPAC_FC, (A.ng + OPAC_GT - 1) / OPAC_GT);
-  const size_t shm = fwd_rows_smem(ctx, A);
-  opacity_fwd_kernel<<<grid, OPAC_GT * 32, shm, ctx->stream>>>(A);
-  return cuda_check(ctx, cudaGetLastError(), "opacity_fwd launch");
+  return launch_fwd(ctx, A);
 }
 
 // Physical opacity (ngs = 1) with the FP64 result in gas_cap's (ng, ncell)
@@ -1386,10 +1405,7 @@ int launch_physical_opacity64(slg_ctx* ctx, const slg_gas* gas, double* gas_sig,
   const int rc = opacity_prepare(ctx, gas, &fl, gas_sig, A);
   if (rc) return rc;
   A.cap32 = gas_cap; A.emiss32 = gas_emiss; A.capg64 = capg64;
-  dim3 grid((A.nc + OPAC_FC - 1) / OPAC_FC, (A.ng + OPAC_GT - 1) / OPAC_GT);
-  const size_t shm = fwd_rows_smem(ctx, A);
-  opacity_fwd_kernel<<<grid, OPAC_GT * 32, shm, ctx->stream>>>(A);
-  return cuda_check(ctx, cudaGetLastError(), "opacity_fwd launch");
+  return launch_fwd(ctx, A);
 }
 
 int launch_opacity_means64(slg_ctx* ctx, const double* temp, const double* sig, const double* cap,

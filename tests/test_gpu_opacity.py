@@ -89,6 +89,14 @@ def test_physical_opacity_many_population_rows(hot, oracle, nrow):
     _assert_opacity_parity(_gpu_opacity(hot, case), oracle.physical_opacity(case))
 
 
+def test_physical_opacity_large_grid_matches_oracle(hot, oracle):
+    """A grid of more than 2048 shells (not a multiple of the block's 128):
+    the forward takes four shells per lane there."""
+    case = cases.reference_opacity_case(oracle, ncell=2100, ng=40, nline=8000, seed=17, lines="synthetic")
+    _setup(hot, case)
+    _assert_opacity_parity(_gpu_opacity(hot, case), oracle.physical_opacity(case))
+
+
 def test_physical_opacity_config2_matches_oracle(hot, oracle):
     """Opacity at the physical-opacity workload's full size (256 shells x 2000
     groups x 5e5 synthetic lines) on the reference's Verner, Sutherland and
