@@ -930,6 +930,7 @@ struct OpacBwd {
   double* goc;         // [slot][cell], added to (bound-free)
   double* ghlp;        // (ncell), added to (d cap / d hlparr)
   double* gfr;         // (0:nelem, ncell), added to
+  double* W;           // [cell][81], added to: free-free table-row weights (null with noff)
 };
 
 // The bound-bound part of the adjoint for one (shell, group): adds
@@ -993,12 +994,13 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const Opac
   extern __shared__ double sm[];
   const int nrow = A.nlrow;                          // population rows the lines reference
   const int nacc = GRED ? 0 : nrow;                  // shared accumulator rows
-  double* s_grnd = sm;                               // [line row][32] (not GRED)
-  double* s_fr = sm + (size_t)nacc * 32;             // [nelem+1][32]
+  double* s_W = sm;                                  // [81][32] free-free table-row weights
+  double* s_grnd = s_W + FF_NU * 32;                 // [line row][32] (not GRED)
+  double* s_fr = s_grnd + (size_t)nacc * 32;         // [nelem+1][32]
   double* s_t = s_fr + (size_t)(A.nelem + 1) * 32;   // [warp][32]
   double* s_h = s_t + OPAC_GT * 32;
   double* s_g = s_h + OPAC_GT * 32;                  // [line row][32] populations of this block's shells
-  const int ntot = (nacc + A.nelem + 1) * 32;
+  const int ntot = (FF_NU + nacc + A.nelem + 1) * 32;
   __shared__ double etab[kExpTabN];
   exp_table_load(etab);
   for (int k = threadIdx.x; k < ntot; k += blockDim.x) sm[k] = 0.0;
@@ -1052,9 +1054,12 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const Opac
       const double dlnhelp = -0.5 / T - eu * uu / (T * (1.0 - eu));
       const double ln10 = 2.302585092994045684;
       const double dru = -10.0 / (ln10 * T), drgg = -5.0 / (ln10 * T);  // table coordinates vs T
+      // this group's weights of table rows iu - 1 and iu, for d cap / d fr of
+      // the unclamped elements (ff_fr_bwd_kernel)
+      atomicAdd(&s_W[(iu - 1) * 32 + lane], u * help * (1.0 - du));
+      atomicAdd(&s_W[iu * 32 + lane], u * help * du);
       // unclamped elements from the shell's sums over elements (ff_sum_kernel):
-      // S = sum z^2 fr gff, dS/dT through the table row (du) and column (dgg);
-      // their d cap / d fr by ff_weight_kernel and ff_fr_bwd_kernel
+      // S = sum z^2 fr gff, dS/dT through the table row (du) and column (dgg)
       const double* Sv = A.ffsum + (size_t)i * FF_NU;
       const double* Dv = A.ffdsum + (size_t)i * FF_NU;
       const double s0 = Sv[iu - 1], s1 = Sv[iu];
@@ -1103,8 +1108,9 @@ __global__ void __launch_bounds__(OPAC_GT * 32, 4) opacity_bwd_kernel(const Opac
     const double v = sm[k];
     const int row = k >> 5, c = blockIdx.x * OPAC_CT + (k & 31);
     if (v == 0.0 || c >= A.nc) continue;
-    if (row < nacc) atomicAdd(&B.ggrnd[(size_t)A.slot_of_lrow[row] * A.nc + c], v);
-    else atomicAdd(&B.gfr[(size_t)c * (A.nelem + 1) + (row - nacc)], v);
+    if (row < FF_NU) atomicAdd(&B.W[(size_t)c * FF_NU + row], v);
+    else if (row < FF_NU + nacc) atomicAdd(&B.ggrnd[(size_t)A.slot_of_lrow[row - FF_NU] * A.nc + c], v);
+    else atomicAdd(&B.gfr[(size_t)c * (A.nelem + 1) + (row - FF_NU - nacc)], v);
   }
 }
 
@@ -1123,47 +1129,11 @@ constexpr int kFwdFourShellsMin = 2048;
 // without the gff >= 1 clamp, where gff_z = (1 - du_g) Gz[iu_g - 1] + du_g
 // Gz[iu_g] is linear in the table-row weights: sum_g u_g help_g gff_z =
 // sum_j W[j] Gz[j] with W[j] the row weights of all groups, weighted by
-// u_g help_g (u = dL/dcap).  ff_weight_kernel forms W per shell (one thread
-// per (shell, group), the warp's contributions to one row summed first),
-// ff_fr_bwd_kernel adds
+// u_g help_g (u = dL/dcap).  opacity_bwd_kernel gathers W per block in shared
+// memory and adds its nonzero entries (a block's eight groups touch a few rows
+// per shell), ff_fr_bwd_kernel adds
 // z^2 sum_j W[j] Gz[j] to gfr (after opacity_bwd_kernel, which adds the
 // clamped elements).
-__global__ void ff_weight_kernel(const OpacArgs A, const double* __restrict__ gcap, double* __restrict__ W) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31;
-  int key = -1;
-  double wlo = 0.0, whi = 0.0;
-  if (t < (int64_t)A.nc * A.ng) {
-    const int i = (int)(t / A.ng), g = (int)(t % A.ng);
-    const double u = A.mass[i] > 0.0 ? gcap[t] : 0.0;
-    if (u != 0.0) {
-      const double h = A.hckt[i];
-      const double wl = A.wlsub[g];
-      const double uu = h / wl;
-      const double ru = 10.0 * (log10(uu) + 4.0) + 1.0;
-      const int iu = !(ru >= 1.0) ? 1 : (ru >= (double)(FF_NU - 1) ? FF_NU - 1 : (int)floor(ru));
-      const double du = ru - iu;
-      const double help = A.ffc1 * sqrt(h) * (1.0 - exp(-uu)) * cube(wl) * A.hlparr[i];
-      key = i * FF_NU + (iu - 1);
-      wlo = u * help * (1.0 - du);
-      whi = u * help * du;
-    }
-  }
-  // one atomic pair per distinct (shell, row) of the warp: a shell's
-  // consecutive groups fall on the same few rows
-  const unsigned grp = __match_any_sync(0xffffffffu, key);
-  double slo = 0.0, shi = 0.0;
-  for (unsigned m = grp; m; m &= m - 1) {
-    const int src = __ffs(m) - 1;
-    slo += __shfl_sync(grp, wlo, src);
-    shi += __shfl_sync(grp, whi, src);
-  }
-  if (key >= 0 && lane == __ffs(grp) - 1) {
-    atomicAdd(W + key, slo);
-    atomicAdd(W + key + 1, shi);
-  }
-}
-
 __global__ void ff_fr_bwd_kernel(const OpacArgs A, const double* __restrict__ W, double* __restrict__ gfr) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (int64_t)A.nc * A.nelem) return;
@@ -1438,12 +1408,18 @@ int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, con
   cudaMemsetAsync(ggrnd, 0, sizeof(double) * ((size_t)nslot * nc + nc), st);
   cudaMemsetAsync(goc, 0, sizeof(double) * (size_t)nslot * nc, st);
   cudaMemsetAsync(gfr, 0, sizeof(double) * (size_t)nc * (A.nelem + 1), st);
-  OpacBwd B{gcap, gT, ggrnd, goc, ghlp, gfr};
+  double* W = nullptr;
+  if (!A.noff) {
+    W = (double*)scratch(ctx, 90, sizeof(double) * ((size_t)nc * FF_NU + 1));
+    if (!W) return SLG_ERR_OOM;
+    cudaMemsetAsync(W, 0, sizeof(double) * ((size_t)nc * FF_NU + 1), st);
+  }
+  OpacBwd B{gcap, gT, ggrnd, goc, ghlp, gfr, W};
   // d/d(population) accumulated in global memory when that array (rows x
   // shells) is large, in shared memory otherwise (bb_adjoint_staged)
   const bool gred = (size_t)A.nlrow * nc >= kBwdGlobalAccMin;
   const size_t shm =
-      sizeof(double) * ((size_t)((gred ? 1 : 2) * A.nlrow + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
+      sizeof(double) * ((size_t)(FF_NU + (gred ? 1 : 2) * A.nlrow + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
   if (shm > 200 * 1024) return set_error(ctx, SLG_ERR_ARG, "opacity adjoint: too many ion slots (%d)", A.nlrow);
   static unsigned raised[2] = {0, 0};  // per device and form (with the static table, before 48 KB)
   if (gred) raise_smem_limit(raised[1], ctx->device, opacity_bwd_kernel<true>, 200 * 1024);
@@ -1454,11 +1430,6 @@ int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, con
   else
     opacity_bwd_kernel<false><<<grid, OPAC_GT * 32, shm, st>>>(A, B);
   if (!A.noff) {
-    double* W = (double*)scratch(ctx, 90, sizeof(double) * ((size_t)nc * FF_NU + 1));
-    if (!W) return SLG_ERR_OOM;
-    cudaMemsetAsync(W, 0, sizeof(double) * ((size_t)nc * FF_NU + 1), st);
-    const int64_t nw = (int64_t)nc * A.ng;
-    ff_weight_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(A, gcap, W);
     const int64_t nf = (int64_t)nc * A.nelem;
     ff_fr_bwd_kernel<<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(A, W, gfr);
   }
