@@ -1162,11 +1162,21 @@ __global__ void __launch_bounds__(BFB_T * 8) bf_bwd_kernel(const OpacArgs A, con
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   for (int g0 = 0; g0 < A.ng; g0 += BFB_T) {
+    // the cross sections first: most (group, slot) tiles lie beyond the slots'
+    // ionisation edges, all zero, and are skipped (the forward skips xs = 0)
+    bool nz = false;
     for (int k = threadIdx.x; k < BFB_T * BFB_T; k += blockDim.x) {
-      const int r = k >> 5, q = k & 31;  // su: shell r, group q (coalesced over groups); sx: group r, slot q
-      const int ii = i0 + r, g = g0 + q, gr = g0 + r, a = a0 + q;
+      const int r = k >> 5, q = k & 31;  // sx: group r, slot q
+      const int gr = g0 + r, a = a0 + q;
+      const double x = (gr < A.ng && a < nact) ? A.xstab[(size_t)gr * A.maxact + a] : 0.0;
+      sx[r][q] = x;
+      nz = nz || x != 0.0;
+    }
+    if (!__syncthreads_or(nz)) continue;  // block-uniform
+    for (int k = threadIdx.x; k < BFB_T * BFB_T; k += blockDim.x) {
+      const int r = k >> 5, q = k & 31;  // su: shell r, group q (coalesced over groups)
+      const int ii = i0 + r, g = g0 + q;
       su[r][q] = (ii < A.nc && g < A.ng) ? B.gcap[(size_t)ii * A.ng + g] : 0.0;
-      sx[r][q] = (gr < A.ng && a < nact) ? A.xstab[(size_t)gr * A.maxact + a] : 0.0;
     }
     __syncthreads();
 #pragma unroll 8
