@@ -90,7 +90,7 @@ def parse():
                          "1 = 256 x 2000 x 5e5")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 per-model comparison")
     ap.add_argument("--no-opacity", action="store_true", help="skip the opacity forward/adjoint measurement")
-    ap.add_argument("--no-configs", action="store_true",
+    ap.add_argument("--no-cases", action="store_true",
                     help="skip the lines of the CPU-runnable case and of the full timestep beside the batched one")
     ap.add_argument("--npart-scale", type=float, default=1.0,
                     help="scale the models' particle budgets (small cases for profilers; default 1)")
@@ -527,10 +527,11 @@ def run_batched(a):
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-        # the single-GPU comparisons (FP64 forms, configs[0]/[2], opacity) would
+        # the single-GPU comparisons (FP64 forms, the snapshot series, the full
+        # timestep, opacity) would
         # only repeat per rank what the N = 1 line reports; the N-GPU line keeps
         # the timed step, e2e and the clocks, so the GPUs are held briefly
-        a.no_fp64 = a.no_configs = a.no_opacity = True
+        a.no_fp64 = a.no_cases = a.no_opacity = True
     b = W.analytic_batch(nmodel=a.nmodel, seed=SEED_BATCH + 1000 * rank)
     if a.npart_scale != 1.0:
         b = W.analytic_batch(nmodel=a.nmodel, seed=SEED_BATCH + 1000 * rank,
@@ -701,9 +702,9 @@ def run_batched(a):
         e = batched_e2e(a, b, params, local, seed0)
         e["value"], e["particle_steps"], e["seconds"] = whole_job(e["particle_steps"], e["seconds"])
         res["e2e"] = e
-    if not a.no_configs:
-        res["config0"] = config0_measure(a, local, rank, world)
-        res["config2"] = config2_measure(a, local, rank, world)
+    if not a.no_cases:
+        res["snapshot_series"] = snapshot_series_measure(a, local, rank, world)
+        res["full_timestep"] = full_timestep_measure(a, local, rank, world)
     if not a.no_opacity:
         res["opacity"] = opacity_measure(local, exp_per_s=pipes["fp64_exp_per_s"]["value"])
         res["opacity_cell_group_evals_per_s"] = res["opacity"]["forward"]["cell_group_evals_per_s"]
@@ -810,10 +811,10 @@ def batched_cpu_baseline(a, b, params, budget_s=20.0):
 
 
 # ------------------------------------------------------------------ the other two transport configurations
-CONFIG0 = dict(nx=64, ng=100, npart=1_000_000, nsnap=20, t0=1.0, t1=30.0, seed=21)
+SNAPSHOT_SERIES = dict(nx=64, ng=100, npart=1_000_000, nsnap=20, t0=1.0, t1=30.0, seed=21)
 
 
-def config0_measure(a, local, rank, world):
+def snapshot_series_measure(a, local, rank, world):
     """The CPU-runnable case: 64 shells (v 0-1.5e9 cm/s, 1 Msun broken power law,
     T ~ U(6000, 14000) K per shell, seeded), analytic grey opacity, 100 groups,
     1e6 particles per snapshot, 20 snapshots log-spaced in t = 1-30 d, the
@@ -826,7 +827,7 @@ def config0_measure(a, local, rank, world):
     import torch
     from superlite_b200 import HotPath, workloads as W
     from superlite_b200.timestep import BatchTimestep
-    C0 = CONFIG0
+    C0 = SNAPSHOT_SERIES
     ts_days = np.geomspace(C0["t0"], C0["t1"], C0["nsnap"])
     params = W.TransportParams()
     steps = 0
@@ -865,11 +866,11 @@ def config0_measure(a, local, rank, world):
            "particle_loop_value": steps / (ms_tr / 1e3), "particle_steps": steps, "ms_all_snapshots": ms_all,
            "ms_particle_loops": ms_tr, "timing": "CUDA events on the library stream, every phase of every snapshot"}
     if rank == 0 and world == 1 and not a.no_cpu:
-        res["cpu_baseline"] = config0_cpu(models, params)
+        res["cpu_baseline"] = snapshot_series_cpu(models, params)
     return res
 
 
-def config0_cpu(models, params, sample=40_000):
+def snapshot_series_cpu(models, params, sample=40_000):
     """The oracle on every snapshot of the CPU-runnable case, a particle sample each."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
@@ -897,7 +898,7 @@ def config0_cpu(models, params, sample=40_000):
                       f"static,1, FP64 oracle), particle loop only, {dt:.1f} s"}
 
 
-def config2_measure(a, local, rank, world, npart=50_000_000):
+def full_timestep_measure(a, local, rank, world, npart=50_000_000):
     """The full timestep: 256 shells x 2000 groups, physical LTE opacity from
     5e5 synthetic lines on the reference's Verner, Sutherland and data.ion
     tables (Saha populations from the device equation of state), 5e7 source

@@ -85,7 +85,7 @@ def test_mixed_matches_fp64_statistically(hot, oracle, t_days, kind):
     assert np.all(np.abs(z) < 3.0), z
 
 
-def test_mixed_pure_ddmc_config2_physics(hot):
+def test_mixed_pure_ddmc_full_timestep_physics(hot):
     """The full-timestep case's physics (256 shells x 2000 groups, every shell
     optically thick): the DDMC random walk."""
     from superlite_b200 import PACKET_DTYPE

@@ -97,7 +97,7 @@ def test_physical_opacity_large_grid_matches_oracle(hot, oracle):
     _assert_opacity_parity(_gpu_opacity(hot, case), oracle.physical_opacity(case))
 
 
-def test_physical_opacity_config2_matches_oracle(hot, oracle):
+def test_physical_opacity_full_timestep_size_matches_oracle(hot, oracle):
     """Opacity at the physical-opacity workload's full size (256 shells x 2000
     groups x 5e5 synthetic lines) on the reference's Verner, Sutherland and
     data.ion tables, against the single-threaded oracle (about 2 s)."""
@@ -112,7 +112,7 @@ def test_physical_opacity_config2_matches_oracle(hot, oracle):
                                rtol=1e-12)
 
 
-def test_physical_opacity_config2_shape_properties(hot):
+def test_physical_opacity_full_timestep_size_shape_properties(hot):
     case = cases.opacity_case(ncell=256, ng=2000, nline=500_000, seed=2)
     _setup(hot, case)
     got = _gpu_opacity(hot, case)
