@@ -34,3 +34,29 @@ def test_stratified_order_is_a_spread_permutation():
     # the first eight models span the range: one from each eighth of the sorted times
     ranks = np.searchsorted(np.sort(t), first8)
     assert np.all(np.diff(ranks // 16) == 1) and ranks[0] < 16
+
+
+def test_profile_commands_parse():
+    """Every `python bench.py ...` command that a summary under profiles/ gives
+    as the one that made its figures is accepted by bench.py's parser (the
+    summaries stay reproducible from the committed files)."""
+    import re
+    import shlex
+    import bench
+    prof = os.path.join(ROOT, "profiles")
+    cmds = []
+    for name in sorted(os.listdir(prof)):
+        if not name.endswith(".md"):
+            continue
+        text = open(os.path.join(prof, name)).read().replace("\\\n", " ")
+        for m in re.finditer(r"python bench\.py([^\n#`]*)", text):
+            args = m.group(1).split(">")[0].split("&&")[0]
+            cmds.append((name, shlex.split(args)))
+    assert cmds
+    saved = sys.argv
+    try:
+        for name, args in cmds:
+            sys.argv = ["bench.py"] + [a for a in args if not a.startswith("<")]
+            bench.parse()  # exits (SystemExit) on an unknown flag
+    finally:
+        sys.argv = saved
