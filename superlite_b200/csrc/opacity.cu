@@ -1427,9 +1427,12 @@ int launch_opacity_bwd(slg_ctx* ctx, const slg_gas* gas, const double* gcap, con
   OpacBwd B{gcap, gT, ggrnd, goc, ghlp, gfr, W};
   // d/d(population) accumulated in global memory when that array (rows x
   // shells) is large, in shared memory otherwise (bb_adjoint_staged)
-  const bool gred = (size_t)A.nlrow * nc >= kBwdGlobalAccMin;
-  const size_t shm =
-      sizeof(double) * ((size_t)(FF_NU + (gred ? 1 : 2) * A.nlrow + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
+  // (and where the shared accumulators would not fit in a block's shared memory)
+  auto bwd_smem = [&](bool g) {
+    return sizeof(double) * ((size_t)(FF_NU + (g ? 1 : 2) * A.nlrow + A.nelem + 1) * 32 + 2 * OPAC_GT * 32);
+  };
+  const bool gred = (size_t)A.nlrow * nc >= kBwdGlobalAccMin || bwd_smem(false) > 200 * 1024;
+  const size_t shm = bwd_smem(gred);
   if (shm > 200 * 1024) return set_error(ctx, SLG_ERR_ARG, "opacity adjoint: too many ion slots (%d)", A.nlrow);
   static unsigned raised[2] = {0, 0};  // per device and form (with the static table, before 48 KB)
   if (gred) raise_smem_limit(raised[1], ctx->device, opacity_bwd_kernel<true>, 200 * 1024);
