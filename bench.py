@@ -59,6 +59,14 @@ BYTES_PER_STEP = 128.0
 # profiles/particle_advance_mixed_batched_128models_npart0.1.md
 MIXED_WARP_INST_PER_STEP = {0: 50.2, 1: 52.6, 2: 55.1, 3: 59.6}
 MIXED_LANES_PER_INST = {0: 9.99, 1: 9.61, 2: 9.33, 3: 9.03}
+# The same for the FP64 particle_advance_kernel<5> (variant 1, the autotuner's
+# choice) on the --workload timestep physics (256 shells x 2000 groups, every
+# event a DDMC one), from one ncu capture at 2e5 particles
+# (profiles/launches_timestep_256x2000_1e6.md): warp instructions, active
+# lanes and DRAM bytes (read + write) per particle-step
+FP64_TIMESTEP_INST_PER_STEP = 54.9
+FP64_TIMESTEP_LANES_PER_INST = 13.3
+FP64_TIMESTEP_DRAM_PER_STEP = 2.86e7 / 6.529e8
 
 
 def parse():
@@ -256,6 +264,9 @@ def run_ours(a):
     tr_ms = statistics.mean(t_tr)
     steps_per_launch = steps_total / a.steps
     achieved = BYTES_PER_STEP * steps_per_launch / (tr_ms / 1e3) / 1e9
+    from superlite_b200 import peaks as PK
+    issue_peak = PK.measure(local)["warp_inst_issue_per_s"]["value"]
+    issue = FP64_TIMESTEP_INST_PER_STEP * steps_per_launch / (tr_ms / 1e3)
     opac_evals = a.ncell * a.ng / (statistics.mean(t_op) / 1e3)
     res = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": a.steps,
@@ -267,10 +278,22 @@ def run_ours(a):
         "phase_ms": {"opacity+means": statistics.mean(t_op), "particle_advance": tr_ms},
         "counters_last_step": {k: counters[-1][k] for k in ("npckt", "nflux", "nstepimc", "nstepddmc", "nstepmax",
                                                             "nmethodswap")},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "particle_advance_kernel",
-                     "basis": f"{BYTES_PER_STEP:.0f} B per particle-step x steps per launch / launch time; "
-                              f"peak {peak_kind}"},
+        # bound by instruction issue and latency like the batched line's loop; the
+        # HBM reading on the 128 B per particle-step basis beside it (non-binding)
+        "roofline": {"bound": "issue", "achieved": issue, "peak": issue_peak, "unit": "warp-instructions/s",
+                     "frac": issue / issue_peak,
+                     "traffic": FP64_TIMESTEP_DRAM_PER_STEP * steps_per_launch,
+                     "traffic_basis": "ncu dram__bytes_read.sum + dram__bytes_write.sum of particle_advance_kernel<5> "
+                                      "at 2e5 particles, per particle-step, times this launch's particle-steps",
+                     "kernel": f"particle_advance_kernel (variant {variant})",
+                     "basis": f"{FP64_TIMESTEP_INST_PER_STEP} warp instructions per particle-step (ncu, variant 1) x "
+                              "particle-steps/s of the particle loop; peak = measured FP32-FMA issue rate of this "
+                              "GPU (slg_pipe_throughput)",
+                     "simt_lanes_per_warp_instruction": FP64_TIMESTEP_LANES_PER_INST,
+                     "hbm": {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                             "binding": False,
+                             "basis": f"{BYTES_PER_STEP:.0f} B per particle-step (event-based SoA traffic); "
+                                      f"peak {peak_kind}"}},
         "clocks": clocks,
         "autotune": {"variant": variant, "sample_ms": tune_ms},
         "gpu_launches": 20 * a.steps,
