@@ -246,7 +246,7 @@ __device__ inline double ddop_dT(double tinv, const double* __restrict__ wlinv, 
   return -dopspeccalc(tinv, wlinv, ig) * tinv * (4.0 - x * ex / (ex - 1.0));
 }
 
-__global__ void __launch_bounds__(GB) leakage_bwd_kernel(const LeakArgsT<double> A0, const double* __restrict__ gol,
+__global__ void __launch_bounds__(GB, 4) leakage_bwd_kernel(const LeakArgsT<double> A0, const double* __restrict__ gol,
                                                          double* __restrict__ gcap, double* __restrict__ gsig,
                                                          double* __restrict__ gT) {
   __shared__ double sh[GB];

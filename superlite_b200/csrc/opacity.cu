@@ -818,33 +818,35 @@ __global__ void __launch_bounds__(256) opacity_means_kernel(int nc, int ng, cons
 }
 
 // ------------------------------------------------------------ adjoint (no reference counterpart)
-// Derivatives of the Planck-weight integrands of groupmod.f with respect to
-// x = hc/(lambda k T); both weights are constant where the reference clamps x
-// at 300, and spectintv's NaN guard (groupmod.f:390-392) gives zero.
-__device__ inline double dfplanck(double x) {
-  if (x >= 300.0) return 0.0;
-  const double ex = exp(x), d = ex - 1.0;
-  return 3.0 * sq(x) / d - cube(x) * ex / sq(d);
-}
-__device__ inline double dfross(double x) {
-  if (x >= 300.0) return 0.0;
-  const double ex = exp(x);
-  const double r = (pow4(x) * ex) / sq(ex - 1.0);
-  const double v = r * (4.0 / x + 1.0 - 2.0 * ex / (ex - 1.0));
-  return v != v ? 0.0 : v;
-}
-// d/dT of specintv_elem / spectintv_elem at temperature T (hct = hck/T).
-__device__ inline double dspecintv_dT(double hct, double T, const double* __restrict__ wlinv, int g0) {
+// specintv_elem and spectintv_elem of group g0 and their d/dT at temperature T
+// (hct = hck/T), from one exp of the group's x: the expressions of fplanck and
+// fross (so the same values) and of their derivatives in x, which are zero
+// where the reference clamps x at 300; spectintv's NaN guard
+// (groupmod.f:390-392) gives zero for both.
+__device__ inline void spec_weights_dT(double hct, double T, const double* __restrict__ wlinv, int g0, double& w,
+                                       double& wr, double& dw, double& dwr) {
   const double x1 = hct * wlinv[g0], x2 = hct * wlinv[g0 + 1];
   const double xm = 0.5 * (x2 + x1), ax = fabs(x2 - x1);
-  return -(ftpi4 * ax * (fplanck(xm) + xm * dfplanck(xm))) / T;
-}
-__device__ inline double dspectintv_dT(double hct, double T, const double* __restrict__ wlinv, int g0) {
-  const double x1 = hct * wlinv[g0], x2 = hct * wlinv[g0 + 1];
-  const double xm = 0.5 * (x2 + x1), ax = fabs(x2 - x1);
-  const double f = fross(xm);
-  if (ftpi4r * ax * f != ftpi4r * ax * f) return 0.0;
-  return -(ftpi4r * ax * (f + xm * dfross(xm))) / T;
+  double fp, fr, dfp, dfr;
+  if (xm >= 300.0) {
+    fp = fplanck(xm);
+    fr = fross(xm);
+    dfp = 0.0;
+    dfr = 0.0;
+  } else {
+    const double ex = exp(xm), d = ex - 1.0;
+    fp = cube(xm) / d;
+    fr = (pow4(xm) * ex) / sq(d);
+    dfp = 3.0 * sq(xm) / d - cube(xm) * ex / sq(d);
+    const double v = fr * (4.0 / xm + 1.0 - 2.0 * ex / d);
+    dfr = v != v ? 0.0 : v;
+  }
+  w = ftpi4 * ax * fp;
+  dw = -(ftpi4 * ax * (fp + xm * dfp)) / T;
+  const double sr = ftpi4r * ax * fr;
+  const bool bad = sr != sr;  // groupmod.f:390-392
+  wr = bad ? 0.0 : sr;
+  dwr = bad ? 0.0 : -(ftpi4r * ax * (fr + xm * dfr)) / T;
 }
 
 // opacity_planckmean / opacity_rossmean on the FP64 opacity in (ng, ncell) layout.
@@ -899,13 +901,13 @@ __global__ void __launch_bounds__(256) means_bwd_kernel(int nc, int ng, const do
   double asig = 0.0, at = 0.0;
   for (int g = threadIdx.x; g < ng; g += blockDim.x) {
     const double c = cap[(size_t)i * ng + g];
-    const double w = specintv_elem(hct, wlinv, g);
-    const double wr = spectintv_elem(hct, wlinv, g);
+    double w, wr, dw, dwr;
+    spec_weights_dT(hct, T, wlinv, g, w, wr, dw, dwr);
     const double inv = 1.0 / (s + c);
     const double dr = wr * inv * inv;  // -dR/dc
     gcap[(size_t)i * ng + g] += ug * w + ur * dr;
     asig = asig + ur * dr;
-    at = at + ug * c * dspecintv_dT(hct, T, wlinv, g) - ur * inv * dspectintv_dT(hct, T, wlinv, g);
+    at = at + ug * c * dw - ur * inv * dwr;
   }
   s1[threadIdx.x] = asig;
   s2[threadIdx.x] = at;
